@@ -1,0 +1,327 @@
+"""ctypes mirror of include/dspw.h and loader for libdspw.so.
+
+The C ABI is the product boundary; this module only describes it to Python
+(tests, benchmark, trainer driver).  Enum values and the descriptor layout must
+match include/dspw.h exactly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent.parent          # dsp-weno_b200/
+LIB_PATH = PKG_DIR / "libdspw.so"
+
+ABI_VERSION = 1
+
+MODEL = {"linadv": 0, "burgers": 1, "euler": 2, "ns_es": 3, "ns_kep": 4}
+FLUX = {
+    "lin_ec": 0, "lin_ec4": 1, "lin_tecno": 2, "lin_tecno4": 3,
+    "bur_ec": 4, "bur_ec4": 5, "bur_tecno": 6, "bur_tecno4": 7,
+    "roe": 10, "kep": 11, "kep4": 12, "kepec": 13, "kepec4": 14,
+    "roe_ec": 15, "roe_ec4": 16, "keps": 17, "keps4": 18,
+    "kep_tecno_roe": 19, "kepes_tecno_roe": 20, "kepes_tecno_rusanov": 21,
+    "roe_tecno_roe": 22, "kepes_tecno4_roe": 23, "kepes_tecno4_rusanov": 24,
+    "roe_tecno4_roe": 25,
+}
+RECON = {"sp_weno": 0, "sp_wenoc": 1, "sp_weno_corr2": 2, "sp_weno_dl": 3,
+         "first": 4, "second": 5, "minmod": 6, "minabs": 7}
+BC = {"periodic": 0, "dirichlet": 1, "neumann": 2, "wall": 3}
+TIME = {"rk1": 0, "ssprk3": 1}
+MU = {"constant": 0, "sutherland": 1, "power": 2}
+PRECISION = {"fp64": 0, "fp32_bf16": 1}
+
+STATUS = {0: "DSPW_OK", 1: "DSPW_ERR_ARG", 2: "DSPW_ERR_CUDA", 3: "DSPW_ERR_NONFINITE",
+          4: "DSPW_ERR_NONPOSITIVE", 5: "DSPW_ERR_TIMEOUT", 6: "DSPW_ERR_UNSUPPORTED",
+          7: "DSPW_ERR_NOMEM", 8: "DSPW_ERR_FINISHED"}
+
+
+class Desc(C.Structure):
+    """struct dspw_desc."""
+    _fields_ = [
+        ("abi_version", C.c_int), ("model", C.c_int), ("flux", C.c_int), ("recon", C.c_int),
+        ("time_scheme", C.c_int), ("precision", C.c_int),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("bc", C.c_int * 6), ("ec1_fix", C.c_int), ("mu_model", C.c_int),
+        ("max_iter", C.c_int), ("t_stamps", C.c_int), ("reserved_i", C.c_int * 8),
+        ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
+        ("zmin", C.c_double), ("zmax", C.c_double),
+        ("gamma", C.c_double), ("gas_const", C.c_double), ("prandtl", C.c_double),
+        ("mu_ref", C.c_double), ("T_ref", C.c_double), ("T_0", C.c_double), ("omega", C.c_double),
+        ("lin_vel", C.c_double * 3), ("cfl", C.c_double), ("final_time", C.c_double),
+        ("bc_state", (C.c_double * 5) * 6),
+        ("nn_w", ((C.c_double * 5) * 5) * 4),
+        ("nn_b", (C.c_double * 5) * 4),
+        ("reserved_d", C.c_double * 8),
+    ]
+
+
+class Globals(C.Structure):
+    _fields_ = [("time", C.c_double), ("dt", C.c_double), ("iter", C.c_int), ("finished", C.c_int),
+                ("total_entropy", C.c_double), ("conserved", C.c_double * 5),
+                ("kinetic_energy", C.c_double)]
+
+
+class StatusOut(C.Structure):
+    _fields_ = [("code", C.c_int), ("nonfinite_cells", C.c_longlong), ("nonpositive_cells", C.c_longlong),
+                ("sign_violations", C.c_longlong), ("faces_checked", C.c_longlong)]
+
+
+class TrainCfg(C.Structure):
+    _fields_ = [("lr", C.c_double), ("beta1", C.c_double), ("beta2", C.c_double),
+                ("weight_decay", C.c_double), ("eps", C.c_double), ("batch", C.c_int), ("seed", C.c_int)]
+
+
+def load_network_file(path) -> tuple[np.ndarray, np.ndarray]:
+    """Read a dsp_weno.txt network file (format of Neural_Network::load_network,
+    enflo/src/neural_network.cc:82-130): 'Weights' then 'Biases', each a list of
+    'Layer k' / BEGIN / rows / END blocks.  Returns W (4,5,5) and b (4,5)."""
+    weights, biases = [], []
+    mode = "w"
+    with open(path) as f:
+        lines = [ln.strip() for ln in f]
+    i = 0
+    while i < len(lines):
+        t = lines[i]
+        if t == "Biases":
+            mode = "b"
+        elif t == "BEGIN":
+            rows = []
+            i += 1
+            while lines[i] != "END":
+                vals = [float(v) for v in lines[i].split()]
+                if vals:
+                    rows.append(vals)
+                i += 1
+            if mode == "w":
+                weights.append(np.array(rows, dtype=np.float64))
+            else:
+                biases.append(np.array([r[0] for r in rows], dtype=np.float64))
+        i += 1
+    W = np.stack(weights)
+    b = np.stack(biases)
+    if W.shape != (4, 5, 5) or b.shape != (4, 5):
+        raise ValueError(f"network file {path}: expected 4 layers of 5x5, got {W.shape} {b.shape}")
+    return W, b
+
+
+def save_network_file(path, W, b) -> None:
+    """Write W (4,5,5) and b (4,5) in the dsp_weno.txt format (the trainer's
+    save_net_weights, DSP-WENO_trainer/DSP-WENO_network_trainer.py:197-213)."""
+    with open(path, "w") as f:
+        f.write("Weights\n")
+        for k in range(4):
+            f.write(f"Layer {k + 1}\nBEGIN\n")
+            for row in W[k]:
+                f.write(" ".join("%.18e" % v for v in row) + "\n")
+            f.write("END\n")
+        f.write("Biases\n")
+        for k in range(4):
+            f.write(f"Layer {k + 1}\nBEGIN\n")
+            for v in b[k]:
+                f.write("%.18e\n" % v)
+            f.write("END\n")
+
+
+def xavier_network(seed: int = 6008) -> tuple[np.ndarray, np.ndarray]:
+    """Xavier-uniform weights for the 5-5-5-5-5 network and PyTorch-default
+    uniform(-1/sqrt(5), 1/sqrt(5)) biases (DSP-WENO_network_trainer.py:59-60)."""
+    rng = np.random.default_rng(seed)
+    a = np.sqrt(6.0 / (5 + 5))
+    W = rng.uniform(-a, a, size=(4, 5, 5))
+    b = rng.uniform(-1 / np.sqrt(5), 1 / np.sqrt(5), size=(4, 5))
+    return W, b
+
+
+def make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=64, ny=1, nz=1,
+              x=(0.0, 1.0), y=(0.0, 1.0), z=(0.0, 1.0), bc="periodic", gamma=1.4, gas_const=1.0,
+              prandtl=1.0, mu_ref=0.0, mu_model="constant", T_ref=1.0, T_0=1.0, omega=1.0,
+              lin_vel=(1.0, 0.0, 0.0), cfl=0.4, final_time=1.0, max_iter=1 << 30, t_stamps=1,
+              ec1_fix=False, precision="fp64", time_scheme="ssprk3", network=None,
+              bc_state=None) -> Desc:
+    """Build a dspw_desc from keyword arguments (names follow param.in)."""
+    d = Desc()
+    d.abi_version = ABI_VERSION
+    d.model = MODEL[model]
+    d.flux = FLUX[flux]
+    d.recon = RECON[recon]
+    d.time_scheme = TIME[time_scheme]
+    d.precision = PRECISION[precision]
+    d.nx, d.ny, d.nz = int(nx), int(ny), int(nz)
+    if isinstance(bc, str):
+        bc = [bc] * 6
+    for i, k in enumerate(bc):
+        d.bc[i] = BC[k]
+    d.ec1_fix = int(bool(ec1_fix))
+    d.mu_model = MU[mu_model]
+    d.max_iter = int(max_iter)
+    d.t_stamps = int(t_stamps)
+    d.xmin, d.xmax = map(float, x)
+    d.ymin, d.ymax = map(float, y)
+    d.zmin, d.zmax = map(float, z)
+    d.gamma, d.gas_const, d.prandtl = float(gamma), float(gas_const), float(prandtl)
+    d.mu_ref, d.T_ref, d.T_0, d.omega = float(mu_ref), float(T_ref), float(T_0), float(omega)
+    for i in range(3):
+        d.lin_vel[i] = float(lin_vel[i])
+    d.cfl, d.final_time = float(cfl), float(final_time)
+    if bc_state is not None:
+        for f in range(6):
+            for c in range(5):
+                d.bc_state[f][c] = float(bc_state[f][c])
+    if network is not None:
+        W, b = network
+        for l in range(4):
+            for j in range(5):
+                d.nn_b[l][j] = float(b[l][j])
+                for k in range(5):
+                    d.nn_w[l][j][k] = float(W[l][j][k])
+    return d
+
+
+def nvar(d: Desc) -> int:
+    return 1 if d.model in (0, 1) else 5
+
+
+_LIB = None
+
+
+def lib():
+    """Load libdspw.so (built in-tree).  Raises if it is missing: there is no
+    fallback path."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = os.environ.get("DSPW_LIB", str(LIB_PATH))
+    if not os.path.exists(path):
+        raise RuntimeError(f"libdspw.so not found at {path}; run __graft_entry__.build()")
+    L = C.CDLL(path)
+    P, I, D, LL = C.c_void_p, C.c_int, C.c_double, C.c_longlong
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    sig = {
+        "dspw_error_string": (C.c_char_p, [I]),
+        "dspw_version": (I, []),
+        "dspw_create": (I, [C.POINTER(Desc), C.POINTER(P)]),
+        "dspw_create_batch": (I, [C.POINTER(Desc), I, C.POINTER(P)]),
+        "dspw_destroy": (I, [P]),
+        "dspw_upload_prim": (I, [P, I, dp]),
+        "dspw_download_prim": (I, [P, I, dp]),
+        "dspw_download_cons": (I, [P, I, dp]),
+        "dspw_compute_dt": (I, [P, I, C.POINTER(D)]),
+        "dspw_residual": (I, [P, I, dp]),
+        "dspw_stage": (I, [P, I, D]),
+        "dspw_step": (I, [P, I, D]),
+        "dspw_run": (I, [P, I, C.POINTER(I)]),
+        "dspw_globals": (I, [P, I, C.POINTER(Globals)]),
+        "dspw_last_status": (I, [P, C.POINTER(StatusOut)]),
+        "dspw_errors": (I, [P, I, I, dp, dp]),
+        "dspw_sync": (I, [P]),
+        "dspw_stream": (P, [P]),
+        "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),
+        "dspw_trainer_create": (I, [C.POINTER(TrainCfg), dp, dp, C.POINTER(P)]),
+        "dspw_trainer_destroy": (I, [P]),
+        "dspw_trainer_set_data": (I, [P, dp, dp, LL]),
+        "dspw_trainer_collect": (I, [P, P, LL, C.POINTER(LL)]),
+        "dspw_trainer_epoch": (I, [P, C.POINTER(D)]),
+        "dspw_trainer_loss_grad": (I, [P, dp, dp, I, C.POINTER(D), dp, dp]),
+        "dspw_trainer_get_params": (I, [P, dp, dp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = L
+    return L
+
+
+class DspwError(RuntimeError):
+    def __init__(self, code, where):
+        self.code = code
+        super().__init__(f"{where}: {STATUS.get(code, code)}")
+
+
+def check(code, where=""):
+    if code != 0:
+        raise DspwError(code, where)
+    return code
+
+
+class Solver:
+    """Thin owner of a dspw_handle (one problem or a batch)."""
+
+    def __init__(self, descs):
+        if isinstance(descs, Desc):
+            descs = [descs]
+        self.descs = list(descs)
+        arr = (Desc * len(self.descs))(*self.descs)
+        h = C.c_void_p()
+        check(lib().dspw_create_batch(arr, len(self.descs), C.byref(h)), "dspw_create_batch")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().dspw_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def shape(self, p=0):
+        d = self.descs[p]
+        return (nvar(d), d.nz, d.ny, d.nx)
+
+    def upload_prim(self, prim, p=0):
+        a = np.ascontiguousarray(prim, dtype=np.float64).reshape(self.shape(p))
+        check(lib().dspw_upload_prim(self.h, p, a), "dspw_upload_prim")
+
+    def prim(self, p=0):
+        a = np.empty(self.shape(p))
+        check(lib().dspw_download_prim(self.h, p, a), "dspw_download_prim")
+        return a
+
+    def cons(self, p=0):
+        a = np.empty(self.shape(p))
+        check(lib().dspw_download_cons(self.h, p, a), "dspw_download_cons")
+        return a
+
+    def residual(self, p=0):
+        a = np.empty(self.shape(p))
+        check(lib().dspw_residual(self.h, p, a), "dspw_residual")
+        return a
+
+    def compute_dt(self, p=0):
+        v = C.c_double()
+        check(lib().dspw_compute_dt(self.h, p, C.byref(v)), "dspw_compute_dt")
+        return v.value
+
+    def step(self, n=1, fixed_dt=0.0):
+        check(lib().dspw_step(self.h, int(n), float(fixed_dt)), "dspw_step")
+
+    def run(self, chunk=64):
+        s = C.c_int()
+        check(lib().dspw_run(self.h, int(chunk), C.byref(s)), "dspw_run")
+        return s.value
+
+    def globals(self, p=0):
+        g = Globals()
+        check(lib().dspw_globals(self.h, p, C.byref(g)), "dspw_globals")
+        return g
+
+    def status(self):
+        s = StatusOut()
+        lib().dspw_last_status(self.h, C.byref(s))
+        return s
+
+    def errors(self, exact, comp=0, p=0):
+        e = np.zeros(3)
+        a = np.ascontiguousarray(exact, dtype=np.float64)
+        check(lib().dspw_errors(self.h, p, comp, a, e), "dspw_errors")
+        return e
+
+    def sync(self):
+        check(lib().dspw_sync(self.h), "dspw_sync")

@@ -1,0 +1,225 @@
+/*
+ * dspw.h -- C ABI of the B200 DSP-WENO / SP-WENO TeCNO finite-volume stage path.
+ *
+ * Plain C, no C++ or CUDA types: the reference's C++ driver (or any FFI) binds
+ * it directly.  The library is libdspw.so, built from dsp-weno_b200/csrc.
+ *
+ * What it replaces.  The reference has no plugin API; its per-stage work is a
+ * set of private members of class FV called from the time loop
+ * (enflo/src/fv.cc:1262-1313, enflo_scalar/src_scalar/fv.cc:553-597):
+ *
+ *   compute_dt()        enflo/src/fv.cc:366-383       -> dspw_compute_dt / dspw_step
+ *   prim_to_ent()       enflo/src/fv.cc:421-552       -> fused into every stage
+ *   compute_residual(rk) enflo/src/fv.cc:591-767      -> dspw_stage / dspw_residual
+ *   update_solution(rk) enflo/src/fv.cc:1163-1198     -> dspw_stage
+ *   con_to_prim()+apply_bc() enflo/src/fv.cc:388-400,121-361 -> fused into every stage
+ *   compute_global()    enflo/src/compute_global.cc:10-89 -> dspw_globals
+ *   compute_error()     enflo/src/compute_errors.cc:9-33  -> dspw_errors
+ *   Neural_Network::load_network enflo/src/neural_network.cc:82-130 -> desc.nn_w/nn_b
+ *
+ * Ownership: a handle owns all device memory, its CUDA stream and its CUDA
+ * graphs.  Host pointers passed in are borrowed for the duration of the call.
+ * Threading: one host thread at a time per handle; handles are independent.
+ * Errors: every call returns an int status (DSPW_OK == 0); nothing aborts or
+ * exits across the ABI.  dspw_error_string() names a status.
+ *
+ * Host array layout: interior cells only, FP64, component planes of shape
+ * (nvar, Nz, Ny, Nx) with x fastest.  Primitive components are
+ * (rho, u, v, w, p) for the Euler/NS models and the single value u for the
+ * scalar models; conserved components are (rho, rho u, rho v, rho w, E).
+ */
+#ifndef DSPW_H
+#define DSPW_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSPW_ABI_VERSION 1
+
+/* models (enflo/src/ext_constants.h:23, enflo_scalar/src_scalar/ext_constants.h:19) */
+enum dspw_model { DSPW_LINADV = 0, DSPW_BURGERS = 1, DSPW_EULER = 2, DSPW_NS_ES = 3, DSPW_NS_KEP = 4 };
+
+/* numerical fluxes: scalar names from enflo_scalar/src_scalar/ext_constants.h:17,
+ * system names from enflo/src/ext_constants.h:17-19 */
+enum dspw_flux {
+  DSPW_LIN_EC = 0, DSPW_LIN_EC4 = 1, DSPW_LIN_TECNO = 2, DSPW_LIN_TECNO4 = 3,
+  DSPW_BUR_EC = 4, DSPW_BUR_EC4 = 5, DSPW_BUR_TECNO = 6, DSPW_BUR_TECNO4 = 7,
+  DSPW_ROE = 10, DSPW_KEP = 11, DSPW_KEP4 = 12, DSPW_KEPEC = 13, DSPW_KEPEC4 = 14,
+  DSPW_ROE_EC = 15, DSPW_ROE_EC4 = 16, DSPW_KEPS = 17, DSPW_KEPS4 = 18,
+  DSPW_KEP_TECNO_ROE = 19, DSPW_KEPES_TECNO_ROE = 20, DSPW_KEPES_TECNO_RUSANOV = 21,
+  DSPW_ROE_TECNO_ROE = 22, DSPW_KEPES_TECNO4_ROE = 23, DSPW_KEPES_TECNO4_RUSANOV = 24,
+  DSPW_ROE_TECNO4_ROE = 25
+};
+
+/* reconstructions: param.in names sp_weno, sp_wenoc, sp_weno_corr2, sp_weno_dl
+ * (enflo/src/parameter.cc:179-206) and the simpler schemes of
+ * enflo/src/reconstruct.cc:14-110 */
+enum dspw_recon {
+  DSPW_REC_SP_WENO = 0, DSPW_REC_SP_WENOC = 1, DSPW_REC_SP_WENO_CORR2 = 2, DSPW_REC_SP_WENO_DL = 3,
+  DSPW_REC_FIRST = 4, DSPW_REC_SECOND = 5, DSPW_REC_MINMOD = 6, DSPW_REC_MINABS = 7
+};
+
+/* boundary conditions (enflo/src/ext_constants.h:25).  DIRICHLET is parsed but
+ * not implemented by the reference (enflo/src/parameter.cc:558-562); here it
+ * means: ghost cells hold the fixed primitive state desc.bc_state[face]. */
+enum dspw_bc { DSPW_BC_PERIODIC = 0, DSPW_BC_DIRICHLET = 1, DSPW_BC_NEUMANN = 2, DSPW_BC_WALL = 3 };
+
+enum dspw_time { DSPW_RK1 = 0, DSPW_SSPRK3 = 1 };
+enum dspw_mu { DSPW_MU_CONSTANT = 0, DSPW_MU_SUTHERLAND = 1, DSPW_MU_POWER = 2 };
+
+/* arithmetic of the stage path */
+enum dspw_precision {
+  DSPW_FP64 = 0,       /* plain form: state, fluxes, reconstruction and network in FP64 */
+  DSPW_FP32_BF16 = 1   /* FP32 state/fluxes/reconstruction; network layers as BF16
+                          tensor-core tiles with FP32 accumulation.  Time, CFL max and
+                          global sums stay FP64. */
+};
+
+enum dspw_status_code {
+  DSPW_OK = 0,
+  DSPW_ERR_ARG = 1,          /* bad argument or descriptor */
+  DSPW_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  DSPW_ERR_NONFINITE = 3,    /* NaN/Inf found in the state */
+  DSPW_ERR_NONPOSITIVE = 4,  /* density or pressure <= 0 */
+  DSPW_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+  DSPW_ERR_UNSUPPORTED = 6,  /* combination not implemented */
+  DSPW_ERR_NOMEM = 7,        /* device allocation failed */
+  DSPW_ERR_FINISHED = 8      /* the problem has reached final_time or max_iter */
+};
+
+/* One problem.  Mirrors the param.in surface (enflo/src/parameter.h:14-74). */
+typedef struct dspw_desc {
+  int abi_version;           /* DSPW_ABI_VERSION */
+  int model;                 /* enum dspw_model */
+  int flux;                  /* enum dspw_flux */
+  int recon;                 /* enum dspw_recon */
+  int time_scheme;           /* enum dspw_time */
+  int precision;             /* enum dspw_precision */
+  int nx, ny, nz;            /* cells; ny == 1 / nz == 1 switch that sweep off */
+  int bc[6];                 /* xleft, xright, yleft, yright, zleft, zright */
+  int ec1_fix;               /* EC1_fix yes/no (enflo/src/parameter.cc:396-406) */
+  int mu_model;              /* enum dspw_mu */
+  int max_iter;
+  int t_stamps;              /* output time_stamps; dt is clipped to them like FV::run */
+  int reserved_i[8];
+  double xmin, xmax, ymin, ymax, zmin, zmax;
+  double gamma, gas_const, prandtl, mu_ref, T_ref, T_0, omega;
+  double lin_vel[3];         /* linadv velocity */
+  double cfl, final_time;
+  double bc_state[6][5];     /* DIRICHLET ghost state, primitive (rho,u,v,w,p) or (u) */
+  double nn_w[4][5][5];      /* DSP-WENO layer weights, row = output, col = input */
+  double nn_b[4][5];         /* DSP-WENO layer biases */
+  double reserved_d[8];
+} dspw_desc;
+
+typedef struct dspw_handle dspw_handle;
+
+/* Global quantities of one problem, FP64 sums on the device.  total_entropy is
+ * sum(-rho s/(gamma-1)) vol for systems (enflo/src/compute_global.cc:18-28) and
+ * sum(u^2/2) vol for scalar laws (enflo_scalar/src_scalar/compute_global.cc:12-21). */
+typedef struct dspw_globals_out {
+  double time;
+  double dt;
+  int iter;
+  int finished;
+  double total_entropy;
+  double conserved[5];       /* sum(U) vol per component */
+  double kinetic_energy;     /* sum(rho |u|^2/2) vol (systems) */
+} dspw_globals_out;
+
+/* Device-side health word, accumulated since the last dspw_last_status call. */
+typedef struct dspw_status_out {
+  int code;                  /* first error seen, DSPW_OK if none */
+  long long nonfinite_cells;
+  long long nonpositive_cells;
+  long long sign_violations;  /* faces where (Zji-Zij)(Z_{i+1}-Z_i) < 0 */
+  long long faces_checked;
+} dspw_status_out;
+
+const char* dspw_error_string(int code);
+int dspw_version(void);
+
+/* Create a handle for one problem / for nprob independent problems advanced
+ * together (one launch per kernel over all problems, per-problem dt). */
+int dspw_create(const dspw_desc* desc, dspw_handle** out);
+int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out);
+int dspw_destroy(dspw_handle* h);
+
+/* Interior primitive state of problem p in, conserved/primitive state out. */
+int dspw_upload_prim(dspw_handle* h, int p, const double* prim);
+int dspw_download_prim(dspw_handle* h, int p, double* prim);
+int dspw_download_cons(dspw_handle* h, int p, double* cons);
+
+/* CFL time step cfl*min(h)/max|speed| of the current state (FV::compute_dt). */
+int dspw_compute_dt(dspw_handle* h, int p, double* dt);
+
+/* Residual of the current state (compute_residual(rk), reference sign). */
+int dspw_residual(dspw_handle* h, int p, double* res);
+
+/* One time-integration stage rk with step dt on every problem (dt <= 0 keeps
+ * the per-problem dt of the current step). */
+int dspw_stage(dspw_handle* h, int rk, double dt);
+
+/* Up to nsteps steps of the FV::run loop body on every unfinished problem:
+ * CFL dt, clipping to the next time stamp, all stages, time += dt.  With
+ * fixed_dt > 0 the CFL step is replaced by fixed_dt.  Steps run as one CUDA
+ * graph per step; nothing is copied to the host. */
+int dspw_step(dspw_handle* h, int nsteps, double fixed_dt);
+
+/* Advance every problem until final_time/max_iter, checking completion every
+ * `chunk` steps.  Returns the number of steps of the longest problem. */
+int dspw_run(dspw_handle* h, int chunk, int* steps);
+
+int dspw_globals(dspw_handle* h, int p, dspw_globals_out* g);
+int dspw_last_status(dspw_handle* h, dspw_status_out* s);
+
+/* L1/L2/Linf error of problem p against host values `exact` (same layout as
+ * dspw_download_prim, component comp), volume-weighted like
+ * enflo_scalar/src_scalar/compute_errors.cc:9-30. */
+int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, double err[3]);
+
+/* Synchronise the handle's stream; returns the first error recorded. */
+int dspw_sync(dspw_handle* h);
+
+/* The handle's CUDA stream (a cudaStream_t) so callers can order their own work. */
+void* dspw_stream(dspw_handle* h);
+
+/* Raw device pointer to the conserved state planes of problem p (component
+ * stride in elements returned in *stride) and the element size in bytes (8 or 4). */
+int dspw_device_state(dspw_handle* h, int p, void** ptr, long long* stride, int* elem_bytes);
+
+/* ---- DSP-WENO network training (no counterpart in the reference's C++; the
+ * reference trains with PyTorch in DSP-WENO_trainer/DSP-WENO_network_trainer.py) */
+
+typedef struct dspw_trainer dspw_trainer;
+
+/* Adam settings follow DSP-WENO_trainer/config.py:25-31. */
+typedef struct dspw_train_cfg {
+  double lr, beta1, beta2, weight_decay, eps;
+  int batch;
+  int seed;
+} dspw_train_cfg;
+
+int dspw_trainer_create(const dspw_train_cfg* cfg, const double* w_init /* 4*25 */,
+                        const double* b_init /* 4*5 */, dspw_trainer** out);
+int dspw_trainer_destroy(dspw_trainer* t);
+/* Device-resident data set: n samples of 4 cell values and 2 target interface
+ * values (left, right), host FP64 in. */
+int dspw_trainer_set_data(dspw_trainer* t, const double* stencils /* n*4 */,
+                          const double* targets /* n*2 */, long long n);
+/* Generate stencil/target pairs on the GPU from the current state of a solver
+ * handle: every face of every component contributes its 4-cell stencil and the
+ * plain SP-WENO interface values as targets.  Appends up to max_pairs. */
+int dspw_trainer_collect(dspw_trainer* t, dspw_handle* h, long long max_pairs, long long* added);
+/* One epoch of minibatch Adam on the device; loss = (MSE_left + MSE_right)/2. */
+int dspw_trainer_epoch(dspw_trainer* t, double* mean_loss);
+/* Loss and gradients for one explicit batch (FP64 host in/out), for checks. */
+int dspw_trainer_loss_grad(dspw_trainer* t, const double* stencils, const double* targets, int n,
+                           double* loss, double* grad_w /* 4*25 */, double* grad_b /* 4*5 */);
+int dspw_trainer_get_params(dspw_trainer* t, double* w /* 4*25 */, double* b /* 4*5 */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSPW_H */
