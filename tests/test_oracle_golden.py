@@ -1,0 +1,113 @@
+"""The oracle (oracle/dspw_oracle.c) against golden vectors produced by the
+reference's own code (tests/golden/make_golden.py).  The oracle keeps the
+reference's operation order and is compiled like the reference (gcc -O3, no
+FMA), so agreement is exact up to libm: asserted at 1e-14 relative, and the
+exact-match fraction is reported."""
+import numpy as np
+import pytest
+
+import oracle as O
+from _common import desc_from_cfg, load, net, run_cases
+from dspw.capi import make_desc
+
+
+def _close(a, b, rtol=1e-14):
+    a = np.asarray(a, dtype=np.float64); b = np.asarray(b, dtype=np.float64)
+    tol = rtol * np.maximum(np.abs(b), np.max(np.abs(b)) * 1e-6 + 1e-300)
+    bad = np.abs(a - b) > tol
+    assert not bad.any(), f"{bad.sum()} mismatches, max |diff| {np.max(np.abs(a - b)):.3e}"
+    return float(np.mean(a == b))
+
+
+def test_logavg_golden():
+    g = load("recon.npz")
+    got = np.array([O.logavg(a, b) for a, b in zip(g["la_a"], g["la_b"])])
+    assert _close(got, g["la"]) == 1.0
+
+
+@pytest.mark.parametrize("corr", [0, 1, 2])
+def test_sp_weno_golden(corr):
+    g = load("recon.npz")
+    L = np.zeros(len(g["U"])); R = np.zeros(len(g["U"]))
+    for t, u in enumerate(g["U"]):
+        L[t], R[t] = O.sp_weno(u, corr)
+    _close(L, g[f"spw{corr}_l"])
+    _close(R, g[f"spw{corr}_r"])
+
+
+def test_nn_forward_golden():
+    g = load("recon.npz")
+    d = make_desc(recon="sp_weno_dl", network=net())
+    m = g["nn_mask"]
+    L = np.zeros(len(g["U"])); R = np.zeros(len(g["U"]))
+    for t, u in enumerate(g["U"]):
+        if m[t]:
+            L[t], R[t] = O.nn_forward(d, u)
+    _close(L[m], g["nn_l"][m])
+    _close(R[m], g["nn_r"][m])
+
+
+def _euler_keys():
+    g = load("faces_euler.npz")
+    return sorted({k.rsplit("|", 1)[0] for k in g.files})
+
+
+@pytest.mark.parametrize("key", _euler_keys())
+def test_euler_face_flux_golden(key):
+    g = load("faces_euler.npz")
+    flux, recon, ec1 = key.split("|")
+    d = make_desc(model="euler", flux=flux, recon=recon, ec1_fix=bool(int(ec1)), network=net())
+    dx, dy, dz = g[key + "|h"]
+    P, dirs = g[key + "|P"], g[key + "|dir"]
+    F = np.zeros((len(P), 5)); V = np.zeros((len(P), 4, 5))
+    for t in range(len(P)):
+        F[t], V[t] = O.euler_face_flux(d, P[t], int(dirs[t]), dx, dy, dz)
+    _close(V, g[key + "|V"])
+    _close(F, g[key + "|F"])
+
+
+def _scalar_keys():
+    g = load("faces_scalar.npz")
+    return sorted({k.rsplit("|", 1)[0] for k in g.files})
+
+
+@pytest.mark.parametrize("key", _scalar_keys())
+def test_scalar_face_flux_golden(key):
+    g = load("faces_scalar.npz")
+    flux, recon = key.split("|")
+    model = "linadv" if flux.startswith("lin") else "burgers"
+    d = make_desc(model=model, flux=flux, recon=recon, lin_vel=(1.0, -0.5, 0.25), network=net())
+    dx, dy, dz = g[key + "|h"]
+    U, dirs = g[key + "|U"], g[key + "|dir"]
+    F = np.array([O.scalar_face_flux(d, U[t], int(dirs[t]), dx, dy, dz) for t in range(len(U))])
+    _close(F, g[key + "|F"])
+
+
+@pytest.mark.parametrize("case", run_cases(), ids=lambda c: c[0])
+def test_run_golden(case):
+    name, kind, cfg, nsteps, fixed_dt = case
+    g = load("runs.npz")
+    p0 = g[f"{name}|prim0"]
+    _, nz, ny, nx = p0.shape
+    o = O.Oracle(desc_from_cfg(cfg, nx, ny, nz))
+    o.set_prim(p0)
+    o.step(nsteps, fixed_dt)
+    t, it, dt = o.time()
+    tid = g[f"{name}|tid"]
+    assert it == int(tid[1])
+    assert abs(t - tid[0]) <= 1e-14 * abs(tid[0])
+    _close(o.cons(), g[f"{name}|final"])
+
+
+def test_ooc_known_answers():
+    """Config-1 L1 errors equal the values the reference prints (l1_err.dat)
+    and the survey measured: 1.75268e-05 (sp_weno), 1.74048e-05 (sp_wenoc),
+    2.68879e-05 (sp_weno_dl) at Nx=400."""
+    g = load("ooc.npz")
+    assert abs(g["sp_weno"][2, 0] - 1.75268e-05) < 5e-11
+    assert abs(g["sp_wenoc"][2, 0] - 1.74048e-05) < 5e-11
+    assert abs(g["sp_weno_dl"][2, 0] - 2.68879e-05) < 5e-11
+    for rec in ("sp_weno", "sp_wenoc", "sp_weno_dl"):
+        l1 = g[rec][:, 0]
+        order = np.log(l1[:-1] / l1[1:]) / np.log(2.0)
+        assert np.all(order > 2.9), (rec, order)
