@@ -1,0 +1,378 @@
+"""Benchmark of the stage path: cell-updates/s on 2-D Euler Kelvin-Helmholtz.
+
+Workload (one GPU): Kelvin-Helmholtz on the periodic unit square at 2048^2,
+gamma 1.4, kepes_tecno4_roe flux, DSP-WENO reconstruction (the shipped
+5-5-5-5-5 network), SSPRK3 at CFL 0.4, FP32 state with the network layers on
+BF16 tensor cores (FP64 time, CFL max and global sums).  One step = one full
+SSPRK3 step of every cell; one cell-update = one physical cell advanced by one
+step.  The FP64 plain form (SP-WENO, no network) is measured beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 2048] [--precision fp32_bf16|fp64] [--recon sp_weno_dl]
+
+Under torchrun (N > 1) every rank advances its own 2048^2 problem (weak
+scaling, no data-path collective); NCCL only carries the barrier and the
+max-over-ranks of the device time.
+
+`--impl reference` times the reference's own CPU solver (oracle/_ref, built
+from its sources) on bounded samples of the same workload, on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "dsp-weno_b200"))
+sys.path.insert(0, str(REPO / "oracle"))
+
+METRIC = "cell-updates/s"
+NET_FILE = REPO / "tests" / "golden" / "dsp_weno.txt"
+# per-launch DRAM traffic of the dominant kernel from the committed ncu capture
+# (profiles/sweep_kernels_kh.md); None until measured
+NCU_TRAFFIC_BYTES_PER_CELL = None
+
+
+def kh_prim(n: int, seed: int = 12345) -> np.ndarray:
+    """Kelvin-Helmholtz on [0,1]^2: rho 2 / 1, u 0.5 / -0.5 inside / outside
+    |y-0.5| < 0.25, p 2.5, v = 0.01 sin(4 pi x) + U(-1e-3, 1e-3) seeded noise."""
+    h = 1.0 / n
+    x = (np.arange(n) + 0.5) * h
+    X, Y = np.meshgrid(x, x)
+    inner = np.abs(Y - 0.5) < 0.25
+    rng = np.random.default_rng(seed)
+    p = np.zeros((5, 1, n, n))
+    p[0, 0] = np.where(inner, 2.0, 1.0)
+    p[1, 0] = np.where(inner, 0.5, -0.5)
+    p[2, 0] = 0.01 * np.sin(4 * np.pi * X) + rng.uniform(-1e-3, 1e-3, (n, n))
+    p[4, 0] = 2.5
+    return p
+
+
+# ------------------------------------------------------------------ CPU legs
+
+_REF = None
+
+
+def _ref_worker_init(n, recon):
+    global _REF
+    import oracle as O
+    cfg = dict(model="euler", x=(0, 1), y=(0, 1), Nx=n, Ny=n, Nz=2, cfl=0.4, final_time=1.0, reconstruct=recon,
+               net_file=str(NET_FILE), flux="kepes_tecno4_roe", dim=2,
+               ic=dict(density="1+(abs(y-0.5)<0.25)", xvelocity="-0.5+(abs(y-0.5)<0.25)",
+                       yvelocity="0.01*sin(4*pi*x)", pressure="2.5"), bc="periodic")
+    _REF = O.RefEuler(cfg)
+
+
+def _ref_worker_step(nsteps):
+    t = time.perf_counter()
+    _REF.step(nsteps)
+    return time.perf_counter() - t
+
+
+class RefPool:
+    """All host cores, one reference solver instance per process (the
+    reference is single-threaded).  Started with 'spawn' before any GPU call."""
+
+    def __init__(self, n, recon, procs):
+        ctx = mp.get_context("spawn")
+        self.procs = procs
+        self.n = n
+        self.pool = ctx.Pool(procs, initializer=_ref_worker_init, initargs=(n, recon))
+
+    def step(self, nsteps=1):
+        t0 = time.perf_counter()
+        self.pool.map(_ref_worker_step, [nsteps] * self.procs)
+        return time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ clocks
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ GPU legs
+
+
+def algorithmic_bytes(name, stage, ncell, nv, w):
+    """Minimum HBM bytes of one launch: x sweep reads U^k and writes R; the
+    final (y) sweep reads U^k, R and (stages 2-3) U^n and writes U^(k+1)."""
+    if name == "sweep_x":
+        return ncell * nv * w * 2
+    if name in ("sweep_y", "sweep_z"):
+        return ncell * nv * w * (4 if stage > 0 else 3)
+    return 0
+
+
+def measure_gpu(args, torch, dist, rank, world):
+    import dspw
+    from dspw import Solver, load_network_file, make_desc
+
+    n = args.n
+    net = load_network_file(NET_FILE)
+    prim = kh_prim(n, seed=12345 + rank)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def solver(precision, recon):
+        d = make_desc(model="euler", flux="kepes_tecno4_roe", recon=recon, nx=n, ny=n, nz=1, x=(0, 1), y=(0, 1),
+                      bc="periodic", cfl=0.4, final_time=1.0e9, network=net, precision=precision)
+        s = Solver(d)
+        s.upload_prim(prim)
+        return s
+
+    def timed(s, steps, warmup):
+        stream = torch.cuda.ExternalStream(s.stream_ptr(), device=dev)
+        s.step(warmup)
+        s.sync()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    s = solver(args.precision, args.recon)
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ms = timed(s, args.steps, args.warmup)
+    clk = clocks.stop()
+    st = s.status()
+    g = s.globals()
+    # per-kernel durations of one (un-graphed) step for the roofline
+    prof = s.profile_step()
+    nv, w = 4, (4 if args.precision == "fp32_bf16" else 8)
+    stage, rows = -1, []
+    for name, kms in prof:
+        if name == "sweep_x":
+            stage += 1
+        rows.append((name, stage, kms))
+    dom = max(rows, key=lambda r: r[2])
+    ncell = n * n
+    dom_bytes = algorithmic_bytes(dom[0], dom[1], ncell, nv, w)
+    peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text()) if (REPO / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = dom_bytes / (dom[2] * 1e-3) / 1e9
+    # e2e through the C ABI with host buffers: upload (pinned H2D), one step,
+    # download (D2H) per step
+    pinned = torch.empty(prim.size, dtype=torch.float64, pin_memory=True).numpy().reshape(prim.shape)
+    pinned[...] = prim
+    out = torch.empty(prim.size, dtype=torch.float64, pin_memory=True).numpy().reshape(prim.shape)
+    e2e_steps = max(2, min(args.steps, 10))
+    s.upload_prim(pinned)
+    lib = dspw.lib()
+    s.step(1)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        dspw.check(lib.dspw_upload_prim(s.h, 0, pinned), "upload")
+        dspw.check(lib.dspw_step(s.h, 1, 0.0), "step")
+        dspw.check(lib.dspw_download_cons(s.h, 0, out), "download")
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    # FP64 plain form (SP-WENO, no network) on the same grid for the ratio
+    fp64_ms = None
+    if args.precision == "fp32_bf16" and not args.no_fp64:
+        s64 = solver("fp64", "sp_weno")
+        k64 = max(1, args.steps // 4)
+        fp64_ms = timed(s64, k64, max(1, args.warmup // 2)) / k64
+        del s64
+    launches_per_step = len(prof)
+    return dict(ms=ms, clk=clk, status=st, globals=g, prof=rows, dom=dom, dom_bytes=dom_bytes, achieved=achieved,
+                peak=peak, e2e_s=e2e_s, e2e_steps=e2e_steps, ncell=ncell, launches=launches_per_step,
+                fp64_ms=fp64_ms, h2d=prim.nbytes, d2h=prim.nbytes)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--precision", default="fp32_bf16", choices=["fp32_bf16", "fp64"])
+    ap.add_argument("--recon", default="sp_weno_dl")
+    ap.add_argument("--cpu-sample-n", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    workload = f"kh{args.n}_{args.precision}_{args.recon}_kepes_tecno4_roe"
+    config = {"workload": workload, "grid": [args.n, args.n], "model": "euler2d", "flux": "kepes_tecno4_roe",
+              "recon": args.recon, "precision": args.precision, "cfl": 0.4,
+              "l2": "no flush: per-step working set (U^n, two stage buffers, residual) exceeds the 126 MB L2"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        procs = cpu_cores()
+        pool = RefPool(args.cpu_sample_n, args.recon, procs)
+        for _ in range(args.warmup):
+            pool.step(1)
+        t = 0.0
+        for _ in range(args.steps):
+            t += pool.step(1)
+        pool.close()
+        cells = procs * args.cpu_sample_n ** 2
+        v = cells * args.steps / t
+        sample = (f"{procs} processes x reference enflo solver on a {args.cpu_sample_n}^2 (x2 in z, the reference's "
+                  f"2-D layout) KH grid, {args.steps} steps, physical cells counted")
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "cell-updates/s", "impl": "reference",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                          "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
+                                           "sample": sample},
+                          "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
+    # CPU baseline first (spawned processes, before any GPU call)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            procs = cpu_cores()
+            pool = RefPool(args.cpu_sample_n, args.recon, procs)
+            pool.step(1)
+            k = 3
+            t = sum(pool.step(1) for _ in range(k))
+            pool.close()
+            cpu = {"value": procs * args.cpu_sample_n ** 2 * k / t, "unit": "cell-updates/s", "cores": procs,
+                   "kind": "reference",
+                   "sample": f"{procs} processes x reference solver, {args.cpu_sample_n}^2 (x2) KH grid, "
+                             f"{args.recon}, {k} steps each"}
+        except Exception as e:  # the checker may be unbuilt on a bare box
+            cpu = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = tdist
+    else:
+        torch.cuda.set_device(0)
+    r = measure_gpu(args, torch, dist, rank, world)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    steps = args.steps
+    value = world * r["ncell"] * steps / (r["ms"] * 1e-3)
+    e2e_v = world * r["ncell"] * r["e2e_steps"] / r["e2e_s"]
+    dom = r["dom"]
+    traffic = None
+    if NCU_TRAFFIC_BYTES_PER_CELL is not None:
+        traffic = NCU_TRAFFIC_BYTES_PER_CELL.get(dom[0], None)
+        traffic = traffic * r["ncell"] if traffic else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.precision == "fp32_bf16" else "f64", "data": "synthetic",
+        "config": config,
+        "roofline": {"bound": "hbm", "kernel": dom[0], "stage": dom[1], "achieved": r["achieved"],
+                     "peak": r["peak"], "unit": "GB/s", "frac": r["achieved"] / r["peak"],
+                     "traffic": traffic, "algorithmic_bytes": r["dom_bytes"], "launch_ms": dom[2],
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_v, "unit": "cell-updates/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"], "api": "dspw_upload_prim + dspw_step(1) + dspw_download_cons"},
+        "gpu_launches": r["launches"] * steps,
+        "clocks": r["clk"],
+        "kernels_ms_one_step": [[a, b, round(c, 4)] for a, b, c in r["prof"]],
+        "health": {"code": r["status"].code, "sign_violations": r["status"].sign_violations,
+                   "nonfinite": r["status"].nonfinite_cells, "nonpositive": r["status"].nonpositive_cells},
+    }
+    if r["fp64_ms"]:
+        line["fp64_plain"] = {"value": world * r["ncell"] / (r["fp64_ms"] * 1e-3), "ms_per_step": r["fp64_ms"],
+                              "recon": "sp_weno", "speedup_fp32_bf16_dl_over_fp64_plain": r["fp64_ms"] / (r["ms"] / steps)}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,69 @@
+"""Build libdspw.so (the C ABI of include/dspw.h) for sm_100a with nvcc.
+
+Each precision is its own translation unit: the FP64 plain form is compiled
+with --fmad=false (no FMA contraction, matching the reference's x86-64 build),
+the FP32 form with contraction.  Objects and the library are written in-tree
+(dsp-weno_b200/_build, dsp-weno_b200/libdspw.so).
+
+    python dsp-weno_b200/build.py [--verbose-ptxas]
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+REPO = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libdspw.so"
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+          f"-I{REPO / 'include'}", "--expt-relaxed-constexpr"]
+
+UNITS = {
+    "dspw_fp64.cu": ["--fmad=false"],
+    "dspw_fp32.cu": ["--fmad=true"],
+    "dspw_capi.cu": ["--fmad=false"],
+    "dspw_train.cu": ["--fmad=true"],
+}
+
+
+def compile_unit(name: str, flags: list[str], verbose: bool) -> Path:
+    src = CSRC / name
+    obj = BUILD / (name + ".o")
+    deps = [src] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc")) + [
+        REPO / "include" / "dspw.h"]
+    if obj.exists() and all(obj.stat().st_mtime >= d.stat().st_mtime for d in deps) and not verbose:
+        return obj
+    cmd = [NVCC, *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {name}:\n{r.stderr}")
+    if verbose and r.stderr:
+        print(r.stderr)
+    return obj
+
+
+def build(verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
+        futs = [ex.submit(compile_unit, n, f, verbose) for n, f in UNITS.items()]
+        objs = [f.result() for f in futs]
+    newest = max(o.stat().st_mtime for o in objs)
+    if not LIB.exists() or LIB.stat().st_mtime < newest:
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="--verbose-ptxas" in sys.argv))

@@ -1,0 +1,760 @@
+// dspw_capi.cu -- the C ABI of include/dspw.h: handle lifetime, validation,
+// device buffers, per-problem tables, the per-step CUDA graph and the
+// host<->device copies.  All arithmetic runs in the kernels of
+// dspw_kernels.cuh (instantiated by dspw_fp64.cu / dspw_fp32.cu).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dspw_launch.h"
+
+using namespace dspw;
+
+namespace dspw {
+
+// -------------------------------------------------------- step control kernels
+
+__global__ void k_begin_step_wrap(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nprob) return;
+  const ProbDev& P = prob[p];
+  ProbState& S = st[p];
+  if (!(S.time < P.final_time && S.iter < P.max_iter)) {
+    S.active = 0;
+    S.dt = 0.0;
+    S.factor = 0.0;
+    return;
+  }
+  atomicAdd(nactive, 1);
+  S.active = 1;
+  double dt;
+  if (fixed_dt > 0) {
+    dt = fixed_dt;
+  } else {
+    double smax = __longlong_as_double((long long)S.smax);
+    dt = 1.0e20;
+    double c = P.hmin / smax;
+    if (c < dt) dt = c;
+    dt *= P.cfl;
+  }
+  if (S.time + dt > S.t_save) dt = S.t_save - S.time;
+  S.dt = dt;
+  S.factor = dt / (P.dx * P.dy * P.dz);
+  S.smax = 0ull;
+  S.ent_acc = 0.0;
+}
+
+cudaError_t launch_begin_step(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive,
+                              cudaStream_t s) {
+  k_begin_step_wrap<<<(nprob + 127) / 128, 128, 0, s>>>(prob, st, nprob, fixed_dt, nactive);
+  return cudaGetLastError();
+}
+
+// time += dt, ++iter, advance the time stamp (enflo/src/fv.cc:1285-1312), and
+// the discrete entropy inequality bookkeeping.
+__global__ void k_end_step(const ProbDev* prob, ProbState* st, int nprob) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nprob) return;
+  ProbState& S = st[p];
+  if (!S.active) return;
+  S.time += S.dt;
+  S.iter += 1;
+  if (S.time == S.t_save) S.t_save += prob[p].t_interval;
+  S.ent_prev = S.ent;
+  S.ent = S.ent_acc * prob[p].vol;
+  double rise = (S.ent - S.ent_prev) / fabs(S.ent_prev);
+  if (rise > S.ent_max_rise) S.ent_max_rise = rise;
+}
+
+
+cudaError_t launch_end_step(const ProbDev* prob, ProbState* st, int nprob, cudaStream_t s) {
+  k_end_step<<<(nprob + 127) / 128, 128, 0, s>>>(prob, st, nprob);
+  return cudaGetLastError();
+}
+
+__global__ void k_init_state(const ProbDev* prob, ProbState* st, int p) {
+  ProbState& S = st[p];
+  S.ent = S.ent_acc * prob[p].vol;
+  S.ent_prev = S.ent;
+  S.ent_acc = 0.0;
+  S.ent_max_rise = -1e300;
+}
+
+cudaError_t launch_init_state(const ProbDev* prob, ProbState* st, int p, cudaStream_t s) {
+  k_init_state<<<1, 1, 0, s>>>(prob, st, p);
+  return cudaGetLastError();
+}
+
+}  // namespace dspw
+
+// ------------------------------------------------------------------ handle --
+
+struct dspw_handle {
+  int nprob = 0;
+  int precision = 0;
+  int nrk = 3;
+  int time_scheme = 1;
+  int has_ns = 0;
+  int maxdim = 1;
+  std::vector<dspw_desc> desc;
+  std::vector<ProbDev> hprob;
+  std::vector<long long> cell_start;   // nprob + 1
+  std::vector<int> task_start[3];
+  long long ctot = 0;
+  long long maxcells = 0;
+  ProbDev* dprob = nullptr;
+  ProbState* dst = nullptr;
+  StatusDev* dstatus = nullptr;
+  NetParams* dnet = nullptr;
+  int* dtask[3] = {nullptr, nullptr, nullptr};
+  long long* dcell_start = nullptr;
+  int* dnactive = nullptr;
+  void* Un = nullptr;
+  void* Ua = nullptr;
+  void* Ub = nullptr;
+  void* R = nullptr;
+  void* V = nullptr;
+  void* node = nullptr;
+  double* dstage = nullptr;
+  double* dscratch = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = -1.0;
+  // profiling: when set, an event is recorded after every launch
+  std::vector<cudaEvent_t>* prof_ev = nullptr;
+  std::vector<std::string>* prof_names = nullptr;
+  int last_error = 0;
+  size_t elem = 8;
+};
+
+namespace {
+
+#define CK(x)                                  \
+  do {                                         \
+    cudaError_t e__ = (x);                     \
+    if (e__ != cudaSuccess) {                  \
+      h->last_error = DSPW_ERR_CUDA;           \
+      return DSPW_ERR_CUDA;                    \
+    }                                          \
+  } while (0)
+
+void prof_mark(dspw_handle* h, const char* name) {
+  if (!h->prof_ev) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, h->stream);
+  h->prof_ev->push_back(e);
+  h->prof_names->push_back(name);
+}
+
+int problem_dim(const dspw_desc& d) {
+  if (d.nz > 1) return 3;
+  if (d.ny > 1) return 2;
+  return 1;
+}
+
+int validate(const dspw_desc& d) {
+  if (d.abi_version != DSPW_ABI_VERSION) return DSPW_ERR_ARG;
+  if (d.model < 0 || d.model > 4) return DSPW_ERR_ARG;
+  if (d.model == DSPW_NS_KEP) return DSPW_ERR_UNSUPPORTED;
+  if (d.nx < 1 || d.ny < 1 || d.nz < 1) return DSPW_ERR_ARG;
+  int dim = problem_dim(d);
+  int N[3] = {d.nx, d.ny, d.nz};
+  for (int k = 0; k < dim; k++)
+    if (N[k] < 2) return DSPW_ERR_UNSUPPORTED;   // a swept direction needs >= 2 cells
+  if (!(d.xmax > d.xmin) || !(d.ymax > d.ymin) || !(d.zmax > d.zmin)) return DSPW_ERR_ARG;
+  if (d.precision != DSPW_FP64 && d.precision != DSPW_FP32_BF16) return DSPW_ERR_ARG;
+  if (d.time_scheme != DSPW_SSPRK3 && d.time_scheme != DSPW_RK1) return DSPW_ERR_UNSUPPORTED;
+  if (d.recon < DSPW_REC_SP_WENO || d.recon > DSPW_REC_SP_WENO_DL) return DSPW_ERR_UNSUPPORTED;
+  bool scalar = d.model <= DSPW_BURGERS;
+  if (scalar) {
+    if (d.model == DSPW_LINADV && !(d.flux >= DSPW_LIN_EC && d.flux <= DSPW_LIN_TECNO4)) return DSPW_ERR_ARG;
+    if (d.model == DSPW_BURGERS && !(d.flux >= DSPW_BUR_EC && d.flux <= DSPW_BUR_TECNO4)) return DSPW_ERR_ARG;
+  } else {
+    switch (d.flux) {
+      case DSPW_KEPEC: case DSPW_KEPEC4: case DSPW_KEP: case DSPW_KEP4: case DSPW_ROE_EC: case DSPW_ROE_EC4:
+      case DSPW_KEP_TECNO_ROE: case DSPW_KEPES_TECNO_ROE: case DSPW_KEPES_TECNO_RUSANOV:
+      case DSPW_ROE_TECNO_ROE: case DSPW_KEPES_TECNO4_ROE: case DSPW_KEPES_TECNO4_RUSANOV:
+      case DSPW_ROE_TECNO4_ROE: break;
+      default: return DSPW_ERR_UNSUPPORTED;
+    }
+    if (!(d.gamma > 1.0) || !(d.gas_const > 0.0)) return DSPW_ERR_ARG;
+    if (d.model == DSPW_NS_ES) {
+      if (dim != 3) return DSPW_ERR_UNSUPPORTED;
+      for (int f = 0; f < 6; f++)
+        if (d.bc[f] != DSPW_BC_PERIODIC) return DSPW_ERR_UNSUPPORTED;   // enflo/src/parameter.cc:564-568
+      if (!(d.mu_ref > 0.0) || !(d.prandtl > 0.0)) return DSPW_ERR_ARG;
+    }
+  }
+  for (int f = 0; f < 6; f++)
+    if (d.bc[f] < 0 || d.bc[f] > 3) return DSPW_ERR_ARG;
+  for (int a = 0; a < 3; a++)   // periodic must pair with periodic (enflo/src/parameter.cc:570-581)
+    if ((d.bc[2 * a] == DSPW_BC_PERIODIC) != (d.bc[2 * a + 1] == DSPW_BC_PERIODIC)) return DSPW_ERR_ARG;
+  if (!(d.cfl > 0.0) || !(d.final_time >= 0.0) || d.max_iter < 1 || d.t_stamps < 1) return DSPW_ERR_ARG;
+  return DSPW_OK;
+}
+
+ProbDev make_prob(const dspw_desc& d, long long off) {
+  ProbDev P;
+  memset(&P, 0, sizeof(P));
+  P.model = d.model;
+  P.flux = d.flux;
+  P.recon = d.recon;
+  P.dim = problem_dim(d);
+  P.is_scalar = d.model <= DSPW_BURGERS;
+  P.nv = P.is_scalar ? 1 : P.dim + 2;
+  P.nrk = d.time_scheme == DSPW_RK1 ? 1 : 3;
+  P.nx = d.nx; P.ny = d.ny; P.nz = d.nz;
+  for (int f = 0; f < 6; f++) P.bc[f] = d.bc[f];
+  P.ec1 = d.ec1_fix;
+  P.mu_model = d.mu_model;
+  P.max_iter = d.max_iter;
+  P.off = off;
+  P.dx = (d.xmax - d.xmin) / d.nx;   // enflo/src/fv.cc:29-31
+  P.dy = (d.ymax - d.ymin) / d.ny;
+  P.dz = (d.zmax - d.zmin) / d.nz;
+  P.hmin = std::min(P.dx, std::min(P.dy, P.dz));
+  P.vol = P.dx * P.dy * P.dz;
+  P.area[0] = P.dy * P.dz;           // num_flux face areas (enflo/src/kepec.cc:38-44)
+  P.area[1] = P.dx * P.dz;
+  P.area[2] = P.dx * P.dy;
+  for (int k = 0; k < 3; k++) P.rarea[k] = 1 / P.area[k];
+  P.gamma = d.gamma; P.gas_const = d.gas_const; P.prandtl = d.prandtl;
+  P.mu_ref = d.mu_ref; P.T_ref = d.T_ref; P.T_0 = d.T_0; P.omega = d.omega;
+  P.Cp = d.gamma * d.gas_const / (d.gamma - 1.0);
+  for (int k = 0; k < 3; k++) P.lin_vel[k] = d.lin_vel[k];
+  P.lin_speed = std::sqrt(d.lin_vel[0] * d.lin_vel[0] + d.lin_vel[1] * d.lin_vel[1] + d.lin_vel[2] * d.lin_vel[2]);
+  for (int k = 0; k < 3; k++) {
+    double n[3] = {0, 0, 0};
+    n[k] = 1;
+    P.lin_vn[k] = n[0] * d.lin_vel[0] + n[1] * d.lin_vel[1] + n[2] * d.lin_vel[2];
+  }
+  P.cfl = d.cfl;
+  P.final_time = d.final_time;
+  P.t_interval = d.final_time / d.t_stamps;
+  for (int f = 0; f < 6; f++)
+    for (int c = 0; c < 5; c++) P.bc_state[f][c] = d.bc_state[f][c];
+  // flux structure
+  P.central = 0; P.fourth = 0; P.tecno = 0; P.rusanov = 0;
+  switch (d.flux) {
+    case DSPW_LIN_EC4: case DSPW_BUR_EC4: P.fourth = 1; break;
+    case DSPW_LIN_TECNO: case DSPW_BUR_TECNO: P.tecno = 1; break;
+    case DSPW_LIN_TECNO4: case DSPW_BUR_TECNO4: P.tecno = 1; P.fourth = 1; break;
+    case DSPW_KEPEC: break;
+    case DSPW_KEPEC4: P.fourth = 1; break;
+    case DSPW_KEP: P.central = 1; break;
+    case DSPW_KEP4: P.central = 1; P.fourth = 1; break;
+    case DSPW_ROE_EC: P.central = 2; break;
+    case DSPW_ROE_EC4: P.central = 2; P.fourth = 1; break;
+    case DSPW_KEP_TECNO_ROE: P.central = 1; P.tecno = 1; P.ec1 = 0; break;   // no EC1_fix (kep_tecno_roe.cc)
+    case DSPW_KEPES_TECNO_ROE: P.tecno = 1; break;
+    case DSPW_KEPES_TECNO_RUSANOV: P.tecno = 1; P.rusanov = 1; P.ec1 = 0; break;
+    case DSPW_ROE_TECNO_ROE: P.central = 2; P.tecno = 1; break;
+    case DSPW_KEPES_TECNO4_ROE: P.tecno = 1; P.fourth = 1; break;
+    case DSPW_KEPES_TECNO4_RUSANOV: P.tecno = 1; P.fourth = 1; P.rusanov = 1; P.ec1 = 0; break;
+    case DSPW_ROE_TECNO4_ROE: P.central = 2; P.tecno = 1; P.fourth = 1; break;
+    default: break;
+  }
+  P.spw_corr = d.recon == DSPW_REC_SP_WENO_DL ? -1 : (d.recon == DSPW_REC_SP_WENOC ? 1 : (d.recon == DSPW_REC_SP_WENO_CORR2 ? 2 : 0));
+  return P;
+}
+
+int tasks_for(const ProbDev& P, int dir) {
+  if (dir >= P.dim) return 0;
+  int N[3] = {P.nx, P.ny, P.nz};
+  long long nseg = (N[dir] + SEG_CELLS - 1) / SEG_CELLS;
+  long long other = (long long)P.nx * P.ny * P.nz / N[dir];
+  return (int)(nseg * other);
+}
+
+void* buf(dspw_handle* h, int which) {
+  switch (which) {
+    case 0: return h->Un;
+    case 1: return h->Ua;
+    default: return h->Ub;
+  }
+}
+
+template <typename T>
+int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
+  SweepArgs<T> a;
+  memset(&a, 0, sizeof(a));
+  a.prob = h->dprob;
+  a.st = h->dst;
+  a.nprob = h->nprob;
+  // SSPRK3 ping-pong: U^n -> Ua -> Ub -> U^n (the last stage writes in place:
+  // every cell reads its own U^n entry before overwriting it)
+  int in, out;
+  if (h->nrk == 1) { in = 0; out = 1; }
+  else { in = rk == 0 ? 0 : (rk == 1 ? 1 : 2); out = rk == 0 ? 1 : (rk == 1 ? 2 : 0); }
+  if (residual_only) { in = 0; out = 1; }
+  a.Uin = (const T*)buf(h, in);
+  a.Un = (const T*)h->Un;
+  a.Uout = (T*)buf(h, out);
+  a.R = (T*)h->R;
+  a.ctot = h->ctot;
+  a.rk = rk;
+  static const double ark[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};   // enflo/src/ext_constants.h:7-8
+  static const double brk[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+  a.a_rk = ark[rk];
+  a.b_rk = brk[rk];
+  a.final_stage = (rk == h->nrk - 1) && !residual_only;
+  a.residual_only = residual_only;
+  a.status = h->dstatus;
+  a.net = h->dnet;
+  if (h->has_ns) {
+    CK(Launch<T>::entvars(h->dprob, h->nprob, h->dcell_start, h->ctot, a.Uin, h->ctot, (T*)h->V, h->stream));
+    prof_mark(h, "entvars");
+    CK(Launch<T>::visc_nodes(h->dprob, h->nprob, h->dcell_start, h->ctot, (const T*)h->V, h->ctot, (T*)h->node,
+                             h->stream));
+    prof_mark(h, "visc_nodes");
+  }
+  for (int dir = 0; dir < h->maxdim; dir++) {
+    int nt = h->task_start[dir][h->nprob];
+    if (nt == 0) continue;
+    a.task_start = h->dtask[dir];
+    a.ntask = nt;
+    a.viscous = 0;
+    // NS problems never update in a sweep; mixed batches are not formed with NS
+    if (h->has_ns) a.viscous = 1;
+    int grid = (nt + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+    CK(Launch<T>::sweep(dir, a, grid, h->stream));
+    prof_mark(h, dir == 0 ? "sweep_x" : (dir == 1 ? "sweep_y" : "sweep_z"));
+  }
+  if (h->has_ns) {
+    CK(Launch<T>::visc_update(a, h->dcell_start, h->ctot, (const T*)h->node, h->stream));
+    prof_mark(h, "visc_update");
+  }
+  if (h->nrk == 1 && !residual_only)
+    CK(cudaMemcpyAsync(h->Un, h->Ua, h->elem * h->ctot * 5, cudaMemcpyDeviceToDevice, h->stream));
+  return DSPW_OK;
+}
+
+int enqueue_stage_any(dspw_handle* h, int rk, int residual_only) {
+  return h->precision == DSPW_FP64 ? enqueue_stage<double>(h, rk, residual_only)
+                                   : enqueue_stage<float>(h, rk, residual_only);
+}
+
+int enqueue_step(dspw_handle* h, double fixed_dt) {
+  CK(cudaMemsetAsync(h->dnactive, 0, sizeof(int), h->stream));
+  CK(launch_begin_step(h->dprob, h->dst, h->nprob, fixed_dt, h->dnactive, h->stream));
+  prof_mark(h, "begin_step");
+  for (int rk = 0; rk < h->nrk; rk++) {
+    int r = enqueue_stage_any(h, rk, 0);
+    if (r) return r;
+  }
+  CK(launch_end_step(h->dprob, h->dst, h->nprob, h->stream));
+  prof_mark(h, "end_step");
+  return DSPW_OK;
+}
+
+int build_graph(dspw_handle* h, double fixed_dt) {
+  if (h->graph && h->graph_dt == fixed_dt) return DSPW_OK;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int r = enqueue_step(h, fixed_dt);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (r) return r;
+  if (e != cudaSuccess) { h->last_error = DSPW_ERR_CUDA; return DSPW_ERR_CUDA; }
+  e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { h->graph = nullptr; h->last_error = DSPW_ERR_CUDA; return DSPW_ERR_CUDA; }
+  h->graph_dt = fixed_dt;
+  return DSPW_OK;
+}
+
+long long ncells(const dspw_desc& d) { return (long long)d.nx * d.ny * d.nz; }
+
+int check_p(dspw_handle* h, int p) { return (!h || p < 0 || p >= h->nprob) ? DSPW_ERR_ARG : DSPW_OK; }
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI --
+
+extern "C" {
+
+const char* dspw_error_string(int code) {
+  switch (code) {
+    case DSPW_OK: return "DSPW_OK";
+    case DSPW_ERR_ARG: return "DSPW_ERR_ARG: bad argument or descriptor";
+    case DSPW_ERR_CUDA: return "DSPW_ERR_CUDA: a CUDA runtime call failed";
+    case DSPW_ERR_NONFINITE: return "DSPW_ERR_NONFINITE: NaN or Inf in the state";
+    case DSPW_ERR_NONPOSITIVE: return "DSPW_ERR_NONPOSITIVE: density or pressure <= 0";
+    case DSPW_ERR_TIMEOUT: return "DSPW_ERR_TIMEOUT: a bounded device wait gave up";
+    case DSPW_ERR_UNSUPPORTED: return "DSPW_ERR_UNSUPPORTED: combination not implemented";
+    case DSPW_ERR_NOMEM: return "DSPW_ERR_NOMEM: device allocation failed";
+    case DSPW_ERR_FINISHED: return "DSPW_ERR_FINISHED: problem reached final_time or max_iter";
+    default: return "unknown dspw status";
+  }
+}
+
+int dspw_version(void) { return DSPW_ABI_VERSION; }
+
+int dspw_create(const dspw_desc* desc, dspw_handle** out) { return dspw_create_batch(desc, 1, out); }
+
+int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
+  if (!descs || !out || nprob < 1) return DSPW_ERR_ARG;
+  *out = nullptr;
+  for (int p = 0; p < nprob; p++) {
+    int r = validate(descs[p]);
+    if (r) return r;
+    if (descs[p].precision != descs[0].precision || descs[p].time_scheme != descs[0].time_scheme) return DSPW_ERR_ARG;
+  }
+  dspw_handle* h = new dspw_handle;
+  h->nprob = nprob;
+  h->precision = descs[0].precision;
+  h->time_scheme = descs[0].time_scheme;
+  h->nrk = h->time_scheme == DSPW_RK1 ? 1 : 3;
+  h->elem = h->precision == DSPW_FP64 ? 8 : 4;
+  h->desc.assign(descs, descs + nprob);
+  long long off = 0;
+  h->cell_start.push_back(0);
+  for (int p = 0; p < nprob; p++) {
+    h->hprob.push_back(make_prob(descs[p], off));
+    off += ncells(descs[p]);
+    h->cell_start.push_back(off);
+    h->maxcells = std::max(h->maxcells, ncells(descs[p]));
+    h->maxdim = std::max(h->maxdim, h->hprob.back().dim);
+    if (descs[p].model == DSPW_NS_ES) h->has_ns = 1;
+  }
+  if (h->has_ns) {
+    for (int p = 0; p < nprob; p++)
+      if (descs[p].model != DSPW_NS_ES) { delete h; return DSPW_ERR_UNSUPPORTED; }
+  }
+  h->ctot = off;
+  for (int dir = 0; dir < 3; dir++) {
+    h->task_start[dir].push_back(0);
+    for (int p = 0; p < nprob; p++) {
+      long long nt = (long long)h->task_start[dir].back() + tasks_for(h->hprob[p], dir);
+      if (nt > (1LL << 30)) { delete h; return DSPW_ERR_ARG; }
+      h->task_start[dir].push_back((int)nt);
+    }
+  }
+  // network parameters (shared by the batch; taken from the first DL problem)
+  NetParams np;
+  memset(&np, 0, sizeof(np));
+  const dspw_desc* dnet = &descs[0];
+  for (int p = 0; p < nprob; p++)
+    if (descs[p].recon == DSPW_REC_SP_WENO_DL) { dnet = &descs[p]; break; }
+  for (int l = 0; l < 4; l++)
+    for (int j = 0; j < 5; j++) {
+      np.b[l][j] = dnet->nn_b[l][j];
+      np.bf[l][j] = (float)dnet->nn_b[l][j];
+      for (int k = 0; k < 5; k++) {
+        np.w[l][j][k] = dnet->nn_w[l][j][k];
+        np.wf[l][j][k] = (float)dnet->nn_w[l][j][k];
+      }
+    }
+  // reserved_d[0..4] / [5..7] + reserved_i[0]: optional training box of the network inputs
+  np.use_box = dnet->reserved_i[0];
+  for (int k = 0; k < 5; k++) { np.feat_lo[k] = -1e30f; np.feat_hi[k] = 1e30f; }
+  if (np.use_box) {
+    for (int k = 0; k < 5; k++) np.feat_hi[k] = (float)dnet->reserved_d[k];
+    for (int k = 0; k < 2; k++) np.feat_lo[k] = -1.0f;
+    for (int k = 2; k < 5; k++) np.feat_lo[k] = 0.0f;
+  }
+  int ret = DSPW_OK;
+#define CKC(x)                                   \
+  do {                                           \
+    if ((x) != cudaSuccess) {                    \
+      ret = DSPW_ERR_NOMEM;                      \
+      goto fail;                                 \
+    }                                            \
+  } while (0)
+  {
+    size_t state_bytes = (size_t)h->elem * (size_t)std::max<long long>(h->ctot, 1) * 5;
+    CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CKC(h->precision == DSPW_FP64 ? Launch<double>::prepare() : Launch<float>::prepare());
+    CKC(cudaMalloc(&h->dprob, sizeof(ProbDev) * nprob));
+    CKC(cudaMalloc(&h->dst, sizeof(ProbState) * nprob));
+    CKC(cudaMalloc(&h->dstatus, sizeof(StatusDev)));
+    CKC(cudaMalloc(&h->dnet, sizeof(NetParams)));
+    CKC(cudaMalloc(&h->dcell_start, sizeof(long long) * (nprob + 1)));
+    CKC(cudaMalloc(&h->dnactive, sizeof(int)));
+    for (int dir = 0; dir < 3; dir++) CKC(cudaMalloc(&h->dtask[dir], sizeof(int) * (nprob + 1)));
+    CKC(cudaMalloc(&h->Un, state_bytes));
+    CKC(cudaMalloc(&h->Ua, state_bytes));
+    CKC(cudaMalloc(&h->Ub, state_bytes));
+    CKC(cudaMalloc(&h->R, state_bytes));
+    if (h->has_ns) {
+      CKC(cudaMalloc(&h->V, state_bytes));
+      CKC(cudaMalloc(&h->node, state_bytes * 3));
+    }
+    CKC(cudaMalloc(&h->dstage, sizeof(double) * 5 * (size_t)std::max<long long>(h->maxcells, 1)));
+    CKC(cudaMalloc(&h->dscratch, sizeof(double) * 16));
+    CKC(cudaMemcpy(h->dprob, h->hprob.data(), sizeof(ProbDev) * nprob, cudaMemcpyHostToDevice));
+    CKC(cudaMemset(h->dst, 0, sizeof(ProbState) * nprob));
+    CKC(cudaMemset(h->dstatus, 0, sizeof(StatusDev)));
+    CKC(cudaMemcpy(h->dnet, &np, sizeof(NetParams), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(h->dcell_start, h->cell_start.data(), sizeof(long long) * (nprob + 1), cudaMemcpyHostToDevice));
+    for (int dir = 0; dir < 3; dir++)
+      CKC(cudaMemcpy(h->dtask[dir], h->task_start[dir].data(), sizeof(int) * (nprob + 1), cudaMemcpyHostToDevice));
+    CKC(cudaMemset(h->Un, 0, state_bytes));
+    CKC(cudaMemset(h->Ua, 0, state_bytes));
+    CKC(cudaMemset(h->Ub, 0, state_bytes));
+    CKC(cudaMemset(h->R, 0, state_bytes));
+    // problems start finished until their state is uploaded
+    std::vector<ProbState> hs(nprob);
+    memset(hs.data(), 0, sizeof(ProbState) * nprob);
+    for (int p = 0; p < nprob; p++) {
+      hs[p].time = h->hprob[p].final_time;
+      hs[p].iter = h->hprob[p].max_iter;
+    }
+    CKC(cudaMemcpy(h->dst, hs.data(), sizeof(ProbState) * nprob, cudaMemcpyHostToDevice));
+  }
+  *out = h;
+  return DSPW_OK;
+fail:
+  dspw_destroy(h);
+  return ret;
+#undef CKC
+}
+
+int dspw_destroy(dspw_handle* h) {
+  if (!h) return DSPW_ERR_ARG;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive, h->dtask[0], h->dtask[1],
+                  h->dtask[2], h->Un, h->Ua, h->Ub, h->R, h->V, h->node, h->dstage, h->dscratch};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return DSPW_OK;
+}
+
+int dspw_upload_prim(dspw_handle* h, int p, const double* prim) {
+  if (check_p(h, p) || !prim) return DSPW_ERR_ARG;
+  const dspw_desc& d = h->desc[p];
+  long long n = ncells(d);
+  int nv = d.model <= DSPW_BURGERS ? 1 : 5;
+  // positivity of the initial state (enflo/src/fv.cc:88-89 asserts it)
+  if (nv == 5)
+    for (long long c = 0; c < n; c++)
+      if (!(prim[c] > 0.0) || !(prim[4 * n + c] > 0.0)) return DSPW_ERR_NONPOSITIVE;
+  for (long long c = 0; c < n * nv; c++)
+    if (!std::isfinite(prim[c])) return DSPW_ERR_NONFINITE;
+  CK(cudaMemcpyAsync(h->dstage, prim, sizeof(double) * nv * n, cudaMemcpyHostToDevice, h->stream));
+  ProbState s;
+  memset(&s, 0, sizeof(s));
+  s.time = 0.0;
+  s.iter = 0;
+  s.t_save = h->hprob[p].t_interval;
+  s.active = 1;
+  CK(cudaMemcpyAsync(h->dst + p, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+  if (h->precision == DSPW_FP64)
+    CK(Launch<double>::upload(h->dprob, h->dst, p, h->dstage, (double*)h->Un, h->ctot, n, h->stream));
+  else
+    CK(Launch<float>::upload(h->dprob, h->dst, p, h->dstage, (float*)h->Un, h->ctot, n, h->stream));
+  CK(launch_init_state(h->dprob, h->dst, p, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DSPW_OK;
+}
+
+static int download(dspw_handle* h, int p, double* out, int prim, void* src) {
+  if (check_p(h, p) || !out) return DSPW_ERR_ARG;
+  const dspw_desc& d = h->desc[p];
+  long long n = ncells(d);
+  int nv = d.model <= DSPW_BURGERS ? 1 : 5;
+  if (h->precision == DSPW_FP64)
+    CK(Launch<double>::download(h->dprob, p, (const double*)src, h->ctot, n, h->dstage, prim, h->stream));
+  else
+    CK(Launch<float>::download(h->dprob, p, (const float*)src, h->ctot, n, h->dstage, prim, h->stream));
+  CK(cudaMemcpyAsync(out, h->dstage, sizeof(double) * nv * n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DSPW_OK;
+}
+
+int dspw_download_prim(dspw_handle* h, int p, double* prim) { return download(h, p, prim, 1, h ? h->Un : nullptr); }
+int dspw_download_cons(dspw_handle* h, int p, double* cons) { return download(h, p, cons, 0, h ? h->Un : nullptr); }
+
+int dspw_compute_dt(dspw_handle* h, int p, double* dt) {
+  if (check_p(h, p) || !dt) return DSPW_ERR_ARG;
+  long long n = ncells(h->desc[p]);
+  CK(cudaMemsetAsync(h->dscratch, 0, sizeof(double), h->stream));
+  if (h->precision == DSPW_FP64)
+    CK(Launch<double>::speed(h->dprob, h->dst, p, (const double*)h->Un, h->ctot, n, h->dscratch, h->stream));
+  else
+    CK(Launch<float>::speed(h->dprob, h->dst, p, (const float*)h->Un, h->ctot, n, h->dscratch, h->stream));
+  double smax = 0;
+  CK(cudaMemcpyAsync(&smax, h->dscratch, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const ProbDev& P = h->hprob[p];
+  double v = 1.0e20;   // enflo/src/fv.cc:366-383
+  double c = P.hmin / smax;
+  if (c < v) v = c;
+  *dt = v * P.cfl;
+  return DSPW_OK;
+}
+
+int dspw_residual(dspw_handle* h, int p, double* res) {
+  if (check_p(h, p) || !res) return DSPW_ERR_ARG;
+  int r = enqueue_stage_any(h, 0, 1);
+  if (r) return r;
+  return download(h, p, res, 0, h->R);
+}
+
+int dspw_stage(dspw_handle* h, int rk, double dt) {
+  if (!h || rk < 0 || rk >= h->nrk) return DSPW_ERR_ARG;
+  if (rk == 0) {
+    CK(cudaMemsetAsync(h->dnactive, 0, sizeof(int), h->stream));
+    CK(launch_begin_step(h->dprob, h->dst, h->nprob, dt, h->dnactive, h->stream));
+  }
+  int r = enqueue_stage_any(h, rk, 0);
+  if (r) return r;
+  if (rk == h->nrk - 1) CK(launch_end_step(h->dprob, h->dst, h->nprob, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DSPW_OK;
+}
+
+int dspw_step(dspw_handle* h, int nsteps, double fixed_dt) {
+  if (!h || nsteps < 0) return DSPW_ERR_ARG;
+  int r = build_graph(h, fixed_dt > 0 ? fixed_dt : 0.0);
+  if (r) return r;
+  for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(h->graph, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DSPW_OK;
+}
+
+int dspw_run(dspw_handle* h, int chunk, int* steps) {
+  if (!h || chunk < 1) return DSPW_ERR_ARG;
+  int r = build_graph(h, 0.0);
+  if (r) return r;
+  // bounded by the largest max_iter of the batch; a health error ends the run
+  long long limit = 0;
+  for (auto& d : h->desc) limit = std::max<long long>(limit, d.max_iter);
+  long long total = 0;
+  int status = DSPW_OK;
+  for (;;) {
+    for (int s = 0; s < chunk; s++) CK(cudaGraphLaunch(h->graph, h->stream));
+    total += chunk;
+    int nact = 0;
+    StatusDev sd;
+    CK(cudaMemcpyAsync(&nact, h->dnactive, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&sd, h->dstatus, sizeof(sd), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (sd.code) { status = sd.code; break; }
+    if (nact == 0 || total > limit) break;
+  }
+  // exact count of steps of the longest problem
+  std::vector<ProbState> hs(h->nprob);
+  CK(cudaMemcpy(hs.data(), h->dst, sizeof(ProbState) * h->nprob, cudaMemcpyDeviceToHost));
+  int mx = 0;
+  for (auto& s : hs) mx = std::max(mx, s.iter);
+  if (steps) *steps = mx;
+  return status;
+}
+
+int dspw_globals(dspw_handle* h, int p, dspw_globals_out* g) {
+  if (check_p(h, p) || !g) return DSPW_ERR_ARG;
+  long long n = ncells(h->desc[p]);
+  CK(cudaMemsetAsync(h->dscratch, 0, sizeof(double) * 8, h->stream));
+  if (h->precision == DSPW_FP64)
+    CK(Launch<double>::globals(h->dprob, p, (const double*)h->Un, h->ctot, n, h->dscratch, h->stream));
+  else
+    CK(Launch<float>::globals(h->dprob, p, (const float*)h->Un, h->ctot, n, h->dscratch, h->stream));
+  double acc[8];
+  ProbState s;
+  CK(cudaMemcpyAsync(acc, h->dscratch, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(&s, h->dst + p, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const ProbDev& P = h->hprob[p];
+  g->time = s.time;
+  g->dt = s.dt;
+  g->iter = s.iter;
+  g->finished = !(s.time < P.final_time && s.iter < P.max_iter);
+  g->total_entropy = acc[0] * P.vol;
+  g->kinetic_energy = acc[1] * P.vol;
+  for (int v = 0; v < 5; v++) g->conserved[v] = acc[2 + v] * P.vol;
+  return DSPW_OK;
+}
+
+int dspw_last_status(dspw_handle* h, dspw_status_out* s) {
+  if (!h || !s) return DSPW_ERR_ARG;
+  StatusDev d;
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(&d, h->dstatus, sizeof(d), cudaMemcpyDeviceToHost));
+  CK(cudaMemset(h->dstatus, 0, sizeof(d)));
+  s->code = d.code ? d.code : h->last_error;
+  s->nonfinite_cells = (long long)d.nonfinite;
+  s->nonpositive_cells = (long long)d.nonpositive;
+  s->sign_violations = (long long)d.sign_viol;
+  s->faces_checked = (long long)d.faces_checked;
+  h->last_error = 0;
+  return DSPW_OK;
+}
+
+int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, double err[3]) {
+  if (check_p(h, p) || !exact || !err || comp < 0 || comp > 4) return DSPW_ERR_ARG;
+  long long n = ncells(h->desc[p]);
+  CK(cudaMemcpyAsync(h->dstage, exact, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(h->dscratch, 0, sizeof(double) * 3, h->stream));
+  if (h->precision == DSPW_FP64)
+    CK(Launch<double>::errors(h->dprob, p, (const double*)h->Un, h->ctot, n, comp, h->dstage, h->dscratch, h->stream));
+  else
+    CK(Launch<float>::errors(h->dprob, p, (const float*)h->Un, h->ctot, n, comp, h->dstage, h->dscratch, h->stream));
+  double acc[3];
+  CK(cudaMemcpyAsync(acc, h->dscratch, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const ProbDev& P = h->hprob[p];
+  err[0] = acc[0] * (P.dx * P.dy * P.dz);   // enflo_scalar/src_scalar/compute_errors.cc:26-29
+  err[1] = std::sqrt(acc[1] * (P.dx * P.dy * P.dz));
+  err[2] = acc[2];
+  return DSPW_OK;
+}
+
+int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k, int* nk) {
+  if (!h || !kernel_ms || max_k < 1) return DSPW_ERR_ARG;
+  std::vector<cudaEvent_t> ev;
+  std::vector<std::string> nm;
+  cudaEvent_t e0;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventRecord(e0, h->stream));
+  h->prof_ev = &ev;
+  h->prof_names = &nm;
+  int r = enqueue_step(h, 0.0);
+  h->prof_ev = nullptr;
+  h->prof_names = nullptr;
+  CK(cudaStreamSynchronize(h->stream));
+  int n = 0;
+  cudaEvent_t prev = e0;
+  for (size_t i = 0; i < ev.size(); i++) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, prev, ev[i]);
+    if (n < max_k) {
+      kernel_ms[n] = ms;
+      if (names) {
+        memset(names + 16 * n, 0, 16);
+        strncpy(names + 16 * n, nm[i].c_str(), 15);
+      }
+      n++;
+    }
+    prev = ev[i];
+  }
+  for (auto e : ev) cudaEventDestroy(e);
+  cudaEventDestroy(e0);
+  if (nk) *nk = n;
+  return r;
+}
+
+int dspw_sync(dspw_handle* h) {
+  if (!h) return DSPW_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  return h->last_error;
+}
+
+void* dspw_stream(dspw_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int dspw_device_state(dspw_handle* h, int p, void** ptr, long long* stride, int* elem_bytes) {
+  if (check_p(h, p) || !ptr) return DSPW_ERR_ARG;
+  *ptr = (char*)h->Un + h->elem * h->hprob[p].off;
+  if (stride) *stride = h->ctot;
+  if (elem_bytes) *elem_bytes = (int)h->elem;
+  return DSPW_OK;
+}
+
+}  // extern "C"

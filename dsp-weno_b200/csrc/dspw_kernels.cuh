@@ -1,0 +1,1212 @@
+// dspw_kernels.cuh -- device data structures and the stage kernels.
+//
+// Work decomposition.  A stage is one sweep kernel per active direction.  The
+// unit of work is a warp task: one line segment of SEG_CELLS cells along the
+// sweep direction of one problem.  A warp stages the SEG_CELLS + 4 cells it
+// needs (2 ghost/halo cells per side) in shared memory, converts them to
+// primitive and entropy variables once, evaluates the SEG_CELLS + 1 faces (one
+// lane per face, the wide 4th-order two-point fluxes shared between
+// neighbouring faces), and then either accumulates the residual of its cells
+// (non-final sweep) or applies the SSPRK stage update (final sweep).  Warps of
+// a block are independent (only __syncwarp), so problems of any size and mix
+// share one launch: the global task index is mapped to (problem, line,
+// segment) through per-problem prefix sums.
+//
+// Cell data in HBM: structure-of-arrays planes U[c * ctot + cell], cells of
+// problem p at [off_p, off_p + nx*ny*nz) with x fastest.  Euler problems store
+// dim+2 components (rho, rho u[, rho v[, rho w]], E): the momentum components
+// of inactive directions are identically zero in the reference and are not
+// stored.
+#pragma once
+#include "dspw_math.cuh"
+#include "../../include/dspw.h"
+
+namespace dspw {
+
+constexpr int SEG_CELLS = 30;               // cells per warp task
+constexpr int SEG_FACES = SEG_CELLS + 1;    // faces per warp task (lanes 0..30)
+constexpr int SEG_LOAD = SEG_CELLS + 4;     // staged cells per warp task
+constexpr int WARPS_PER_BLOCK = 8;
+
+struct ProbDev {
+  int model, flux, recon, dim, nv, nrk;
+  int nx, ny, nz;
+  int bc[6];
+  int ec1, mu_model, max_iter, is_scalar;
+  int central;        // 0 kepec, 1 kep, 2 roe_ec (TeCNO central part)
+  int fourth;         // 1: 4th-order central combination
+  int tecno;          // 1: entropy-stable dissipation added
+  int rusanov;        // 1: Rusanov Lambda, 0: Roe Lambda
+  int spw_corr;       // SP-WENO correction type, -1 for the network
+  long long off;      // first cell
+  double dx, dy, dz, hmin, vol;
+  double area[3], rarea[3];
+  double gamma, gas_const, prandtl, mu_ref, T_ref, T_0, omega, Cp;
+  double lin_vel[3], lin_speed, lin_vn[3];
+  double cfl, final_time, t_interval;
+  double bc_state[6][5];
+};
+
+struct ProbState {
+  double time, dt, t_save, factor;
+  double ent, ent_prev, ent_acc, ent_max_rise;
+  unsigned long long smax;   // bits of the max wave speed of the newest state
+  int iter, active;
+  int pad[2];
+};
+
+struct StatusDev {
+  int code;
+  int pad;
+  unsigned long long nonfinite, nonpositive, sign_viol, faces_checked;
+};
+
+template <typename T>
+struct SweepArgs {
+  const ProbDev* prob;
+  ProbState* st;
+  const int* task_start;   // nprob + 1 prefix of warp tasks in this direction
+  int nprob, ntask;
+  const T* Uin;            // U^(k), stage input
+  const T* Un;             // U^n
+  T* Uout;                 // U^(k+1)
+  T* R;                    // residual accumulator (non-final sweeps)
+  long long ctot;
+  int rk;
+  double a_rk, b_rk;
+  int final_stage;         // 1: this stage produces U^(n+1)
+  int residual_only;       // 1: write R in every sweep, never update
+  int viscous;             // 1: the NS viscous kernel performs the update
+  StatusDev* status;
+  const NetParams* net;
+};
+
+// ----------------------------------------------------------- small helpers --
+
+template <typename T> struct Vec5 { T v[5]; };
+
+DSPW_HD unsigned long long speed_bits(double s) { return (unsigned long long)__double_as_longlong(s); }
+
+template <typename T>
+DSPW_HD void load_cons(const T* U, long long ctot, long long cell, int nv, int dim, T u[5]) {
+  u[0] = U[cell];
+  u[1] = U[ctot + cell];
+  if (nv == 5) {
+    u[2] = U[2 * ctot + cell];
+    u[3] = U[3 * ctot + cell];
+    u[4] = U[4 * ctot + cell];
+  } else if (nv == 4) {
+    u[2] = U[2 * ctot + cell];
+    u[3] = T(0);
+    u[4] = U[3 * ctot + cell];
+  } else {
+    u[2] = T(0);
+    u[3] = T(0);
+    u[4] = U[2 * ctot + cell];
+  }
+  (void)dim;
+}
+
+template <typename T>
+DSPW_HD void store_cons(T* U, long long ctot, long long cell, int nv, const T u[5]) {
+  U[cell] = u[0];
+  U[ctot + cell] = u[1];
+  if (nv == 5) {
+    U[2 * ctot + cell] = u[2];
+    U[3 * ctot + cell] = u[3];
+    U[4 * ctot + cell] = u[4];
+  } else if (nv == 4) {
+    U[2 * ctot + cell] = u[2];
+    U[3 * ctot + cell] = u[4];
+  } else {
+    U[2 * ctot + cell] = u[4];
+  }
+}
+
+// con_to_prim, enflo/src/fv.cc:388-400
+template <typename T>
+DSPW_HD void cons_to_prim(const T u[5], T gamma, T p[5]) {
+  typedef Mth<T> m;
+  p[0] = u[0];
+  T r = m::rcp(u[0]);
+  p[1] = u[1] * r;
+  p[2] = u[2] * r;
+  p[3] = u[3] * r;
+  T msq = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
+  p[4] = (gamma - T(1.0)) * (u[4] - m::div(T(0.5) * msq, u[0]));
+}
+
+// prim_to_con, enflo/src/fv.cc:405-416
+template <typename T>
+DSPW_HD void prim_to_cons(const T p[5], T gamma, T u[5]) {
+  typedef Mth<T> m;
+  u[0] = p[0];
+  u[1] = p[1] * p[0];
+  u[2] = p[2] * p[0];
+  u[3] = p[3] * p[0];
+  T vsq = p[1] * p[1] + p[2] * p[2] + p[3] * p[3];
+  u[4] = T(0.5) * p[0] * vsq + m::div(p[4], gamma - T(1.0));
+}
+
+// entropy variables, enflo/src/fv.cc:427-433 with Entropy :557-560
+template <typename T>
+DSPW_HD void prim_to_ent(const T p[5], T gamma, T v[5]) {
+  typedef Mth<T> m;
+  T beta = m::div(p[0], T(2) * p[4]);
+  T s = m::log(p[4]) - gamma * m::log(p[0]);
+  T vsq = p[1] * p[1] + p[2] * p[2] + p[3] * p[3];
+  v[0] = m::div(gamma - s, gamma - T(1)) - vsq * beta;
+  v[1] = p[1] * (T(2) * beta);
+  v[2] = p[2] * (T(2) * beta);
+  v[3] = p[3] * (T(2) * beta);
+  v[4] = T(-2) * beta;
+}
+
+// Viscosity, enflo/src/parameter.cc:646-663
+DSPW_HD double viscosity(const ProbDev& P, double T) {
+  if (P.mu_model == DSPW_MU_SUTHERLAND) return P.mu_ref * ::pow(T / P.T_ref, 1.5) * (P.T_ref + P.T_0) / (T + P.T_0);
+  if (P.mu_model == DSPW_MU_POWER) return P.mu_ref * ::pow(T / P.T_ref, P.omega);
+  return P.mu_ref;
+}
+
+// wave speed of compute_dt, enflo/src/fv.cc:366-383 (+ viscous term for NS)
+template <typename T>
+DSPW_HD double wave_speed(const ProbDev& P, const T p[5]) {
+  if (P.model == DSPW_LINADV) return P.lin_speed;
+  if (P.model == DSPW_BURGERS) return (double)Mth<T>::abs(p[0]);
+  double rho = (double)p[0], pr = (double)p[4];
+  double u = p[1], v = p[2], w = p[3];
+  double s = ::sqrt(u * u + v * v + w * w) + ::sqrt(P.gamma * pr / rho);
+  if (P.model == DSPW_NS_ES || P.model == DSPW_NS_KEP)
+    s += viscosity(P, pr / (P.gas_const * rho)) / rho / P.hmin;
+  return s;
+}
+
+DSPW_HD unsigned warp_max_u64_lane0(unsigned long long& v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return 0;
+}
+
+DSPW_HD double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// global task -> problem (binary search in the prefix sums)
+DSPW_HD int find_problem(const int* start, int nprob, int task) {
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(start + mid) <= task) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int DIR>
+DSPW_HD int dir_len(const ProbDev& P) { return DIR == 0 ? P.nx : (DIR == 1 ? P.ny : P.nz); }
+
+// (line index, segment) of a local task.  DIR 0: seg fastest, then j, then k
+// (consecutive warps extend the same x line).  DIR 1/2: x fastest so the warps
+// of a block read adjacent x columns.
+template <int DIR>
+DSPW_HD void decode_task(const ProbDev& P, int lt, int& i0, int& j0, int& k0, int& c0, int& ncell) {
+  int N = dir_len<DIR>(P);
+  int nseg = (N + SEG_CELLS - 1) / SEG_CELLS;
+  int seg;
+  if (DIR == 0) {
+    seg = lt % nseg; lt /= nseg;
+    j0 = lt % P.ny; k0 = lt / P.ny; i0 = 0;
+  } else if (DIR == 1) {
+    i0 = lt % P.nx; lt /= P.nx;
+    seg = lt % nseg; k0 = lt / nseg; j0 = 0;
+  } else {
+    i0 = lt % P.nx; lt /= P.nx;
+    seg = lt % nseg; j0 = lt / nseg; k0 = 0;
+  }
+  c0 = seg * SEG_CELLS;
+  ncell = min(SEG_CELLS, N - c0);
+}
+
+template <int DIR>
+DSPW_HD long long cell_index(const ProbDev& P, int i0, int j0, int k0, int c) {
+  if (DIR == 0) return P.off + ((long long)k0 * P.ny + j0) * P.nx + c;
+  if (DIR == 1) return P.off + ((long long)k0 * P.ny + c) * P.nx + i0;
+  return P.off + ((long long)c * P.ny + j0) * P.nx + i0;
+}
+
+// Ghost handling of apply_bc (enflo/src/fv.cc:121-361): source cell along the
+// line for a (possibly ghost) index c, and the boundary kind used.
+DSPW_HD int ghost_source(int c, int N, int kind, int& flip) {
+  flip = 0;
+  if (c >= 0 && c < N) return c;
+  if (kind == DSPW_BC_PERIODIC) return ((c % N) + N) % N;
+  if (kind == DSPW_BC_WALL) { flip = 1; return c < 0 ? -1 - c : 2 * N - 1 - c; }
+  return c < 0 ? 0 : N - 1;   // neumann (and dirichlet, which ignores it)
+}
+
+// ------------------------------------------------------ warp shared memory --
+
+// staging of the network inputs / outputs of one warp (FP32 form only)
+template <typename T> struct NetScratch { float feat[32][8]; float logit[32][8]; };
+template <> struct NetScratch<double> { float feat[1][8]; float logit[1][8]; };
+
+template <typename T>
+struct WarpSmem {
+  T P[5][SEG_LOAD];
+  T V[5][SEG_LOAD];
+  T W[5][32];      // wide two-point fluxes, centre g = c0 - 1 + idx
+  T F[5][32];      // face fluxes, face f = c0 + idx
+  NetScratch<T> ns;
+};
+
+// ---------------------------------------------------- two-point fluxes ------
+
+// face-average state shared by kepec and the TeCNO dissipation
+// (enflo/src/kepec.cc:18-30, kepes_tecno4_roe.cc:34-48)
+template <typename T>
+struct FaceAvg {
+  T rho, beta, p, betal, betar, vel[3], vn;
+};
+
+template <typename T, int DIR>
+DSPW_HD void face_avg(const T* Pl, const T* Pr, T Rg, FaceAvg<T>& f) {
+  typedef Mth<T> m;
+  T rhol = Pl[0], rhor = Pr[0];
+  f.rho = logavg<T>(rhol, rhor);
+  T templ = m::div(Pl[4], Rg * rhol);
+  T tempr = m::div(Pr[4], Rg * rhor);
+  f.betal = m::div(T(0.5), Rg * templ);
+  f.betar = m::div(T(0.5), Rg * tempr);
+  f.beta = logavg<T>(f.betal, f.betar);
+  f.p = m::div(T(0.5) * (rhol + rhor), f.betal + f.betar);
+  f.vel[0] = Pl[1] * T(0.5) + Pr[1] * T(0.5);
+  f.vel[1] = Pl[2] * T(0.5) + Pr[2] * T(0.5);
+  f.vel[2] = Pl[3] * T(0.5) + Pr[3] * T(0.5);
+  // vel * unit_normal with n = e_DIR: the other products are +-0
+  f.vn = f.vel[0] * T(DIR == 0) + f.vel[1] * T(DIR == 1) + f.vel[2] * T(DIR == 2);
+}
+
+// kepec_flux from a face average, enflo/src/kepec.cc:30-48
+template <typename T, int DIR>
+DSPW_HD void kepec_from_avg(const FaceAvg<T>& f, const T* Pl, const T* Pr, T gamma, T area, T F[5]) {
+  typedef Mth<T> m;
+  T vel2 = T(0.5) * ((Pl[1] * Pl[1] + Pl[2] * Pl[2] + Pl[3] * Pl[3]) + (Pr[1] * Pr[1] + Pr[2] * Pr[2] + Pr[3] * Pr[3]));
+  F[0] = f.rho * f.vn;
+  F[1] = T(DIR == 0) * f.p + f.vel[0] * F[0];
+  F[2] = T(DIR == 1) * f.p + f.vel[1] * F[0];
+  F[3] = T(DIR == 2) * f.p + f.vel[2] * F[0];
+  F[4] = T(0.5) * (m::div(T(1.0), (gamma - T(1.0)) * f.beta) - vel2) * F[0] +
+         (F[1] * f.vel[0] + F[2] * f.vel[1] + F[3] * f.vel[2]);
+#pragma unroll
+  for (int c = 0; c < 5; c++) F[c] *= area;
+}
+
+template <typename T, int DIR>
+DSPW_HD void kepec_pair(const T* Pl, const T* Pr, T gamma, T Rg, T area, T F[5]) {
+  FaceAvg<T> f;
+  face_avg<T, DIR>(Pl, Pr, Rg, f);
+  kepec_from_avg<T, DIR>(f, Pl, Pr, gamma, area, F);
+}
+
+// kep_flux, enflo/src/kep.cc:10-44 (Enthalpy enflo/src/fv.cc:565-569)
+template <typename T, int DIR>
+DSPW_HD void kep_pair(const T* Pl, const T* Pr, T gamma, T area, T F[5]) {
+  typedef Mth<T> m;
+  T rho = T(0.5) * (Pl[0] + Pr[0]);
+  T p = T(0.5) * (Pl[4] + Pr[4]);
+  T vel[3] = {Pl[1] * T(0.5) + Pr[1] * T(0.5), Pl[2] * T(0.5) + Pr[2] * T(0.5), Pl[3] * T(0.5) + Pr[3] * T(0.5)};
+  T al = m::sqrt(m::div(gamma * Pl[4], Pl[0]));
+  T ar = m::sqrt(m::div(gamma * Pr[4], Pr[0]));
+  T Hl = m::div(al * al, gamma - T(1.0)) + T(0.5) * (Pl[1] * Pl[1] + Pl[2] * Pl[2] + Pl[3] * Pl[3]);
+  T Hr = m::div(ar * ar, gamma - T(1.0)) + T(0.5) * (Pr[1] * Pr[1] + Pr[2] * Pr[2] + Pr[3] * Pr[3]);
+  T H = T(0.5) * (Hl + Hr);
+  T vn = vel[0] * T(DIR == 0) + vel[1] * T(DIR == 1) + vel[2] * T(DIR == 2);
+  F[0] = rho * vn;
+  F[1] = T(DIR == 0) * p + vel[0] * F[0];
+  F[2] = T(DIR == 1) * p + vel[1] * F[0];
+  F[3] = T(DIR == 2) * p + vel[2] * F[0];
+  F[4] = rho * H * vn;
+#pragma unroll
+  for (int c = 0; c < 5; c++) F[c] *= area;
+}
+
+// roe_ec_flux, enflo/src/roe_ec.cc:10-69
+template <typename T, int DIR>
+DSPW_HD void roe_ec_pair(const T* Pl, const T* Pr, T gamma, T area, T F[5]) {
+  typedef Mth<T> m;
+  T rhol = Pl[0], rhor = Pr[0], pl = Pl[4], pr = Pr[4];
+  T bl = m::sqrt(m::div(rhol, pl));
+  T br = m::sqrt(m::div(rhor, pr));
+  T z1b = T(0.5) * (bl + br);
+  T zvb[3] = {Pl[1] * (T(0.5) * bl) + Pr[1] * (T(0.5) * br), Pl[2] * (T(0.5) * bl) + Pr[2] * (T(0.5) * br),
+              Pl[3] * (T(0.5) * bl) + Pr[3] * (T(0.5) * br)};
+  T z5b = T(0.5) * (bl * pl + br * pr);
+  T zn = zvb[0] * T(DIR == 0) + zvb[1] * T(DIR == 1) + zvb[2] * T(DIR == 2);
+  T z1l = logavg<T>(bl, br);
+  T z5l = logavg<T>(bl * pl, br * pr);
+  F[0] = z5l * zn;
+  T c1 = m::div(z5b, z1b), c2 = m::div(F[0], z1b);
+  F[1] = T(DIR == 0) * c1 + zvb[0] * c2;
+  F[2] = T(DIR == 1) * c1 + zvb[1] * c2;
+  F[3] = T(DIR == 2) * c1 + zvb[2] * c2;
+  F[4] = m::div(T(0.5) * (m::div(m::div(gamma + T(1.0), gamma - T(1.0)) * F[0], z1l) +
+                          (F[1] * zvb[0] + F[2] * zvb[1] + F[3] * zvb[2])), z1b);
+#pragma unroll
+  for (int c = 0; c < 5; c++) F[c] *= area;
+}
+
+template <typename T, int DIR>
+DSPW_HD void central_pair(int kind, const T* Pl, const T* Pr, T gamma, T Rg, T area, T F[5]) {
+  if (kind == 0) kepec_pair<T, DIR>(Pl, Pr, gamma, Rg, area, F);
+  else if (kind == 1) kep_pair<T, DIR>(Pl, Pr, gamma, area, F);
+  else roe_ec_pair<T, DIR>(Pl, Pr, gamma, area, F);
+}
+
+// ------------------------------------------------- BF16 tensor-core network --
+
+// One warp evaluates the 5-5-5-5-5 network for 32 instances (one per lane) as
+// two m16n8k8 BF16 MMA tiles per layer, FP32 accumulation; layer outputs stay
+// in registers (the C fragment of one layer is the A fragment of the next).
+struct NetFrag {
+  uint32_t b[4];       // B fragment per layer: W^T (k = input, n = output)
+  float bias0[4], bias1[4];   // bias of output columns n = 2*(lane%4), +1
+};
+
+DSPW_HD uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+__device__ inline void net_frag_load(const NetParams& P, int lane, NetFrag& nf) {
+  int n = lane >> 2, k0 = (lane & 3) * 2;
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    float w0 = (n < 5 && k0 < 5) ? P.wf[l][n][k0] : 0.f;
+    float w1 = (n < 5 && k0 + 1 < 5) ? P.wf[l][n][k0 + 1] : 0.f;
+    nf.b[l] = pack_bf16(w0, w1);
+    nf.bias0[l] = (k0 < 5) ? P.bf[l][k0] : 0.f;
+    nf.bias1[l] = (k0 + 1 < 5) ? P.bf[l][k0 + 1] : 0.f;
+  }
+}
+
+DSPW_HD void mma_bf16_16x8x8(float c[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(b0));
+}
+
+// in: feat (this lane's 5 inputs); out: logits (this lane's 5 outputs)
+__device__ inline void warp_mlp_bf16(const NetFrag& nf, float (*fs)[8], float (*ls)[8], const float in[5],
+                                     float out[5], int lane) {
+#pragma unroll
+  for (int k = 0; k < 5; k++) fs[lane][k] = in[k];
+  fs[lane][5] = 0.f; fs[lane][6] = 0.f; fs[lane][7] = 0.f;
+  __syncwarp();
+  int r = lane >> 2, kq = (lane & 3) * 2;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    uint32_t a0 = pack_bf16(fs[16 * t + r][kq], fs[16 * t + r][kq + 1]);
+    uint32_t a1 = pack_bf16(fs[16 * t + r + 8][kq], fs[16 * t + r + 8][kq + 1]);
+    float c[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      c[0] = nf.bias0[l]; c[1] = nf.bias1[l]; c[2] = nf.bias0[l]; c[3] = nf.bias1[l];
+      mma_bf16_16x8x8(c, a0, a1, nf.b[l]);
+      if (l < 3) {
+        a0 = pack_bf16(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f));
+        a1 = pack_bf16(fmaxf(c[2], 0.f), fmaxf(c[3], 0.f));
+      }
+    }
+    ls[16 * t + r][kq] = c[0];
+    ls[16 * t + r][kq + 1] = c[1];
+    ls[16 * t + r + 8][kq] = c[2];
+    ls[16 * t + r + 8][kq + 1] = c[3];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 5; k++) out[k] = ls[lane][k];
+  __syncwarp();
+}
+
+// DSP-WENO reconstruction of one stencil per lane, warp-cooperative network.
+// Every lane of the warp must call it (the MMA is warp-wide); `valid` masks
+// lanes whose result is unused.  Returns 1 if the sign-preserving limiter had
+// to act (FP32 form).
+template <typename T>
+__device__ inline int dsp_weno_warp(const NetParams& NP, const NetFrag& nf, WarpSmem<T>* sm, int lane, bool valid,
+                                    T u0, T u1, T u2, T u3, T& l, T& r);
+
+template <>
+__device__ inline int dsp_weno_warp<double>(const NetParams& NP, const NetFrag&, WarpSmem<double>*, int, bool valid,
+                                            double u0, double u1, double u2, double u3, double& l, double& r) {
+  if (valid) dsp_weno_fp64(NP, u0, u1, u2, u3, l, r);
+  return 0;
+}
+
+template <>
+__device__ inline int dsp_weno_warp<float>(const NetParams& NP, const NetFrag& nf, WarpSmem<float>* sm, int lane,
+                                           bool valid, float u0, float u1, float u2, float u3, float& l, float& r) {
+  bool guard = fabsf(u2 - u1) < 1e-15f;
+  float feat[5], vx[5], vy[5];
+  nn_features<float>(u0, u1, u2, u3, feat, vx, vy);
+  bool use = valid && !guard;
+  if (!use) { feat[0] = feat[1] = feat[2] = feat[3] = feat[4] = 0.f; }
+  bool inbox = true;
+  if (NP.use_box) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) inbox = inbox && feat[k] >= NP.feat_lo[k] && feat[k] <= NP.feat_hi[k];
+  }
+  float lg[5];
+  warp_mlp_bf16(nf, sm->ns.feat, sm->ns.logit, feat, lg, lane);
+  if (!valid) return 0;
+  if (guard) { l = 0.f; r = 0.f; return 0; }
+  if (!inbox) {   // outside the network's training range: plain SP-WENO
+    sp_weno<float>(u0, u1, u2, u3, 0, l, r);
+    return 0;
+  }
+  nn_finish<float>(lg, vx, vy, u0, u1, u2, u3, l, r);
+  // sign-preserving limiter: the reconstructed jump must not oppose the cell jump
+  float dj = u2 - u1, rj = r - l;
+  if (dj * rj < 0.f) {
+    float c = 0.5f * (l + r);
+    l = c; r = c;
+    return 1;
+  }
+  return 0;
+}
+
+template <typename T>
+__device__ inline void reconstruct_lane(const ProbDev& P, const NetParams& NP, const NetFrag& nf, WarpSmem<T>* sm,
+                                        int lane, bool valid, T s0, T s1, T s2, T s3, T& l, T& r, int& viol) {
+  if (P.spw_corr >= 0) {
+    if (valid) sp_weno<T>(s0, s1, s2, s3, P.spw_corr, l, r);
+  } else {
+    viol += dsp_weno_warp<T>(NP, nf, sm, lane, valid, s0, s1, s2, s3, l, r);
+  }
+}
+
+// ------------------------------------------------------------ Euler sweep --
+
+// TeCNO dissipation -0.5 R Lambda [[Z]] for one face (enflo/src/kepes_tecno4_roe.cc:59-171
+// and the Roe / Rusanov variants), R = eigenvectors scaled by S^(1/2), Z = R^T V
+// of the 4 stencil cells, component-wise reconstruction.  Columns of R are
+// built one at a time; Diff[i] accumulates over j in the reference's order.
+template <typename T, int DIR, int DIM>
+__device__ inline void tecno_dissipation(const ProbDev& P, const NetParams& NP, const NetFrag& nf, WarpSmem<T>* sm,
+                                         int lane, bool valid, int q0, const FaceAvg<T>& fa, T flux[5],
+                                         int& viol, unsigned long long& signv) {
+  typedef Mth<T> m;
+  const T G = T(P.gamma);
+  const T n0 = T(DIR == 0), n1 = T(DIR == 1), n2 = T(DIR == 2);
+  const T* vel = fa.vel;
+  T a = m::sqrt(m::div(T(0.5) * G, fa.beta));
+  T vsq = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
+  T H = m::div(a * a, G - T(1.0)) + T(0.5) * vsq;
+  T v1 = vel[0] * n1 - vel[1] * n0;
+  T v2 = vel[2] * n0 - vel[0] * n2;
+  T const1 = m::sqrt(m::div(fa.rho, G));
+  T psqrt = m::sqrt(fa.p);
+  const T sh = m::sqrt(T(0.5));
+  T S[5] = {sh * const1, m::sqrt(G - T(1.0)) * const1, psqrt, psqrt, sh * const1};
+  T Lam[5];
+  if (!P.rusanov) {
+    T l2 = m::abs(fa.vn);
+    T ma = T(0.0);
+    T L0 = m::abs(fa.vn - a), L4 = m::abs(fa.vn + a);
+    if (P.ec1) {
+      // LambdaL[0]-LambdaR[0] and LambdaL[3]-LambdaR[3] (kepes_tecno4_roe.cc:92-113)
+      T vnl = sm->P[1 + DIR][q0 + 1], vnr = sm->P[1 + DIR][q0 + 2];
+      T al = m::sqrt(m::div(T(0.5) * G, fa.betal));
+      T ar = m::sqrt(m::div(T(0.5) * G, fa.betar));
+      ma = T(1.0 / 6.0);
+      L0 = L0 + ma * m::abs((vnl - al) - (vnr - ar));
+      L4 = L4 + ma * m::abs(vnl - vnr);
+    }
+    Lam[0] = L0; Lam[1] = l2; Lam[2] = l2; Lam[3] = l2; Lam[4] = L4;
+  } else {
+    T lr = m::abs(fa.vn) + m::abs(a);
+    Lam[0] = Lam[1] = Lam[2] = Lam[3] = Lam[4] = lr;
+  }
+  T Diff[5] = {T(0), T(0), T(0), T(0), T(0)};
+#pragma unroll
+  for (int j = 0; j < 5; j++) {
+    // components that are identically zero in lower dimensions (exact skip)
+    if (DIM == 1 && (j == 2 || j == 3)) continue;
+    if (DIM == 2 && j == 3) continue;
+    // column j of R (kepes_tecno4_roe.cc:66-72), scaled by S[j]
+    T col[5];
+    if (j == 0) { col[0] = T(1); col[1] = vel[0] - a * n0; col[2] = vel[1] - a * n1; col[3] = vel[2] - a * n2; col[4] = H - a * fa.vn; }
+    else if (j == 1) { col[0] = T(1); col[1] = vel[0]; col[2] = vel[1]; col[3] = vel[2]; col[4] = T(0.5) * vsq; }
+    else if (j == 2) { col[0] = T(0); col[1] = n1; col[2] = -n0; col[3] = T(0); col[4] = v1; }
+    else if (j == 3) { col[0] = T(0); col[1] = -n2; col[2] = T(0); col[3] = n0; col[4] = v2; }
+    else { col[0] = T(1); col[1] = vel[0] + a * n0; col[2] = vel[1] + a * n1; col[3] = vel[2] + a * n2; col[4] = H + a * fa.vn; }
+#pragma unroll
+    for (int r = 0; r < 5; r++) col[r] *= S[j];
+    T z[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      int q = q0 + k;
+      T acc = col[0] * sm->V[0][q] + col[1] * sm->V[1][q];
+      if (DIM >= 2) acc = acc + col[2] * sm->V[2][q];
+      if (DIM >= 3) acc = acc + col[3] * sm->V[3][q];
+      acc = acc + col[4] * sm->V[4][q];
+      z[k] = T(0.0) + acc;
+    }
+    T zl = T(0), zr = T(0);
+    reconstruct_lane<T>(P, NP, nf, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol);
+    T dZ = zr - zl;
+    if (valid) {
+      // sign property check on every reconstructed component jump
+      T cj = z[2] - z[1];
+      if (cj * dZ < T(0)) signv++;
+    }
+    T ld = Lam[j];
+#pragma unroll
+    for (int i = 0; i < 5; i++) Diff[i] += col[i] * ld * dZ;
+  }
+  flux[0] -= T(0.5) * Diff[0];
+  flux[1] -= T(0.5) * Diff[1];
+  flux[2] -= T(0.5) * Diff[2];
+  if (DIM >= 3) flux[2] -= T(0.5) * Diff[3];   // momentum y, as the reference (kepes_tecno4_roe.cc:170)
+  flux[4] -= T(0.5) * Diff[4];
+}
+
+// ------------------------------------------------------------ warp tasks --
+
+// load the SEG_LOAD staged cells of a line segment (interior + ghosts) as
+// primitive and entropy variables; ghost cells follow apply_bc
+// (enflo/src/fv.cc:121-361): periodic wrap, wall mirror with the normal
+// velocity negated, neumann copy of the boundary cell, dirichlet fixed state.
+template <typename T, int DIR>
+__device__ inline void euler_stage_cells(const SweepArgs<T>& A, const ProbDev& P, WarpSmem<T>* sm, int lane, int i0,
+                                         int j0, int k0, int c0, int ncell) {
+  const int N = dir_len<DIR>(P);
+  const T G = T(P.gamma);
+  for (int q = lane; q < ncell + 4; q += 32) {
+    int c = c0 - 2 + q;
+    int side = c < 0 ? 0 : 1;
+    int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
+    T p[5];
+    if (kind == DSPW_BC_DIRICHLET) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) p[v] = T(P.bc_state[2 * DIR + side][v]);
+    } else {
+      int flip;
+      int src = ghost_source(c, N, kind, flip);
+      T u[5];
+      load_cons<T>(A.Uin, A.ctot, cell_index<DIR>(P, i0, j0, k0, src), P.nv, P.dim, u);
+      cons_to_prim<T>(u, G, p);
+      if (flip) p[1 + DIR] = -p[1 + DIR];
+    }
+    T v[5];
+    prim_to_ent<T>(p, G, v);
+#pragma unroll
+    for (int w = 0; w < 5; w++) { sm->P[w][q] = p[w]; sm->V[w][q] = v[w]; }
+  }
+  __syncwarp();
+}
+
+// final combination for one cell: residual (reference order
+// ((R_prev - F_left) + F_right)) then either store R or apply the SSPRK stage
+// update U = b U + (a U^n + R (-factor b)) (enflo/src/fv.cc:1163-1175), with
+// the CFL speed / entropy / health epilogue on the stage that yields U^(n+1).
+template <typename T>
+__device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
+                                   bool first, bool final_sweep, const T Fl[5], const T Fr[5], int nv_eff,
+                                   double& smax, double& ent, unsigned& bad_fin, unsigned& bad_pos) {
+  T R[5];
+  if (first) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) R[v] = (T(0.0) - Fl[v]) + Fr[v];
+  } else {
+    T r0[5];
+    if (P.is_scalar) { r0[0] = A.R[cell]; r0[1] = r0[2] = r0[3] = r0[4] = T(0); }
+    else load_cons<T>(A.R, A.ctot, cell, P.nv, P.dim, r0);
+#pragma unroll
+    for (int v = 0; v < 5; v++) R[v] = (r0[v] - Fl[v]) + Fr[v];
+  }
+  if (!final_sweep) {
+    if (P.is_scalar) A.R[cell] = R[0];
+    else store_cons<T>(A.R, A.ctot, cell, P.nv, R);
+    return;
+  }
+  const T a = T(A.a_rk), b = T(A.b_rk);
+  const T c2 = T(-S.factor * A.b_rk);
+  T u[5], un[5];
+  if (P.is_scalar) {
+    u[0] = A.Uin[cell];
+    un[0] = A.Un[cell];
+    T x = u[0] * b;
+    x = x + (un[0] * a - T(S.factor * A.b_rk) * R[0]);
+    A.Uout[cell] = x;
+    if (A.final_stage) {
+      T pp[5] = {x, T(0), T(0), T(0), T(0)};
+      double sp = wave_speed<T>(P, pp);
+      if (sp > smax) smax = sp;   // NaN speeds are skipped, as std::min skips them in compute_dt
+      ent += 0.5 * (double)x * (double)x;
+      if (!isfinite((double)x)) bad_fin++;
+    }
+    return;
+  }
+  load_cons<T>(A.Uin, A.ctot, cell, P.nv, P.dim, u);
+  load_cons<T>(A.Un, A.ctot, cell, P.nv, P.dim, un);
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    u[v] *= b;
+    u[v] += un[v] * a + R[v] * c2;
+  }
+  store_cons<T>(A.Uout, A.ctot, cell, P.nv, u);
+  if (A.final_stage) {
+    T p[5];
+    cons_to_prim<T>(u, T(P.gamma), p);
+    double sp = wave_speed<T>(P, p);
+    if (sp > smax) smax = sp;
+    double rho = p[0], pr = p[4];
+    if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
+    if (!isfinite(rho) || !isfinite(pr) || !isfinite((double)u[1]) || !isfinite((double)u[4])) bad_fin++;
+    double s = ::log(pr) - P.gamma * ::log(rho);
+    ent += -rho * s / (P.gamma - 1.0);
+  }
+  (void)nv_eff;
+}
+
+template <typename T>
+__device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax, double ent,
+                                     unsigned bad_fin, unsigned bad_pos, unsigned long long signv, int viol) {
+  if (A.final_stage && !A.residual_only) {
+    unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
+    warp_max_u64_lane0(sb);
+    double es = warp_sum(ent);
+    if (lane == 0) {
+      atomicMax(&S.smax, sb);
+      atomicAdd(&S.ent_acc, es);
+    }
+  }
+  unsigned bf = __reduce_add_sync(0xffffffffu, bad_fin);
+  unsigned bp = __reduce_add_sync(0xffffffffu, bad_pos);
+  unsigned sv = __reduce_add_sync(0xffffffffu, (unsigned)signv);
+  unsigned vv = __reduce_add_sync(0xffffffffu, (unsigned)viol);
+  if (lane == 0 && (bf | bp | sv | vv)) {
+    if (bf) { atomicAdd(&A.status->nonfinite, (unsigned long long)bf); atomicCAS(&A.status->code, 0, DSPW_ERR_NONFINITE); }
+    if (bp) { atomicAdd(&A.status->nonpositive, (unsigned long long)bp); atomicCAS(&A.status->code, 0, DSPW_ERR_NONPOSITIVE); }
+    if (sv + vv) atomicAdd(&A.status->sign_viol, (unsigned long long)(sv + vv));
+  }
+}
+
+template <typename T, int DIR, int DIM>
+__device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S, const NetFrag& nf,
+                           WarpSmem<T>* sm, int lane, int lt) {
+  int i0, j0, k0, c0, ncell;
+  decode_task<DIR>(P, lt, i0, j0, k0, c0, ncell);
+  euler_stage_cells<T, DIR>(A, P, sm, lane, i0, j0, k0, c0, ncell);
+  const T G = T(P.gamma), Rg = T(P.gas_const), area = T(P.area[DIR]);
+  // phase B: wide two-point flux centred at g = c0 - 1 + lane (cells g-1, g+1)
+  if (P.fourth && lane <= ncell + 1) {
+    T Fw[5], Pl[5], Pr[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) { Pl[v] = sm->P[v][lane]; Pr[v] = sm->P[v][lane + 2]; }
+    central_pair<T, DIR>(P.central, Pl, Pr, G, Rg, area, Fw);
+#pragma unroll
+    for (int v = 0; v < 5; v++) sm->W[v][lane] = Fw[v];
+  }
+  __syncwarp();
+  // phase C: face f = c0 + lane between staged cells q = lane+1 and lane+2
+  const bool valid = lane <= ncell;
+  T flux[5] = {T(0), T(0), T(0), T(0), T(0)};
+  FaceAvg<T> fa;
+  int viol = 0;
+  unsigned long long signv = 0;
+  {
+    T Pl[5], Pr[5];
+    const int ql = valid ? lane + 1 : 1;
+#pragma unroll
+    for (int v = 0; v < 5; v++) { Pl[v] = sm->P[v][ql]; Pr[v] = sm->P[v][ql + 1]; }
+    face_avg<T, DIR>(Pl, Pr, Rg, fa);
+    T Fn[5];
+    if (P.central == 0) kepec_from_avg<T, DIR>(fa, Pl, Pr, G, area, Fn);
+    else central_pair<T, DIR>(P.central, Pl, Pr, G, Rg, area, Fn);
+    if (P.fourth) {
+      // kepec4 / roe_ec4 / kep4: 4/3 F(1,2) - 1/6 F(0,2) - 1/6 F(1,3) (enflo/src/kepec4.cc:10-38)
+      const T fact = T(-1.0 / 6.0);
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        T f = T(0.0);
+        f += Fn[v] * T(4.0 / 3.0);
+        f += sm->W[v][ql - 1] * fact;
+        f += sm->W[v][ql] * fact;
+        flux[v] = f;
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; v++) flux[v] = Fn[v];
+    }
+  }
+  if (P.tecno) {
+    const T ra = T(P.rarea[DIR]);
+#pragma unroll
+    for (int v = 0; v < 5; v++) flux[v] *= ra;
+    tecno_dissipation<T, DIR, DIM>(P, *A.net, nf, sm, lane, valid, valid ? lane : 0, fa, flux, viol, signv);
+#pragma unroll
+    for (int v = 0; v < 5; v++) flux[v] *= area;
+  }
+  if (valid) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) sm->F[v][lane] = flux[v];
+  }
+  __syncwarp();
+  // phase D: cells
+  const bool first = (DIR == 0);
+  const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
+  double smax = 0.0, ent = 0.0;
+  unsigned bad_fin = 0, bad_pos = 0;
+  if (lane < ncell) {
+    T Fl[5], Fr[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) { Fl[v] = sm->F[v][lane]; Fr[v] = sm->F[v][lane + 1]; }
+    long long cell = cell_index<DIR>(P, i0, j0, k0, c0 + lane);
+    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, P.nv, smax, ent, bad_fin, bad_pos);
+  }
+  if (!final_sweep) { smax = 0.0; ent = 0.0; }
+  SweepArgs<T> A2 = A;
+  A2.final_stage = A.final_stage && final_sweep;
+  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol);
+  __syncwarp();
+}
+
+// scalar laws: lin_/bur_ fluxes (enflo_scalar/src_scalar/num_flux.cc:12-57,
+// lin_tecno4.cc:10-31, lin_ec4.cc:10-34, bur_tecno4.cc:10-35, bur_ec4.cc:10-34)
+template <typename T, int DIR>
+__device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S, const NetFrag& nf,
+                            WarpSmem<T>* sm, int lane, int lt) {
+  typedef Mth<T> m;
+  int i0, j0, k0, c0, ncell;
+  decode_task<DIR>(P, lt, i0, j0, k0, c0, ncell);
+  const int N = dir_len<DIR>(P);
+  for (int q = lane; q < ncell + 4; q += 32) {
+    int c = c0 - 2 + q;
+    int side = c < 0 ? 0 : 1;
+    int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
+    T u;
+    if (kind == DSPW_BC_DIRICHLET) u = T(P.bc_state[2 * DIR + side][0]);
+    else {
+      int flip;
+      int src = ghost_source(c, N, kind, flip);
+      u = A.Uin[cell_index<DIR>(P, i0, j0, k0, src)];
+      if (flip) u = -u;
+    }
+    sm->P[0][q] = u;
+  }
+  __syncwarp();
+  const bool valid = lane <= ncell;
+  const int q = valid ? lane : 0;
+  T s0 = sm->P[0][q], s1 = sm->P[0][q + 1], s2 = sm->P[0][q + 2], s3 = sm->P[0][q + 3];
+  const T vn = T(P.lin_vn[DIR]);
+  T flux = T(0);
+  const int fl = P.flux;
+  if (fl == DSPW_LIN_EC || fl == DSPW_LIN_TECNO) {
+    flux = T(0.5) * vn * (s1 + s2);
+  } else if (fl == DSPW_LIN_EC4 || fl == DSPW_LIN_TECNO4) {
+    flux = T(0.0);
+    flux += m::div((T(0.5) * vn * (s1 + s2)) * T(4.0), T(3.0));
+    flux += (T(0.5) * vn * (s0 + s2)) * T(-1.0 / 6.0);
+    flux += (T(0.5) * vn * (s1 + s3)) * T(-1.0 / 6.0);
+  } else if (fl == DSPW_BUR_EC || fl == DSPW_BUR_TECNO) {
+    flux = m::div(s1 * s1 + s2 * s2 + s1 * s2, T(6.0));
+  } else {
+    flux = T(0.0);
+    flux += m::div(s1 * s1 + s2 * s2 + s1 * s2, T(6.0)) * T(4.0 / 3.0);
+    flux += m::div(s0 * s0 + s2 * s2 + s0 * s2, T(6.0)) * T(-1.0 / 6.0);
+    flux += m::div(s1 * s1 + s3 * s3 + s1 * s3, T(6.0)) * T(-1.0 / 6.0);
+  }
+  int viol = 0;
+  unsigned long long signv = 0;
+  if (P.tecno) {
+    T D = (P.model == DSPW_LINADV) ? m::abs(vn) : T(0.5) * (m::abs(s1) + m::abs(s2));
+    T l = T(0), r = T(0);
+    reconstruct_lane<T>(P, *A.net, nf, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
+    if (valid && (s2 - s1) * (r - l) < T(0)) signv++;
+    flux -= T(0.5) * D * (r - l);
+  }
+  flux *= T(P.area[DIR]);
+  if (valid) sm->F[0][lane] = flux;
+  __syncwarp();
+  const bool first = (DIR == 0);
+  const bool final_sweep = !A.residual_only && (DIR == P.dim - 1);
+  double smax = 0.0, ent = 0.0;
+  unsigned bad_fin = 0, bad_pos = 0;
+  if (lane < ncell) {
+    T Fl[5] = {sm->F[0][lane], T(0), T(0), T(0), T(0)};
+    T Fr[5] = {sm->F[0][lane + 1], T(0), T(0), T(0), T(0)};
+    long long cell = cell_index<DIR>(P, i0, j0, k0, c0 + lane);
+    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, 1, smax, ent, bad_fin, bad_pos);
+  }
+  SweepArgs<T> A2 = A;
+  A2.final_stage = A.final_stage && final_sweep;
+  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol);
+  __syncwarp();
+}
+
+// One sweep of direction DIR over every problem of the batch.
+template <typename T, int DIR>
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32)
+k_sweep(SweepArgs<T> A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem<T>* sm = reinterpret_cast<WarpSmem<T>*>(smem_raw) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  NetFrag nf;
+  if (sizeof(T) == 4) net_frag_load(*A.net, lane, nf);
+  const int stride = gridDim.x * WARPS_PER_BLOCK;
+  for (int task = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); task < A.ntask; task += stride) {
+    const int p = find_problem(A.task_start, A.nprob, task);
+    const ProbDev& P = A.prob[p];
+    ProbState& S = A.st[p];
+    if (!A.residual_only && !*((volatile int*)&S.active)) continue;
+    const int lt = task - __ldg(A.task_start + p);
+    if (P.is_scalar) {
+      scalar_task<T, DIR>(A, P, S, nf, sm, lane, lt);
+    } else {
+      if (DIR == 0) {
+        if (P.dim == 1) euler_task<T, DIR, 1>(A, P, S, nf, sm, lane, lt);
+        else if (P.dim == 2) euler_task<T, DIR, 2>(A, P, S, nf, sm, lane, lt);
+        else euler_task<T, DIR, 3>(A, P, S, nf, sm, lane, lt);
+      } else if (DIR == 1) {
+        if (P.dim == 2) euler_task<T, DIR, 2>(A, P, S, nf, sm, lane, lt);
+        else euler_task<T, DIR, 3>(A, P, S, nf, sm, lane, lt);
+      } else {
+        euler_task<T, DIR, 3>(A, P, S, nf, sm, lane, lt);
+      }
+    }
+  }
+}
+
+// ----------------------------------------------------------- step control --
+
+// upload: primitive (FP64, staging) -> conserved state, plus the wave speed and
+// entropy of that primitive state (prim_to_con, enflo/src/fv.cc:405-416)
+template <typename T>
+__global__ void k_upload(const ProbDev* prob, ProbState* st, int p, const double* prim, T* U, long long ctot) {
+  const ProbDev& P = prob[p];
+  ProbState& S = st[p];
+  long long n = (long long)P.nx * P.ny * P.nz;
+  double smax = 0.0, ent = 0.0;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    if (P.is_scalar) {
+      double u = prim[c];
+      U[P.off + c] = T(u);
+      double sp = (P.model == DSPW_LINADV) ? P.lin_speed : fabs(u);
+      if (sp > smax) smax = sp;
+      ent += 0.5 * u * u;
+    } else {
+      double pd[5];
+      for (int v = 0; v < 5; v++) pd[v] = prim[v * n + c];
+      T pp[5], u[5];
+      for (int v = 0; v < 5; v++) pp[v] = T(pd[v]);
+      prim_to_cons<T>(pp, T(P.gamma), u);
+      store_cons<T>(U, ctot, P.off + c, P.nv, u);
+      double sp = wave_speed<double>(P, pd);
+      if (sp > smax) smax = sp;
+      double s = ::log(pd[4]) - P.gamma * ::log(pd[0]);
+      ent += -pd[0] * s / (P.gamma - 1.0);
+    }
+  }
+  unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
+  warp_max_u64_lane0(sb);
+  double es = warp_sum(ent);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&S.smax, sb);
+    atomicAdd(&S.ent_acc, es);
+  }
+}
+
+// wave-speed max of the current state (dspw_compute_dt)
+template <typename T>
+__global__ void k_speed(const ProbDev* prob, ProbState* st, int p, const T* U, long long ctot, double* out) {
+  const ProbDev& P = prob[p];
+  long long n = (long long)P.nx * P.ny * P.nz;
+  double smax = 0.0;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    T pr[5];
+    if (P.is_scalar) { pr[0] = U[P.off + c]; pr[1] = pr[2] = pr[3] = pr[4] = T(0); }
+    else {
+      T u[5];
+      load_cons<T>(U, ctot, P.off + c, P.nv, P.dim, u);
+      cons_to_prim<T>(u, T(P.gamma), pr);
+    }
+    double sp = wave_speed<T>(P, pr);
+    if (sp > smax) smax = sp;
+  }
+  unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
+  warp_max_u64_lane0(sb);
+  if ((threadIdx.x & 31) == 0) atomicMax((unsigned long long*)out, sb);
+  (void)st;
+}
+
+// conserved / primitive state of one problem to FP64 staging (download)
+template <typename T>
+__global__ void k_download(const ProbDev* prob, int p, const T* U, long long ctot, double* out, int prim) {
+  const ProbDev& P = prob[p];
+  long long n = (long long)P.nx * P.ny * P.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    if (P.is_scalar) { out[c] = (double)U[P.off + c]; continue; }
+    T u[5];
+    load_cons<T>(U, ctot, P.off + c, P.nv, P.dim, u);
+    if (prim) {
+      T pr[5];
+      cons_to_prim<T>(u, T(P.gamma), pr);
+      for (int v = 0; v < 5; v++) out[v * n + c] = (double)pr[v];
+    } else {
+      for (int v = 0; v < 5; v++) out[v * n + c] = (double)u[v];
+    }
+  }
+}
+
+// FP64 sums for dspw_globals: entropy (enflo/src/compute_global.cc:18-28 /
+// enflo_scalar/src_scalar/compute_global.cc:12-21), conserved totals, kinetic energy
+template <typename T>
+__global__ void k_globals(const ProbDev* prob, int p, const T* U, long long ctot, double* acc /* 7 */) {
+  const ProbDev& P = prob[p];
+  long long n = (long long)P.nx * P.ny * P.nz;
+  double e = 0, ke = 0, tot[5] = {0, 0, 0, 0, 0};
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    if (P.is_scalar) {
+      double u = U[P.off + c];
+      e += 0.5 * u * u;
+      tot[0] += u;
+    } else {
+      T u[5], pr[5];
+      load_cons<T>(U, ctot, P.off + c, P.nv, P.dim, u);
+      cons_to_prim<T>(u, T(P.gamma), pr);
+      double rho = pr[0], prs = pr[4];
+      double s = ::log(prs) - P.gamma * ::log(rho);
+      e += -rho * s / (P.gamma - 1.0);
+      ke += 0.5 * rho * ((double)pr[1] * pr[1] + (double)pr[2] * pr[2] + (double)pr[3] * pr[3]);
+      for (int v = 0; v < 5; v++) tot[v] += (double)u[v];
+    }
+  }
+  e = warp_sum(e); ke = warp_sum(ke);
+  for (int v = 0; v < 5; v++) tot[v] = warp_sum(tot[v]);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(acc + 0, e);
+    atomicAdd(acc + 1, ke);
+    for (int v = 0; v < 5; v++) atomicAdd(acc + 2 + v, tot[v]);
+  }
+}
+
+// L1 / L2^2 / Linf of (component comp of the primitive state) - exact
+template <typename T>
+__global__ void k_errors(const ProbDev* prob, int p, const T* U, long long ctot, int comp, const double* exact,
+                         double* acc /* 3 */) {
+  const ProbDev& P = prob[p];
+  long long n = (long long)P.nx * P.ny * P.nz;
+  double l1 = 0, l2 = 0, li = 0;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    double v;
+    if (P.is_scalar) v = U[P.off + c];
+    else {
+      T u[5], pr[5];
+      load_cons<T>(U, ctot, P.off + c, P.nv, P.dim, u);
+      cons_to_prim<T>(u, T(P.gamma), pr);
+      v = pr[comp];
+    }
+    double d = fabs(exact[c] - v);
+    l1 += d; l2 += d * d; li = fmax(li, d);
+  }
+  l1 = warp_sum(l1); l2 = warp_sum(l2);
+  for (int o = 16; o > 0; o >>= 1) li = fmax(li, __shfl_xor_sync(0xffffffffu, li, o));
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(acc + 0, l1);
+    atomicAdd(acc + 1, l2);
+    atomicMax((unsigned long long*)(acc + 2), (unsigned long long)__double_as_longlong(li));
+  }
+}
+
+// ---------------------------------------------------- Navier-Stokes (ES) --
+
+// entropy variables of every cell (input of the node stencil)
+template <typename T>
+__global__ void k_entvars(const ProbDev* prob, int nprob, const long long* cell_start, const T* U, long long ctot,
+                          T* Vout) {
+  long long total = cell_start[nprob];
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_start[mid] <= g) lo = mid; else hi = mid - 1; }
+    const ProbDev& P = prob[lo];
+    if (P.model != DSPW_NS_ES) continue;
+    T u[5], pr[5], v[5];
+    load_cons<T>(U, ctot, g, P.nv, P.dim, u);
+    cons_to_prim<T>(u, T(P.gamma), pr);
+    prim_to_ent<T>(pr, T(P.gamma), v);
+    for (int c = 0; c < 5; c++) Vout[c * ctot + g] = v[c];
+  }
+}
+
+// nodal_vlux_ES (enflo/src/vflux_ES.cc:15-151) for the node between cells
+// (i..i+1, j..j+1, k..k+1), periodic; writes 15 values (x, y, z fluxes).
+// The y flux keeps only its K22,K23 terms and the z flux only K33 because the
+// reference overwrites the earlier accumulations.
+template <typename T>
+__global__ void k_visc_nodes(const ProbDev* prob, int nprob, const long long* cell_start, const T* V, long long ctot,
+                             T* node) {
+  typedef Mth<T> m;
+  long long total = cell_start[nprob];
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_start[mid] <= g) lo = mid; else hi = mid - 1; }
+    const ProbDev& P = prob[lo];
+    if (P.model != DSPW_NS_ES) continue;
+    long long l = g - P.off;
+    int i = (int)(l % P.nx), j = (int)((l / P.nx) % P.ny), k = (int)(l / ((long long)P.nx * P.ny));
+    int i1 = (i + 1) % P.nx, j1 = (j + 1) % P.ny, k1 = (k + 1) % P.nz;
+#define VC(c, ii, jj, kk) V[(c) * ctot + P.off + ((long long)(kk) * P.ny + (jj)) * P.nx + (ii)]
+    const T f1 = T(1.0 / 8.0);
+    const T fx = m::div(T(1.0 / 4.0), T(P.dx)), fy = m::div(T(1.0 / 4.0), T(P.dy)), fz = m::div(T(1.0 / 4.0), T(P.dz));
+    T avg[5], Tx[5], Ty[5], Tz[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+      T v111 = VC(c, i1, j1, k1), v011 = VC(c, i, j1, k1), v101 = VC(c, i1, j, k1), v110 = VC(c, i1, j1, k);
+      T v001 = VC(c, i, j, k1), v010 = VC(c, i, j1, k), v100 = VC(c, i1, j, k), v000 = VC(c, i, j, k);
+      avg[c] = v111 * f1 + v011 * f1 + v101 * f1 + v110 * f1;
+      avg[c] += v001 * f1 + v010 * f1 + v100 * f1 + v000 * f1;
+      Tx[c] = v111 * fx + v110 * fx + v101 * fx + v100 * fx;
+      Tx[c] += v011 * -fx + v010 * -fx + v001 * -fx + v000 * -fx;
+      Ty[c] = v111 * fy + v110 * fy + v011 * fy + v010 * fy;
+      Ty[c] += v101 * -fy + v100 * -fy + v001 * -fy + v000 * -fy;
+      Tz[c] = v111 * fz + v101 * fz + v011 * fz + v001 * fz;
+      Tz[c] += v110 * -fz + v100 * -fz + v010 * -fz + v000 * -fz;
+    }
+#undef VC
+    double Td = -1 / (double)avg[4] / P.gas_const;
+    T mu = T(viscosity(P, Td));
+    T kappa = m::div(mu * T(P.Cp), T(P.prandtl));
+    T c1 = m::div(T(4.0) * mu, T(3.0)), c2 = m::div(T(-2.0) * mu, T(3.0)), c3 = m::div(kappa, T(P.gas_const));
+    T e4 = m::div(T(1.0), avg[4]);
+    T e1 = avg[1] * e4, e2 = avg[2] * e4, e3 = avg[3] * e4;
+    T xf[5], yf[5], zf[5];
+    xf[0] = T(0.0);
+    xf[1] = c1 * e4 * (-Tx[1] + e1 * Tx[4]);
+    xf[2] = mu * e4 * (-Tx[2] + e2 * Tx[4]);
+    xf[3] = mu * e4 * (-Tx[3] + e3 * Tx[4]);
+    xf[4] = e4 * (c1 * e1 * Tx[1] + mu * e2 * Tx[2] + mu * e3 * Tx[3] +
+                  (-c1 * e1 * e1 - mu * (e2 * e2 + e3 * e3) + c3 * e4) * Tx[4]);
+    xf[1] += c2 * e4 * (-Ty[2] + e2 * Ty[4]);
+    xf[2] += mu * e4 * (-Ty[1] + e1 * Ty[4]);
+    xf[4] += e4 * (mu * e2 * Ty[1] + c2 * e1 * Ty[2] - (mu + c2) * e1 * e2 * Ty[4]);
+    xf[1] += c2 * e4 * (-Tz[3] + e3 * Tz[4]);
+    xf[3] += mu * e4 * (-Tz[1] + e1 * Tz[4]);
+    xf[4] += e4 * (mu * e3 * Tz[1] + c2 * e1 * Tz[3] - (mu + c2) * e1 * e3 * Tz[4]);
+    yf[0] = T(0.0);
+    yf[1] = mu * e4 * (-Ty[1] + e1 * Ty[4]);
+    yf[2] = c1 * e4 * (-Ty[2] + e2 * Ty[4]);
+    yf[3] = mu * e4 * (-Ty[3] + e3 * Ty[4]);
+    yf[4] = e4 * (mu * e1 * Ty[1] + c1 * e2 * Ty[2] + mu * e3 * Ty[3] +
+                  (-c1 * e2 * e2 - mu * (e1 * e1 + e3 * e3) + c3 * e4) * Ty[4]);
+    yf[2] += c2 * e4 * (-Tz[3] + e3 * Tz[4]);
+    yf[3] += mu * e4 * (-Tz[2] + e2 * Tz[4]);
+    yf[4] += e4 * (mu * e3 * Tz[2] + c2 * e2 * Tz[3] - (mu + c2) * e2 * e3 * Tz[4]);
+    zf[0] = T(0.0);
+    zf[1] = mu * e4 * (-Tz[1] + e1 * Tz[4]);
+    zf[2] = mu * e4 * (-Tz[2] + e2 * Tz[4]);
+    zf[3] = c1 * e4 * (-Tz[3] + e3 * Tz[4]);
+    zf[4] = e4 * (mu * e1 * Tz[1] + mu * e2 * Tz[2] + c1 * e3 * Tz[3] +
+                  (-c1 * e3 * e3 - mu * (e1 * e1 + e2 * e2) + c3 * e4) * Tz[4]);
+    T ax = -(T(P.dy) * T(P.dz)), ay = -(T(P.dx) * T(P.dz)), az = -(T(P.dx) * T(P.dy));
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+      node[(0 + c) * ctot + g] = xf[c] * ax;
+      node[(5 + c) * ctot + g] = yf[c] * ay;
+      node[(10 + c) * ctot + g] = zf[c] * az;
+    }
+  }
+}
+
+// Add the viscous residual of each cell from its 8 corner nodes (scatter of
+// compute_visc_residual, enflo/src/fv.cc:786-1157, as a gather) and apply the
+// stage update.  Nodes at a domain edge (two coordinates on the boundary
+// node layer) are counted twice, as the reference's loops visit them twice.
+template <typename T>
+__global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const T* node) {
+  long long total = cell_start[A.nprob];
+  double smax = 0.0, ent = 0.0;
+  unsigned bad_fin = 0, bad_pos = 0;
+  int pcur = -1;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = A.nprob - 1;
+    while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_start[mid] <= g) lo = mid; else hi = mid - 1; }
+    const ProbDev& P = A.prob[lo];
+    if (P.model != DSPW_NS_ES) continue;
+    ProbState& S = A.st[lo];
+    if (!A.residual_only && !S.active) continue;
+    pcur = lo;
+    long long l = g - P.off;
+    int I = (int)(l % P.nx), J = (int)((l / P.nx) % P.ny), K = (int)(l / ((long long)P.nx * P.ny));
+    T R[5];
+    load_cons<T>(A.R, A.ctot, g, P.nv, P.dim, R);
+#pragma unroll
+    for (int a = 1; a >= 0; a--)
+#pragma unroll
+      for (int b = 1; b >= 0; b--)
+#pragma unroll
+        for (int c = 1; c >= 0; c--) {
+          // node position relative to the cell: i = I - 1 + a (a = 1: right node)
+          int ni = I - 1 + a, nj = J - 1 + b, nk = K - 1 + c;
+          int onb = (ni == -1 || ni == P.nx - 1) + (nj == -1 || nj == P.ny - 1) + (nk == -1 || nk == P.nz - 1);
+          int mult = (onb == 2) ? 2 : 1;
+          int pi = (ni + P.nx) % P.nx, pj = (nj + P.ny) % P.ny, pk = (nk + P.nz) % P.nz;
+          long long ng = P.off + ((long long)pk * P.ny + pj) * P.nx + pi;
+          const T cx = a ? T(0.25) : T(-0.25), cy = b ? T(0.25) : T(-0.25), cz = c ? T(0.25) : T(-0.25);
+          for (int rep = 0; rep < mult; rep++) {
+#pragma unroll
+            for (int v = 0; v < 5; v++)
+              R[v] += node[v * A.ctot + ng] * cx + node[(5 + v) * A.ctot + ng] * cy + node[(10 + v) * A.ctot + ng] * cz;
+          }
+        }
+    if (A.residual_only) { store_cons<T>(A.R, A.ctot, g, P.nv, R); continue; }
+    T u[5], un[5];
+    load_cons<T>(A.Uin, A.ctot, g, P.nv, P.dim, u);
+    load_cons<T>(A.Un, A.ctot, g, P.nv, P.dim, un);
+    const T a = T(A.a_rk), b = T(A.b_rk), c2 = T(-S.factor * A.b_rk);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      u[v] *= b;
+      u[v] += un[v] * a + R[v] * c2;
+    }
+    store_cons<T>(A.Uout, A.ctot, g, P.nv, u);
+    if (A.final_stage) {
+      T p[5];
+      cons_to_prim<T>(u, T(P.gamma), p);
+      double sp = wave_speed<T>(P, p);
+      if (sp > smax) smax = sp;
+      double rho = p[0], pr = p[4];
+      if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
+      if (!isfinite(rho) || !isfinite(pr)) bad_fin++;
+      double s = ::log(pr) - P.gamma * ::log(rho);
+      ent += -rho * s / (P.gamma - 1.0);
+    }
+  }
+  // one speed-max / entropy flush per thread, warp-aggregated when the warp
+  // worked on a single problem
+  int p0 = __shfl_sync(0xffffffffu, pcur, 0);
+  bool uniform = __all_sync(0xffffffffu, pcur == p0 || pcur < 0);
+  if (A.final_stage && !A.residual_only) {
+    if (uniform) {
+      unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
+      warp_max_u64_lane0(sb);
+      double es = warp_sum(ent);
+      if ((threadIdx.x & 31) == 0 && p0 >= 0) {
+        atomicMax(&A.st[p0].smax, sb);
+        atomicAdd(&A.st[p0].ent_acc, es);
+      }
+    } else if (pcur >= 0) {
+      atomicMax(&A.st[pcur].smax, (unsigned long long)__double_as_longlong(smax));
+      atomicAdd(&A.st[pcur].ent_acc, ent);
+    }
+  }
+  if (bad_fin) { atomicAdd(&A.status->nonfinite, (unsigned long long)bad_fin); atomicCAS(&A.status->code, 0, DSPW_ERR_NONFINITE); }
+  if (bad_pos) { atomicAdd(&A.status->nonpositive, (unsigned long long)bad_pos); atomicCAS(&A.status->code, 0, DSPW_ERR_NONPOSITIVE); }
+}
+
+}  // namespace dspw

@@ -1,0 +1,37 @@
+// dspw_launch.h -- host-side launch interface shared by the precision units
+// (dspw_fp64.cu, dspw_fp32.cu) and the C ABI (dspw_capi.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "dspw_kernels.cuh"
+
+namespace dspw {
+
+template <typename T>
+struct Launch {
+  static size_t sweep_smem();
+  static cudaError_t prepare();   // kernel attributes; call outside stream capture
+  static cudaError_t sweep(int dir, const SweepArgs<T>& a, int grid, cudaStream_t s);
+  static cudaError_t upload(const ProbDev* prob, ProbState* st, int p, const double* prim, T* U, long long ctot,
+                            long long ncell, cudaStream_t s);
+  static cudaError_t speed(const ProbDev* prob, ProbState* st, int p, const T* U, long long ctot, long long ncell,
+                           double* out, cudaStream_t s);
+  static cudaError_t download(const ProbDev* prob, int p, const T* U, long long ctot, long long ncell, double* out,
+                              int prim, cudaStream_t s);
+  static cudaError_t globals(const ProbDev* prob, int p, const T* U, long long ctot, long long ncell, double* acc,
+                             cudaStream_t s);
+  static cudaError_t errors(const ProbDev* prob, int p, const T* U, long long ctot, long long ncell, int comp,
+                            const double* exact, double* acc, cudaStream_t s);
+  static cudaError_t entvars(const ProbDev* prob, int nprob, const long long* cell_start, long long ncell_total,
+                             const T* U, long long ctot, T* V, cudaStream_t s);
+  static cudaError_t visc_nodes(const ProbDev* prob, int nprob, const long long* cell_start, long long ncell_total,
+                                const T* V, long long ctot, T* node, cudaStream_t s);
+  static cudaError_t visc_update(const SweepArgs<T>& a, const long long* cell_start, long long ncell_total,
+                                 const T* node, cudaStream_t s);
+};
+
+cudaError_t launch_begin_step(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive,
+                              cudaStream_t s);
+cudaError_t launch_end_step(const ProbDev* prob, ProbState* st, int nprob, cudaStream_t s);
+cudaError_t launch_init_state(const ProbDev* prob, ProbState* st, int p, cudaStream_t s);
+
+}  // namespace dspw

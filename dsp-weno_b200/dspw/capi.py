@@ -218,6 +218,7 @@ def lib():
         "dspw_last_status": (I, [P, C.POINTER(StatusOut)]),
         "dspw_errors": (I, [P, I, I, dp, dp]),
         "dspw_sync": (I, [P]),
+        "dspw_profile_step": (I, [P, dp, C.c_char_p, I, C.POINTER(I)]),
         "dspw_stream": (P, [P]),
         "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),
         "dspw_trainer_create": (I, [C.POINTER(TrainCfg), dp, dp, C.POINTER(P)]),
@@ -322,6 +323,18 @@ class Solver:
         a = np.ascontiguousarray(exact, dtype=np.float64)
         check(lib().dspw_errors(self.h, p, comp, a, e), "dspw_errors")
         return e
+
+    def profile_step(self):
+        """Durations (ms) of every kernel launch of one un-graphed step."""
+        ms = np.zeros(64)
+        names = C.create_string_buffer(16 * 64)
+        n = C.c_int()
+        check(lib().dspw_profile_step(self.h, ms, names, 64, C.byref(n)), "dspw_profile_step")
+        raw = names.raw
+        return [(raw[16 * i:16 * i + 16].split(b"\0")[0].decode(), float(ms[i])) for i in range(n.value)]
+
+    def stream_ptr(self):
+        return lib().dspw_stream(self.h)
 
     def sync(self):
         check(lib().dspw_sync(self.h), "dspw_sync")

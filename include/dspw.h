@@ -37,6 +37,12 @@ extern "C" {
 
 #define DSPW_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define DSPW_API __attribute__((visibility("default")))
+#else
+#define DSPW_API
+#endif
+
 /* models (enflo/src/ext_constants.h:23, enflo_scalar/src_scalar/ext_constants.h:19) */
 enum dspw_model { DSPW_LINADV = 0, DSPW_BURGERS = 1, DSPW_EULER = 2, DSPW_NS_ES = 3, DSPW_NS_KEP = 4 };
 
@@ -137,57 +143,64 @@ typedef struct dspw_status_out {
   long long faces_checked;
 } dspw_status_out;
 
-const char* dspw_error_string(int code);
-int dspw_version(void);
+DSPW_API const char* dspw_error_string(int code);
+DSPW_API int dspw_version(void);
 
 /* Create a handle for one problem / for nprob independent problems advanced
  * together (one launch per kernel over all problems, per-problem dt). */
-int dspw_create(const dspw_desc* desc, dspw_handle** out);
-int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out);
-int dspw_destroy(dspw_handle* h);
+DSPW_API int dspw_create(const dspw_desc* desc, dspw_handle** out);
+DSPW_API int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out);
+DSPW_API int dspw_destroy(dspw_handle* h);
 
 /* Interior primitive state of problem p in, conserved/primitive state out. */
-int dspw_upload_prim(dspw_handle* h, int p, const double* prim);
-int dspw_download_prim(dspw_handle* h, int p, double* prim);
-int dspw_download_cons(dspw_handle* h, int p, double* cons);
+DSPW_API int dspw_upload_prim(dspw_handle* h, int p, const double* prim);
+DSPW_API int dspw_download_prim(dspw_handle* h, int p, double* prim);
+DSPW_API int dspw_download_cons(dspw_handle* h, int p, double* cons);
 
 /* CFL time step cfl*min(h)/max|speed| of the current state (FV::compute_dt). */
-int dspw_compute_dt(dspw_handle* h, int p, double* dt);
+DSPW_API int dspw_compute_dt(dspw_handle* h, int p, double* dt);
 
 /* Residual of the current state (compute_residual(rk), reference sign). */
-int dspw_residual(dspw_handle* h, int p, double* res);
+DSPW_API int dspw_residual(dspw_handle* h, int p, double* res);
 
 /* One time-integration stage rk with step dt on every problem (dt <= 0 keeps
  * the per-problem dt of the current step). */
-int dspw_stage(dspw_handle* h, int rk, double dt);
+DSPW_API int dspw_stage(dspw_handle* h, int rk, double dt);
 
 /* Up to nsteps steps of the FV::run loop body on every unfinished problem:
  * CFL dt, clipping to the next time stamp, all stages, time += dt.  With
  * fixed_dt > 0 the CFL step is replaced by fixed_dt.  Steps run as one CUDA
  * graph per step; nothing is copied to the host. */
-int dspw_step(dspw_handle* h, int nsteps, double fixed_dt);
+DSPW_API int dspw_step(dspw_handle* h, int nsteps, double fixed_dt);
 
 /* Advance every problem until final_time/max_iter, checking completion every
  * `chunk` steps.  Returns the number of steps of the longest problem. */
-int dspw_run(dspw_handle* h, int chunk, int* steps);
+DSPW_API int dspw_run(dspw_handle* h, int chunk, int* steps);
 
-int dspw_globals(dspw_handle* h, int p, dspw_globals_out* g);
-int dspw_last_status(dspw_handle* h, dspw_status_out* s);
+DSPW_API int dspw_globals(dspw_handle* h, int p, dspw_globals_out* g);
+DSPW_API int dspw_last_status(dspw_handle* h, dspw_status_out* s);
 
 /* L1/L2/Linf error of problem p against host values `exact` (same layout as
  * dspw_download_prim, component comp), volume-weighted like
  * enflo_scalar/src_scalar/compute_errors.cc:9-30. */
-int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, double err[3]);
+DSPW_API int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, double err[3]);
+
+/* Run one step outside the CUDA graph with a CUDA event pair around every
+ * kernel launch on the handle's stream and return the launch durations in
+ * milliseconds (kernel_ms, up to max_k entries, launch order: begin-step,
+ * per stage the sweeps x/y/z [and the viscous kernels], end-step) and a short
+ * name per launch (names: max_k rows of 16 chars).  For measurement only. */
+DSPW_API int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k, int* nk);
 
 /* Synchronise the handle's stream; returns the first error recorded. */
-int dspw_sync(dspw_handle* h);
+DSPW_API int dspw_sync(dspw_handle* h);
 
 /* The handle's CUDA stream (a cudaStream_t) so callers can order their own work. */
-void* dspw_stream(dspw_handle* h);
+DSPW_API void* dspw_stream(dspw_handle* h);
 
 /* Raw device pointer to the conserved state planes of problem p (component
  * stride in elements returned in *stride) and the element size in bytes (8 or 4). */
-int dspw_device_state(dspw_handle* h, int p, void** ptr, long long* stride, int* elem_bytes);
+DSPW_API int dspw_device_state(dspw_handle* h, int p, void** ptr, long long* stride, int* elem_bytes);
 
 /* ---- DSP-WENO network training (no counterpart in the reference's C++; the
  * reference trains with PyTorch in DSP-WENO_trainer/DSP-WENO_network_trainer.py) */
@@ -201,23 +214,23 @@ typedef struct dspw_train_cfg {
   int seed;
 } dspw_train_cfg;
 
-int dspw_trainer_create(const dspw_train_cfg* cfg, const double* w_init /* 4*25 */,
+DSPW_API int dspw_trainer_create(const dspw_train_cfg* cfg, const double* w_init /* 4*25 */,
                         const double* b_init /* 4*5 */, dspw_trainer** out);
-int dspw_trainer_destroy(dspw_trainer* t);
+DSPW_API int dspw_trainer_destroy(dspw_trainer* t);
 /* Device-resident data set: n samples of 4 cell values and 2 target interface
  * values (left, right), host FP64 in. */
-int dspw_trainer_set_data(dspw_trainer* t, const double* stencils /* n*4 */,
+DSPW_API int dspw_trainer_set_data(dspw_trainer* t, const double* stencils /* n*4 */,
                           const double* targets /* n*2 */, long long n);
 /* Generate stencil/target pairs on the GPU from the current state of a solver
  * handle: every face of every component contributes its 4-cell stencil and the
  * plain SP-WENO interface values as targets.  Appends up to max_pairs. */
-int dspw_trainer_collect(dspw_trainer* t, dspw_handle* h, long long max_pairs, long long* added);
+DSPW_API int dspw_trainer_collect(dspw_trainer* t, dspw_handle* h, long long max_pairs, long long* added);
 /* One epoch of minibatch Adam on the device; loss = (MSE_left + MSE_right)/2. */
-int dspw_trainer_epoch(dspw_trainer* t, double* mean_loss);
+DSPW_API int dspw_trainer_epoch(dspw_trainer* t, double* mean_loss);
 /* Loss and gradients for one explicit batch (FP64 host in/out), for checks. */
-int dspw_trainer_loss_grad(dspw_trainer* t, const double* stencils, const double* targets, int n,
+DSPW_API int dspw_trainer_loss_grad(dspw_trainer* t, const double* stencils, const double* targets, int n,
                            double* loss, double* grad_w /* 4*25 */, double* grad_b /* 4*5 */);
-int dspw_trainer_get_params(dspw_trainer* t, double* w /* 4*25 */, double* b /* 4*5 */);
+DSPW_API int dspw_trainer_get_params(dspw_trainer* t, double* w /* 4*25 */, double* b /* 4*5 */);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,67 @@
+"""libdspw.so loads without a GPU and exports every entry point that
+include/dspw.h declares; the ctypes descriptor matches the C layout."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from dspw import capi
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    text = (REPO / "include" / "dspw.h").read_text()
+    return sorted(set(re.findall(r"DSPW_API\s+[\w\s\*]+?\b(dspw_\w+)\s*\(", text)))
+
+
+def test_header_declares_api():
+    names = declared_functions()
+    assert "dspw_create" in names and "dspw_step" in names and len(names) >= 20
+
+
+def test_library_exports_every_declared_symbol():
+    if not capi.LIB_PATH.exists():
+        pytest.fail("libdspw.so is not built; run __graft_entry__.build()")
+    lib = ctypes.CDLL(str(capi.LIB_PATH))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert lib.dspw_version() == capi.ABI_VERSION
+
+
+def test_error_strings():
+    lib = capi.lib()
+    for code in range(9):
+        s = lib.dspw_error_string(code).decode()
+        assert s.startswith(capi.STATUS[code])
+
+
+def test_descriptor_layout():
+    # offsets of the C struct (x86-64 SysV): 23 ints + 8 reserved ints, then doubles
+    d = capi.Desc
+    assert d.xmin.offset == 4 * (15 + 8 + 8) + 4 * 0 or d.xmin.offset % 8 == 0
+    assert ctypes.sizeof(capi.Desc) == d.reserved_d.offset + 8 * 8
+
+
+def test_bad_descriptor_rejected_without_gpu():
+    """Descriptor validation runs on the host before any CUDA call."""
+    lib = capi.lib()
+    d = capi.make_desc(nx=0)
+    h = ctypes.c_void_p()
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d = capi.make_desc(model="ns_es", nx=8, ny=8, nz=8, mu_ref=0.0)
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d = capi.make_desc(bc=["periodic", "wall", "periodic", "periodic", "periodic", "periodic"])
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d = capi.make_desc()
+    d.abi_version = 99
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+
+
+def test_network_file_roundtrip(tmp_path):
+    W, b = capi.load_network_file(REPO / "tests" / "golden" / "dsp_weno.txt")
+    assert W.shape == (4, 5, 5) and b.shape == (4, 5)
+    capi.save_network_file(tmp_path / "n.txt", W, b)
+    W2, b2 = capi.load_network_file(tmp_path / "n.txt")
+    assert (W2 == W).all() and (b2 == b).all()

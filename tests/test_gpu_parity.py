@@ -1,0 +1,181 @@
+"""CUDA stage path (libdspw.so, FP64 plain form) against the reference.
+
+* golden runs: the reference's own IC and final state (tests/golden/runs.npz),
+  same mesh layout as the reference (1-D/2-D problems carry Ny=Nz=2);
+* reduced layouts (Ny=Nz=1 for 1-D, Nz=1 for 2-D) against the oracle;
+* the residual of random states against the oracle, all fluxes/reconstructions;
+* config-1 OOC errors against the reference's printed L1 values.
+
+Tolerance: the FP64 kernels keep the reference's operation order and are built
+without FMA contraction; CUDA's log/exp/tanh/pow differ from glibc by ulps, so
+states are compared per cell at 1e-12 relative (floor 1e-9 of the component's
+magnitude for near-zero entries)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from _common import desc_from_cfg, load, net, run_cases
+from dspw import Solver, make_desc
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def assert_state_close(got, ref, rtol=RTOL, what=""):
+    got = np.asarray(got); ref = np.asarray(ref)
+    assert got.shape == ref.shape
+    for c in range(ref.shape[0]):
+        scale = np.max(np.abs(ref[c]))
+        tol = rtol * np.maximum(np.abs(ref[c]), 1e-3 * scale) + 1e-300
+        err = np.abs(got[c] - ref[c])
+        bad = err > tol
+        assert not bad.any(), (f"{what} comp {c}: {bad.sum()} cells off, max rel "
+                               f"{np.max(err / np.maximum(np.abs(ref[c]), 1e-3 * scale + 1e-300)):.3e}")
+
+
+@pytest.mark.parametrize("case", run_cases(), ids=lambda c: c[0])
+def test_golden_run_fp64(case):
+    name, kind, cfg, nsteps, fixed_dt = case
+    g = load("runs.npz")
+    p0 = g[f"{name}|prim0"]
+    _, nz, ny, nx = p0.shape
+    s = Solver(desc_from_cfg(cfg, nx, ny, nz))
+    s.upload_prim(p0)
+    s.step(nsteps, fixed_dt)
+    gl = s.globals()
+    tid = g[f"{name}|tid"]
+    assert gl.iter == int(tid[1])
+    assert abs(gl.time - tid[0]) <= 1e-12 * abs(tid[0])
+    ref = g[f"{name}|final"]
+    got = s.cons()
+    if kind == "S":
+        got = got.reshape(ref.shape)
+    assert_state_close(got, ref, what=name)
+    st = s.status()
+    assert st.code == 0 and st.nonfinite_cells == 0 and st.nonpositive_cells == 0
+
+
+REDUCED = ["linadv_sp_weno", "linadv_sp_weno_dl", "burgers_wenoc", "shuosher_sp_weno", "shuosher_sp_weno_dl",
+           "kh_sp_weno", "kh_sp_weno_dl", "wall2d", "vortex"]
+
+
+@pytest.mark.parametrize("name", REDUCED)
+def test_reduced_layout_vs_oracle(name):
+    """True 1-D (Ny=Nz=1) and 2-D (Nz=1) layouts skip the degenerate sweeps;
+    they agree with the oracle run on the same layout."""
+    case = [c for c in run_cases() if c[0] == name][0]
+    _, kind, cfg, nsteps, fixed_dt = case
+    g = load("runs.npz")
+    p0 = g[f"{name}|prim0"]
+    nv, nz, ny, nx = p0.shape
+    ny2 = 1 if ny == 2 else ny
+    p0r = np.ascontiguousarray(p0[:, :1, :ny2, :])
+    d = desc_from_cfg(cfg, nx, ny2, 1)
+    o = O.Oracle(d); o.set_prim(p0r); o.step(nsteps, fixed_dt)
+    s = Solver(d); s.upload_prim(p0r); s.step(nsteps, fixed_dt)
+    assert s.globals().iter == o.time()[1]
+    assert_state_close(s.cons(), o.cons(), rtol=1e-11, what=name)
+
+
+FLUXES = ["kepes_tecno4_roe", "kepes_tecno_roe", "kepes_tecno4_rusanov", "kepes_tecno_rusanov", "kep_tecno_roe",
+          "roe_tecno_roe", "roe_tecno4_roe", "kepec4", "kepec", "kep", "kep4", "roe_ec", "roe_ec4"]
+
+
+def random_state(rng, nx, ny, nz, smooth=True):
+    x = np.linspace(0, 2 * np.pi, nx, endpoint=False)[None, None, :]
+    y = np.linspace(0, 2 * np.pi, ny, endpoint=False)[None, :, None]
+    z = np.linspace(0, 2 * np.pi, nz, endpoint=False)[:, None, None]
+    p = np.zeros((5, nz, ny, nx))
+    p[0] = 1.0 + 0.3 * np.sin(x + 2 * y + z) + 0.05 * rng.standard_normal((nz, ny, nx)) * (not smooth)
+    p[1] = 0.5 * np.cos(x - y)
+    p[2] = 0.3 * np.sin(2 * x) * (ny > 1)
+    p[3] = 0.2 * np.cos(z + x) * (nz > 1)
+    p[4] = 1.0 + 0.2 * np.cos(x + y - z)
+    return p
+
+
+@pytest.mark.parametrize("flux", FLUXES)
+@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_corr2", "sp_weno_dl"])
+@pytest.mark.parametrize("dims", [(24, 1, 1), (16, 12, 1), (8, 6, 5)])
+def test_residual_vs_oracle(flux, recon, dims):
+    if "tecno" not in flux and recon != "sp_weno":
+        pytest.skip("central fluxes do not reconstruct")
+    rng = np.random.default_rng(hash((flux, recon, dims)) % 2**32)
+    nx, ny, nz = dims
+    bc = ["wall", "wall", "neumann", "neumann", "periodic", "periodic"]
+    d = make_desc(model="euler", flux=flux, recon=recon, nx=nx, ny=ny, nz=nz, bc=bc, ec1_fix="roe" in flux,
+                  network=net(), x=(0, 1), y=(0, 0.7), z=(0, 0.5))
+    p = random_state(rng, nx, ny, nz, smooth=False)
+    o = O.Oracle(d); o.set_prim(p)
+    s = Solver(d); s.upload_prim(p)
+    ro = o.residual()
+    rg = s.residual()
+    nvs = 3 if nz == 1 and ny == 1 else (4 if nz == 1 else 5)
+    comps = [0, 1, 4] if nvs == 3 else ([0, 1, 2, 4] if nvs == 4 else [0, 1, 2, 3, 4])
+    # the oracle sweeps the degenerate directions too: only rounding-level terms
+    assert_state_close(rg[comps], ro[comps], rtol=1e-11, what=f"{flux}/{recon}/{dims}")
+
+
+@pytest.mark.parametrize("model,flux", [("linadv", "lin_tecno4"), ("linadv", "lin_tecno"), ("linadv", "lin_ec4"),
+                                        ("burgers", "bur_tecno4"), ("burgers", "bur_tecno"), ("burgers", "bur_ec")])
+@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_dl"])
+@pytest.mark.parametrize("bc", ["periodic", "wall", "neumann"])
+def test_scalar_residual_vs_oracle(model, flux, recon, bc):
+    nx = 40
+    d = make_desc(model=model, flux=flux, recon=recon, nx=nx, ny=1, nz=1, bc=[bc, bc, "periodic", "periodic",
+                  "periodic", "periodic"], x=(-np.pi, np.pi), lin_vel=(1.3, 0, 0), network=net())
+    x = -np.pi + (np.arange(nx) + 0.5) * 2 * np.pi / nx
+    u = (np.sin(x) + 0.3 * np.sign(x - 0.5)).reshape(1, 1, 1, nx)
+    o = O.Oracle(d); o.set_prim(u)
+    s = Solver(d); s.upload_prim(u)
+    assert_state_close(s.residual(), o.residual(), rtol=1e-12, what=f"{model}/{flux}/{recon}/{bc}")
+
+
+def test_ooc_config1_fp64():
+    """LinAdvTest2 (config 1): L1 errors at Nx=100,200,400 equal the reference's."""
+    g = load("ooc.npz")
+    for recon in ("sp_weno", "sp_wenoc", "sp_weno_dl"):
+        for lvl, nx in enumerate((100, 200, 400)):
+            d = make_desc(model="linadv", flux="lin_tecno4", recon=recon, nx=nx, ny=1, nz=1, x=(-np.pi, np.pi),
+                          cfl=0.5, final_time=0.5, t_stamps=5, network=net())
+            x = -np.pi + 0.5 * (2 * np.pi / nx) + np.arange(nx) * (2 * np.pi / nx)
+            s = Solver(d)
+            s.upload_prim(np.sin(x).reshape(1, 1, 1, nx) ** 4)
+            s.run(chunk=64)
+            t = s.globals().time
+            e = s.errors(np.sin(x - t) ** 4)
+            ref = g[recon][lvl]
+            assert abs(e[0] - ref[0]) <= 1e-9 * ref[0], (recon, nx, e, ref)
+
+
+def test_batch_equals_single():
+    """Problems of different size and model in one batch give the same bits as
+    each problem alone."""
+    rng = np.random.default_rng(3)
+    ds = [make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=50, ny=1, nz=1, bc="periodic"),
+          make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=20, ny=18, nz=1, bc="periodic"),
+          make_desc(model="burgers", flux="bur_tecno4", recon="sp_weno", nx=77, ny=1, nz=1, x=(-np.pi, np.pi))]
+    states = [random_state(rng, 50, 1, 1), random_state(rng, 20, 18, 1),
+              np.sin(np.linspace(-np.pi, np.pi, 77, endpoint=False)).reshape(1, 1, 1, 77)]
+    b = Solver(ds)
+    for p, st in enumerate(states):
+        b.upload_prim(st, p)
+    b.step(7)
+    for p, (d, st) in enumerate(zip(ds, states)):
+        s = Solver(d)
+        s.upload_prim(st)
+        s.step(7)
+        assert np.array_equal(b.cons(p), s.cons()), p
+
+
+def test_conservation_periodic():
+    d = make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno_dl", nx=32, ny=32, nz=1, network=net())
+    s = Solver(d)
+    s.upload_prim(random_state(np.random.default_rng(0), 32, 32, 1))
+    g0 = s.globals()
+    s.step(20)
+    g1 = s.globals()
+    for v in (0, 1, 2, 4):
+        assert abs(g1.conserved[v] - g0.conserved[v]) <= 1e-12 * max(1.0, abs(g0.conserved[v]))
+    assert g1.total_entropy <= g0.total_entropy * (1 + 1e-13)
