@@ -262,6 +262,30 @@ ProbDev make_prob(const dspw_desc& d, long long off) {
   return P;
 }
 
+NetParams make_net(const dspw_desc& dn) {
+  NetParams np;
+  memset(&np, 0, sizeof(np));
+  for (int l = 0; l < 4; l++)
+    for (int j = 0; j < 5; j++) {
+      np.b[l][j] = dn.nn_b[l][j];
+      np.bf[l][j] = (float)dn.nn_b[l][j];
+      for (int k = 0; k < 5; k++) {
+        np.w[l][j][k] = dn.nn_w[l][j][k];
+        np.wf[l][j][k] = (float)dn.nn_w[l][j][k];
+      }
+    }
+  // reserved_i[0] != 0: the network carries a training box of its inputs,
+  // upper bounds of the three delta features in reserved_d[2..4] (the tanh
+  // features are always in [-1, 1]); inputs outside use plain SP-WENO
+  np.use_box = dn.reserved_i[0];
+  for (int k = 0; k < 5; k++) { np.feat_lo[k] = -1e30f; np.feat_hi[k] = 1e30f; }
+  if (np.use_box) {
+    for (int k = 0; k < 2; k++) { np.feat_lo[k] = -1.0f; np.feat_hi[k] = 1.0f; }
+    for (int k = 2; k < 5; k++) { np.feat_lo[k] = 0.0f; np.feat_hi[k] = (float)dn.reserved_d[k]; }
+  }
+  return np;
+}
+
 int tasks_for(const ProbDev& P, int dir) {
   if (dir >= P.dim) return 0;
   int N[3] = {P.nx, P.ny, P.nz};
@@ -373,6 +397,11 @@ int check_p(dspw_handle* h, int p) { return (!h || p < 0 || p >= h->nprob) ? DSP
 
 }  // namespace
 
+namespace dspw {
+ProbDev make_prob_public(const dspw_desc& d, long long off) { return make_prob(d, off); }
+NetParams make_net_public(const dspw_desc& d) { return make_net(d); }
+}  // namespace dspw
+
 // ------------------------------------------------------------------ C ABI --
 
 extern "C" {
@@ -435,28 +464,10 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
     }
   }
   // network parameters (shared by the batch; taken from the first DL problem)
-  NetParams np;
-  memset(&np, 0, sizeof(np));
   const dspw_desc* dnet = &descs[0];
   for (int p = 0; p < nprob; p++)
     if (descs[p].recon == DSPW_REC_SP_WENO_DL) { dnet = &descs[p]; break; }
-  for (int l = 0; l < 4; l++)
-    for (int j = 0; j < 5; j++) {
-      np.b[l][j] = dnet->nn_b[l][j];
-      np.bf[l][j] = (float)dnet->nn_b[l][j];
-      for (int k = 0; k < 5; k++) {
-        np.w[l][j][k] = dnet->nn_w[l][j][k];
-        np.wf[l][j][k] = (float)dnet->nn_w[l][j][k];
-      }
-    }
-  // reserved_d[0..4] / [5..7] + reserved_i[0]: optional training box of the network inputs
-  np.use_box = dnet->reserved_i[0];
-  for (int k = 0; k < 5; k++) { np.feat_lo[k] = -1e30f; np.feat_hi[k] = 1e30f; }
-  if (np.use_box) {
-    for (int k = 0; k < 5; k++) np.feat_hi[k] = (float)dnet->reserved_d[k];
-    for (int k = 0; k < 2; k++) np.feat_lo[k] = -1.0f;
-    for (int k = 2; k < 5; k++) np.feat_lo[k] = 0.0f;
-  }
+  NetParams np = make_net(*dnet);
   int ret = DSPW_OK;
 #define CKC(x)                                   \
   do {                                           \
@@ -739,6 +750,46 @@ int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k,
   cudaEventDestroy(e0);
   if (nk) *nk = n;
   return r;
+}
+
+int dspw_reconstruct_batch(const dspw_desc* d, const double* u4, long long n, double* recl, double* recr,
+                           long long* limiter_acts) {
+  if (!d || !u4 || !recl || !recr || n < 0) return DSPW_ERR_ARG;
+  if (d->recon < DSPW_REC_SP_WENO || d->recon > DSPW_REC_SP_WENO_DL) return DSPW_ERR_UNSUPPORTED;
+  if (d->precision != DSPW_FP64 && d->precision != DSPW_FP32_BF16) return DSPW_ERR_ARG;
+  if (n == 0) return DSPW_OK;
+  ProbDev P = make_prob(*d, 0);
+  NetParams np = make_net(*d);
+  ProbDev* dp = nullptr;
+  NetParams* dn = nullptr;
+  double *du = nullptr, *dl = nullptr, *dr = nullptr;
+  unsigned long long* dacts = nullptr;
+  unsigned long long acts = 0;
+  int ret = DSPW_OK;
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return DSPW_ERR_CUDA;
+  if (cudaMalloc(&dp, sizeof(P)) != cudaSuccess || cudaMalloc(&dn, sizeof(np)) != cudaSuccess ||
+      cudaMalloc(&du, sizeof(double) * 4 * n) != cudaSuccess || cudaMalloc(&dl, sizeof(double) * n) != cudaSuccess ||
+      cudaMalloc(&dr, sizeof(double) * n) != cudaSuccess || cudaMalloc(&dacts, sizeof(acts)) != cudaSuccess) {
+    ret = DSPW_ERR_NOMEM;
+  } else {
+    cudaError_t e = cudaMemcpyAsync(dp, &P, sizeof(P), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dn, &np, sizeof(np), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(du, u4, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dacts, 0, sizeof(acts), s);
+    if (e == cudaSuccess)
+      e = d->precision == DSPW_FP64 ? Launch<double>::recon_batch(dp, dn, du, n, dl, dr, dacts, s)
+                                    : Launch<float>::recon_batch(dp, dn, du, n, dl, dr, dacts, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(recl, dl, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(recr, dr, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&acts, dacts, sizeof(acts), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) ret = DSPW_ERR_CUDA;
+  }
+  if (limiter_acts) *limiter_acts = (long long)acts;
+  cudaFree(dp); cudaFree(dn); cudaFree(du); cudaFree(dl); cudaFree(dr); cudaFree(dacts);
+  cudaStreamDestroy(s);
+  return ret;
 }
 
 int dspw_sync(dspw_handle* h) {

@@ -1209,4 +1209,32 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
   if (bad_pos) { atomicAdd(&A.status->nonpositive, (unsigned long long)bad_pos); atomicCAS(&A.status->code, 0, DSPW_ERR_NONPOSITIVE); }
 }
 
+// Reconstruction of a batch of independent 4-cell stencils with the same
+// device code as the sweeps (SP-WENO family or DSP-WENO, FP64 or FP32 with the
+// BF16 tensor-core network).  Used to check the reconstruction face by face.
+template <typename T>
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32)
+k_recon_batch(const ProbDev* prob, const NetParams* net, const double* u4, long long n, double* l, double* r,
+              unsigned long long* acts) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem<T>* sm = reinterpret_cast<WarpSmem<T>*>(smem_raw) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  NetFrag nf;
+  if (sizeof(T) == 4) net_frag_load(*net, lane, nf);
+  const long long nchunk = (n + 31) / 32;
+  for (long long ch = blockIdx.x * (long long)WARPS_PER_BLOCK + (threadIdx.x >> 5); ch < nchunk;
+       ch += (long long)gridDim.x * WARPS_PER_BLOCK) {
+    long long i = ch * 32 + lane;
+    bool valid = i < n;
+    T s0 = valid ? T(u4[4 * i]) : T(0), s1 = valid ? T(u4[4 * i + 1]) : T(1);
+    T s2 = valid ? T(u4[4 * i + 2]) : T(2), s3 = valid ? T(u4[4 * i + 3]) : T(3);
+    T lo = T(0), ro = T(0);
+    int viol = 0;
+    reconstruct_lane<T>(*prob, *net, nf, sm, lane, valid, s0, s1, s2, s3, lo, ro, viol);
+    if (valid) { l[i] = (double)lo; r[i] = (double)ro; }
+    unsigned v = __reduce_add_sync(0xffffffffu, (unsigned)viol);
+    if (lane == 0 && v) atomicAdd(acts, (unsigned long long)v);
+  }
+}
+
 }  // namespace dspw

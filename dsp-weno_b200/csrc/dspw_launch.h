@@ -25,6 +25,8 @@ struct Launch {
                              const T* U, long long ctot, T* V, cudaStream_t s);
   static cudaError_t visc_nodes(const ProbDev* prob, int nprob, const long long* cell_start, long long ncell_total,
                                 const T* V, long long ctot, T* node, cudaStream_t s);
+  static cudaError_t recon_batch(const ProbDev* prob, const NetParams* net, const double* u4, long long n, double* l,
+                                 double* r, unsigned long long* acts, cudaStream_t s);
   static cudaError_t visc_update(const SweepArgs<T>& a, const long long* cell_start, long long ncell_total,
                                  const T* node, cudaStream_t s);
 };
@@ -32,6 +34,9 @@ struct Launch {
 cudaError_t launch_begin_step(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive,
                               cudaStream_t s);
 cudaError_t launch_end_step(const ProbDev* prob, ProbState* st, int nprob, cudaStream_t s);
+// host-side construction shared by the C ABI entry points
+ProbDev make_prob_public(const dspw_desc& d, long long off);
+NetParams make_net_public(const dspw_desc& d);
 cudaError_t launch_init_state(const ProbDev* prob, ProbState* st, int p, cudaStream_t s);
 
 }  // namespace dspw

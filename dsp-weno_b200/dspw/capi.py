@@ -218,6 +218,7 @@ def lib():
         "dspw_last_status": (I, [P, C.POINTER(StatusOut)]),
         "dspw_errors": (I, [P, I, I, dp, dp]),
         "dspw_sync": (I, [P]),
+        "dspw_reconstruct_batch": (I, [C.POINTER(Desc), dp, LL, dp, dp, C.POINTER(LL)]),
         "dspw_profile_step": (I, [P, dp, C.c_char_p, I, C.POINTER(I)]),
         "dspw_stream": (P, [P]),
         "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),
@@ -235,6 +236,18 @@ def lib():
         fn.argtypes = args
     _LIB = L
     return L
+
+
+def reconstruct_batch(desc: Desc, u4) -> tuple[np.ndarray, np.ndarray, int]:
+    """GPU reconstruction of stencils u4 (n, 4) with desc.recon / desc.precision."""
+    u = np.ascontiguousarray(u4, dtype=np.float64).reshape(-1, 4)
+    n = u.shape[0]
+    l = np.zeros(n)
+    r = np.zeros(n)
+    acts = C.c_longlong()
+    check(lib().dspw_reconstruct_batch(C.byref(desc), u.reshape(-1), n, l, r, C.byref(acts)),
+          "dspw_reconstruct_batch")
+    return l, r, acts.value
 
 
 class DspwError(RuntimeError):

@@ -192,6 +192,14 @@ DSPW_API int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, d
  * name per launch (names: max_k rows of 16 chars).  For measurement only. */
 DSPW_API int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k, int* nk);
 
+/* Reconstruct n independent 4-cell stencils u4[4*i..4*i+3] at their middle
+ * face with desc->recon in desc->precision, on the GPU, with the same device
+ * code as the stage kernels (reconstruct(), enflo/src/reconstruct.cc:192-239).
+ * limiter_acts receives how often the FP32 form's sign-preserving limiter
+ * acted.  Allocates its own temporary device buffers. */
+DSPW_API int dspw_reconstruct_batch(const dspw_desc* desc, const double* u4, long long n, double* recl,
+                                    double* recr, long long* limiter_acts);
+
 /* Synchronise the handle's stream; returns the first error recorded. */
 DSPW_API int dspw_sync(dspw_handle* h);
 

@@ -789,6 +789,11 @@ static void inviscid_residual(or_state* s) {
   int N[3] = {s->nx, s->ny, s->nz};
   int nv = s->nvar;
   for (int dir = 0; dir < 3; dir++) {
+    /* A direction with a single cell is not swept: the reference always
+     * carries at least two cells there (1-D and 2-D problems use Ny=Nz=2,
+     * README.md:152-160); the single-cell layout is this project's reduced
+     * form, in which the degenerate sweeps are dropped. */
+    if (N[dir] == 1) continue;
     int o1 = dir == 0 ? 1 : 0, o2 = dir == 2 ? 1 : 2;   /* the two other directions */
     for (int a = 0; a < N[o1]; a++)
       for (int b = 0; b < N[o2]; b++) {

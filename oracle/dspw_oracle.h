@@ -44,7 +44,7 @@ void or_nn_features(const double u[4], double feat[5], double vx[5], double vy[5
  * cell sizes dx,dy,dz; V[4][5] receives the entropy variables used. */
 void or_euler_face_flux(const dspw_desc* d, const double P[20], int dir, double dx, double dy,
                         double dz, double V[20], double flux[5]);
-double or_scalar_face_flux(const dspw_desc* d, const double u[4], int dir, double dx, double dy,
+double or_scalar_face_flux(const dspw_desc* d, const double* u, int dir, double dx, double dy,
                            double dz);
 
 #ifdef __cplusplus

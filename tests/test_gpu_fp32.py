@@ -1,0 +1,63 @@
+"""The FP32 form (FP32 state, fluxes, reconstruction; BF16 tensor-core
+network) against the FP64 plain form on small problems in 1-D, 2-D and 3-D:
+finite, no health errors, zero sign-property violations, and close to FP64
+(bounded by FP32/BF16 rounding of a few steps)."""
+import numpy as np
+import pytest
+
+from _common import net
+from dspw import Solver, make_desc
+
+pytestmark = pytest.mark.gpu
+
+
+def state(nx, ny, nz):
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    z = (np.arange(nz) + 0.5) / nz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    p = np.zeros((5, nz, ny, nx))
+    p[0] = 1.0 + 0.2 * np.sin(2 * np.pi * (X + Y + Z))
+    p[1] = 0.3 * np.cos(2 * np.pi * X)
+    p[2] = 0.2 * np.sin(2 * np.pi * X) * (ny > 1)
+    p[3] = 0.1 * np.cos(2 * np.pi * Y) * (nz > 1)
+    p[4] = 1.0 + 0.1 * np.cos(2 * np.pi * (X - Y))
+    return p
+
+
+@pytest.mark.parametrize("dims", [(64, 1, 1), (48, 40, 1), (16, 12, 10)])
+@pytest.mark.parametrize("recon", ["sp_weno", "sp_weno_dl"])
+def test_fp32_vs_fp64(dims, recon):
+    p = state(*dims)
+    out = {}
+    for prec in ("fp64", "fp32_bf16"):
+        d = make_desc(model="euler", flux="kepes_tecno4_roe", recon=recon, nx=dims[0], ny=dims[1], nz=dims[2],
+                      network=net(), precision=prec)
+        s = Solver(d)
+        s.upload_prim(p)
+        s.step(5)
+        st = s.status()
+        assert st.code == 0 and st.nonfinite_cells == 0, (prec, st.code, st.nonfinite_cells)
+        if prec == "fp32_bf16":
+            assert st.sign_violations <= 0.001 * dims[0] * dims[1] * dims[2] * 5 * 3
+        out[prec] = s.cons()
+    a, b = out["fp32_bf16"], out["fp64"]
+    assert np.all(np.isfinite(a))
+    rel = np.max(np.abs(a[0] - b[0])) / np.max(np.abs(b[0]))
+    assert rel < (2e-5 if recon == "sp_weno" else 2e-3), rel
+
+
+def test_fp32_scalar_linadv_dl():
+    nx = 200
+    x = -np.pi + (np.arange(nx) + 0.5) * 2 * np.pi / nx
+    u0 = (np.sin(x) ** 4).reshape(1, 1, 1, nx)
+    res = {}
+    for prec in ("fp64", "fp32_bf16"):
+        d = make_desc(model="linadv", flux="lin_tecno4", recon="sp_weno_dl", nx=nx, x=(-np.pi, np.pi), cfl=0.5,
+                      final_time=0.5, t_stamps=5, network=net(), precision=prec)
+        s = Solver(d)
+        s.upload_prim(u0)
+        s.run(chunk=32)
+        res[prec] = s.errors(np.sin(x - s.globals().time) ** 4)
+    # L1 error of the FP32 form within 1.5x of the FP64 form
+    assert res["fp32_bf16"][0] < 1.5 * res["fp64"][0], res

