@@ -247,6 +247,21 @@ DSPW_HD int ghost_source(int c, int N, int kind, int& flip) {
   return c < 0 ? 0 : N - 1;   // neumann (and dirichlet, which ignores it)
 }
 
+// Sign property of the reconstruction (the trainer's sign_property,
+// DSP-WENO_trainer/DSP-WENO_network_trainer.py:110-116): the reconstructed jump
+// zr - zl has the sign of the cell jump z2 - z1 or is zero.  "Zero" allows the
+// rounding of the arithmetic type (the trainer uses 1e-14 for FP64 data of
+// order one): 8 ulps of the largest value involved.
+template <typename T>
+DSPW_HD bool sign_violation(T z1, T z2, T zl, T zr) {
+  T rj = zr - zl, cj = z2 - z1;
+  if (!(rj * cj < T(0))) return false;
+  typedef Mth<T> m;
+  T sc = m::max(m::max(m::abs(zl), m::abs(zr)), m::max(m::abs(z1), m::abs(z2)));
+  const T eps = sizeof(T) == 8 ? T(2.220446049250313e-16) : T(1.1920929e-07);
+  return m::abs(rj) > T(8) * eps * sc;
+}
+
 // ------------------------------------------------------ warp shared memory --
 
 // staging of the network inputs / outputs of one warp (FP32 form only)
@@ -450,10 +465,17 @@ __device__ inline int dsp_weno_warp<double>(const NetParams& NP, const NetFrag&,
 template <>
 __device__ inline int dsp_weno_warp<float>(const NetParams& NP, const NetFrag& nf, WarpSmem<float>* sm, int lane,
                                            bool valid, float u0, float u1, float u2, float u3, float& l, float& r) {
-  bool guard = fabsf(u2 - u1) < 1e-15f;
+  // The reference skips the network when |u2 - u1| < 1e-15 (reconstruct.cc:152);
+  // in FP32 the equivalent "no jump" test is a jump of a few ulps of the values,
+  // below which the scaled differences of the features are rounding noise.
+  float mag = fmaxf(fabsf(u1), fabsf(u2));
+  bool guard = fabsf(u2 - u1) < fmaxf(1e-15f, 4.0f * 1.1920929e-07f * mag);
   float feat[5], vx[5], vy[5];
   nn_features<float>(u0, u1, u2, u3, feat, vx, vy);
-  bool use = valid && !guard;
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < 5; k++) finite = finite && isfinite(feat[k]) && isfinite(vx[k]) && isfinite(vy[k]);
+  bool use = valid && !guard && finite;
   if (!use) { feat[0] = feat[1] = feat[2] = feat[3] = feat[4] = 0.f; }
   bool inbox = true;
   if (NP.use_box) {
@@ -464,17 +486,20 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, const NetFrag& n
   warp_mlp_bf16(nf, sm->ns.feat, sm->ns.logit, feat, lg, lane);
   if (!valid) return 0;
   if (guard) { l = 0.f; r = 0.f; return 0; }
-  if (!inbox) {   // outside the network's training range: plain SP-WENO
+  if (!finite || !inbox) {   // degenerate features or outside the training range: plain SP-WENO
     sp_weno<float>(u0, u1, u2, u3, 0, l, r);
     return 0;
   }
   nn_finish<float>(lg, vx, vy, u0, u1, u2, u3, l, r);
-  // sign-preserving limiter: the reconstructed jump must not oppose the cell jump
+  // sign-preserving limiter: the reconstructed jump must not oppose the cell
+  // jump; an opposing jump is replaced by zero, so the property holds exactly.
+  // Only corrections larger than rounding are counted.
   float dj = u2 - u1, rj = r - l;
   if (dj * rj < 0.f) {
+    int counted = sign_violation<float>(u1, u2, l, r);
     float c = 0.5f * (l + r);
     l = c; r = c;
-    return 1;
+    return counted;
   }
   return 0;
 }
@@ -559,11 +584,7 @@ __device__ inline void tecno_dissipation(const ProbDev& P, const NetParams& NP, 
     T zl = T(0), zr = T(0);
     reconstruct_lane<T>(P, NP, nf, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol);
     T dZ = zr - zl;
-    if (valid) {
-      // sign property check on every reconstructed component jump
-      T cj = z[2] - z[1];
-      if (cj * dZ < T(0)) signv++;
-    }
+    if (valid && sign_violation<T>(z[1], z[2], zl, zr)) signv++;
     T ld = Lam[j];
 #pragma unroll
     for (int i = 0; i < 5; i++) Diff[i] += col[i] * ld * dZ;
@@ -828,7 +849,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
     T D = (P.model == DSPW_LINADV) ? m::abs(vn) : T(0.5) * (m::abs(s1) + m::abs(s2));
     T l = T(0), r = T(0);
     reconstruct_lane<T>(P, *A.net, nf, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
-    if (valid && (s2 - s1) * (r - l) < T(0)) signv++;
+    if (valid && sign_violation<T>(s1, s2, l, r)) signv++;
     flux -= T(0.5) * D * (r - l);
   }
   flux *= T(P.area[DIR]);

@@ -57,6 +57,7 @@ def test_golden_run_fp64(case):
     assert_state_close(got, ref, what=name)
     st = s.status()
     assert st.code == 0 and st.nonfinite_cells == 0 and st.nonpositive_cells == 0
+    assert st.sign_violations == 0
 
 
 REDUCED = ["linadv_sp_weno", "linadv_sp_weno_dl", "burgers_wenoc", "shuosher_sp_weno", "shuosher_sp_weno_dl",
