@@ -366,6 +366,7 @@ def main():
         "clocks": r["clk"],
         "kernels_ms_one_step": [[a, b, round(c, 4)] for a, b, c in r["prof"]],
         "health": {"code": r["status"].code, "sign_violations": r["status"].sign_violations,
+                   "faces_checked": r["status"].faces_checked, "limiter_acts": r["status"].limiter_acts,
                    "nonfinite": r["status"].nonfinite_cells, "nonpositive": r["status"].nonpositive_cells},
     }
     if r["fp64_ms"]:

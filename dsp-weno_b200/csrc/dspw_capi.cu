@@ -695,6 +695,7 @@ int dspw_last_status(dspw_handle* h, dspw_status_out* s) {
   s->nonpositive_cells = (long long)d.nonpositive;
   s->sign_violations = (long long)d.sign_viol;
   s->faces_checked = (long long)d.faces_checked;
+  s->limiter_acts = (long long)d.limiter_acts;
   h->last_error = 0;
   return DSPW_OK;
 }

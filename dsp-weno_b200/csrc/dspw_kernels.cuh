@@ -58,7 +58,7 @@ struct ProbState {
 struct StatusDev {
   int code;
   int pad;
-  unsigned long long nonfinite, nonpositive, sign_viol, faces_checked;
+  unsigned long long nonfinite, nonpositive, sign_viol, faces_checked, limiter_acts;
 };
 
 template <typename T>
@@ -253,13 +253,14 @@ DSPW_HD int ghost_source(int c, int N, int kind, int& flip) {
 // rounding of the arithmetic type (the trainer uses 1e-14 for FP64 data of
 // order one): 8 ulps of the largest value involved.
 template <typename T>
-DSPW_HD bool sign_violation(T z1, T z2, T zl, T zr) {
+DSPW_HD bool sign_violation(T z0, T z1, T z2, T z3, T zl, T zr) {
   T rj = zr - zl, cj = z2 - z1;
   if (!(rj * cj < T(0))) return false;
   typedef Mth<T> m;
-  T sc = m::max(m::max(m::abs(zl), m::abs(zr)), m::max(m::abs(z1), m::abs(z2)));
+  T sc = m::max(m::max(m::max(m::abs(zl), m::abs(zr)), m::max(m::abs(z1), m::abs(z2))),
+                m::max(m::abs(z0), m::abs(z3)));
   const T eps = sizeof(T) == 8 ? T(2.220446049250313e-16) : T(1.1920929e-07);
-  return m::abs(rj) > T(8) * eps * sc;
+  return m::abs(rj) > T(64) * eps * sc;
 }
 
 // ------------------------------------------------------ warp shared memory --
@@ -493,13 +494,11 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, const NetFrag& n
   nn_finish<float>(lg, vx, vy, u0, u1, u2, u3, l, r);
   // sign-preserving limiter: the reconstructed jump must not oppose the cell
   // jump; an opposing jump is replaced by zero, so the property holds exactly.
-  // Only corrections larger than rounding are counted.
   float dj = u2 - u1, rj = r - l;
   if (dj * rj < 0.f) {
-    int counted = sign_violation<float>(u1, u2, l, r);
     float c = 0.5f * (l + r);
     l = c; r = c;
-    return counted;
+    return 1;
   }
   return 0;
 }
@@ -584,7 +583,7 @@ __device__ inline void tecno_dissipation(const ProbDev& P, const NetParams& NP, 
     T zl = T(0), zr = T(0);
     reconstruct_lane<T>(P, NP, nf, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol);
     T dZ = zr - zl;
-    if (valid && sign_violation<T>(z[1], z[2], zl, zr)) signv++;
+    if (valid && sign_violation<T>(z[0], z[1], z[2], z[3], zl, zr)) signv++;
     T ld = Lam[j];
 #pragma unroll
     for (int i = 0; i < 5; i++) Diff[i] += col[i] * ld * dZ;
@@ -697,7 +696,8 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
 
 template <typename T>
 __device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax, double ent,
-                                     unsigned bad_fin, unsigned bad_pos, unsigned long long signv, int viol) {
+                                     unsigned bad_fin, unsigned bad_pos, unsigned long long signv, int viol,
+                                     unsigned checked) {
   if (A.final_stage && !A.residual_only) {
     unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
     warp_max_u64_lane0(sb);
@@ -711,10 +711,13 @@ __device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int la
   unsigned bp = __reduce_add_sync(0xffffffffu, bad_pos);
   unsigned sv = __reduce_add_sync(0xffffffffu, (unsigned)signv);
   unsigned vv = __reduce_add_sync(0xffffffffu, (unsigned)viol);
-  if (lane == 0 && (bf | bp | sv | vv)) {
+  unsigned ck = __reduce_add_sync(0xffffffffu, checked);
+  if (lane == 0) {
+    if (ck) atomicAdd(&A.status->faces_checked, (unsigned long long)ck);
     if (bf) { atomicAdd(&A.status->nonfinite, (unsigned long long)bf); atomicCAS(&A.status->code, 0, DSPW_ERR_NONFINITE); }
     if (bp) { atomicAdd(&A.status->nonpositive, (unsigned long long)bp); atomicCAS(&A.status->code, 0, DSPW_ERR_NONPOSITIVE); }
-    if (sv + vv) atomicAdd(&A.status->sign_viol, (unsigned long long)(sv + vv));
+    if (sv) atomicAdd(&A.status->sign_viol, (unsigned long long)sv);
+    if (vv) atomicAdd(&A.status->limiter_acts, (unsigned long long)vv);
   }
 }
 
@@ -794,7 +797,8 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
   if (!final_sweep) { smax = 0.0; ent = 0.0; }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol);
+  unsigned checked = (P.tecno && valid) ? (DIM == 1 ? 3u : (DIM == 2 ? 4u : 5u)) : 0u;
+  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
   __syncwarp();
 }
 
@@ -849,7 +853,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
     T D = (P.model == DSPW_LINADV) ? m::abs(vn) : T(0.5) * (m::abs(s1) + m::abs(s2));
     T l = T(0), r = T(0);
     reconstruct_lane<T>(P, *A.net, nf, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
-    if (valid && sign_violation<T>(s1, s2, l, r)) signv++;
+    if (valid && sign_violation<T>(s0, s1, s2, s3, l, r)) signv++;
     flux -= T(0.5) * D * (r - l);
   }
   flux *= T(P.area[DIR]);
@@ -867,7 +871,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol);
+  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, (P.tecno && valid) ? 1u : 0u);
   __syncwarp();
 }
 

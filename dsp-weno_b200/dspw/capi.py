@@ -67,7 +67,8 @@ class Globals(C.Structure):
 
 class StatusOut(C.Structure):
     _fields_ = [("code", C.c_int), ("nonfinite_cells", C.c_longlong), ("nonpositive_cells", C.c_longlong),
-                ("sign_violations", C.c_longlong), ("faces_checked", C.c_longlong)]
+                ("sign_violations", C.c_longlong), ("faces_checked", C.c_longlong),
+                ("limiter_acts", C.c_longlong)]
 
 
 class TrainCfg(C.Structure):

@@ -139,8 +139,10 @@ typedef struct dspw_status_out {
   int code;                  /* first error seen, DSPW_OK if none */
   long long nonfinite_cells;
   long long nonpositive_cells;
-  long long sign_violations;  /* faces where (Zji-Zij)(Z_{i+1}-Z_i) < 0 */
-  long long faces_checked;
+  long long sign_violations;  /* reconstructions whose jump Zji-Zij opposes Z_{i+1}-Z_i by
+                                 more than rounding (64 ulps of the stencil's magnitude) */
+  long long faces_checked;    /* component-face reconstructions checked */
+  long long limiter_acts;     /* FP32 form: opposing jumps zeroed by the sign-preserving limiter */
 } dspw_status_out;
 
 DSPW_API const char* dspw_error_string(int code);
