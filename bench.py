@@ -206,6 +206,11 @@ def measure_gpu(args, torch, dist, rank, world):
         return ms
 
     s = solver(args.precision, args.recon)
+    if args.profile_only:
+        s.step(args.warmup)
+        s.step(args.steps)
+        s.sync()
+        return None
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     ms = timed(s, args.steps, args.warmup)
@@ -272,6 +277,8 @@ def main():
     ap.add_argument("--cpu-sample-n", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="warm-up and timed steps only (no e2e, CPU or FP64 legs); for ncu captures")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -337,6 +344,8 @@ def main():
     else:
         torch.cuda.set_device(0)
     r = measure_gpu(args, torch, dist, rank, world)
+    if r is None:
+        return
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -18,8 +18,9 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 REPO = PKG.parent
 CSRC = PKG / "csrc"
-BUILD = PKG / "_build"
-LIB = PKG / "libdspw.so"
+BUILD = Path(os.environ.get("DSPW_BUILD_DIR", PKG / "_build"))
+LIB = Path(os.environ.get("DSPW_OUT", PKG / "libdspw.so"))
+EXTRA = os.environ.get("DSPW_EXTRA_FLAGS", "").split()
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -40,7 +41,7 @@ def compile_unit(name: str, flags: list[str], verbose: bool) -> Path:
         REPO / "include" / "dspw.h"]
     if obj.exists() and all(obj.stat().st_mtime >= d.stat().st_mtime for d in deps) and not verbose:
         return obj
-    cmd = [NVCC, *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]
+    cmd = [NVCC, *ARCH, *COMMON, *EXTRA, *flags, "-c", str(src), "-o", str(obj)]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -52,7 +53,7 @@ def compile_unit(name: str, flags: list[str], verbose: bool) -> Path:
 
 
 def build(verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+    BUILD.mkdir(parents=True, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
         futs = [ex.submit(compile_unit, n, f, verbose) for n, f in UNITS.items()]
         objs = [f.result() for f in futs]

@@ -27,6 +27,14 @@ constexpr int SEG_CELLS = 30;               // cells per warp task
 constexpr int SEG_FACES = SEG_CELLS + 1;    // faces per warp task (lanes 0..30)
 constexpr int SEG_LOAD = SEG_CELLS + 4;     // staged cells per warp task
 constexpr int WARPS_PER_BLOCK = 8;
+#ifndef DSPW_MINB_F64
+#define DSPW_MINB_F64 2
+#endif
+#ifndef DSPW_MINB_F32
+#define DSPW_MINB_F32 3
+#endif
+// resident blocks per SM requested from the register allocator
+template <typename T> struct MinBlocks { static constexpr int value = sizeof(T) == 8 ? DSPW_MINB_F64 : DSPW_MINB_F32; };
 
 struct ProbDev {
   int model, flux, recon, dim, nv, nrk;
@@ -877,7 +885,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
 
 // One sweep of direction DIR over every problem of the batch.
 template <typename T, int DIR>
-__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32)
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MinBlocks<T>::value)
 k_sweep(SweepArgs<T> A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem<T>* sm = reinterpret_cast<WarpSmem<T>*>(smem_raw) + (threadIdx.x >> 5);
