@@ -729,12 +729,11 @@ __device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int la
   }
 }
 
+// Faces of one staged line segment (phases B and C): wide two-point fluxes,
+// face central flux, TeCNO dissipation; face fluxes end in sm->F.
 template <typename T, int DIR, int DIM>
-__device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S, const NetFrag& nf,
-                           WarpSmem<T>* sm, int lane, int lt) {
-  int i0, j0, k0, c0, ncell;
-  decode_task<DIR>(P, lt, i0, j0, k0, c0, ncell);
-  euler_stage_cells<T, DIR>(A, P, sm, lane, i0, j0, k0, c0, ncell);
+__device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, const NetFrag& nf, WarpSmem<T>* sm,
+                                   int lane, int ncell, int& viol, unsigned long long& signv, unsigned& checked) {
   const T G = T(P.gamma), Rg = T(P.gas_const), area = T(P.area[DIR]);
   // phase B: wide two-point flux centred at g = c0 - 1 + lane (cells g-1, g+1)
   if (P.fourth && lane <= ncell + 1) {
@@ -750,8 +749,6 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
   const bool valid = lane <= ncell;
   T flux[5] = {T(0), T(0), T(0), T(0), T(0)};
   FaceAvg<T> fa;
-  int viol = 0;
-  unsigned long long signv = 0;
   {
     T Pl[5], Pr[5];
     const int ql = valid ? lane + 1 : 1;
@@ -784,12 +781,25 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
     tecno_dissipation<T, DIR, DIM>(P, *A.net, nf, sm, lane, valid, valid ? lane : 0, fa, flux, viol, signv);
 #pragma unroll
     for (int v = 0; v < 5; v++) flux[v] *= area;
+    checked = valid ? (DIM == 1 ? 3u : (DIM == 2 ? 4u : 5u)) : 0u;
   }
   if (valid) {
 #pragma unroll
     for (int v = 0; v < 5; v++) sm->F[v][lane] = flux[v];
   }
   __syncwarp();
+}
+
+template <typename T, int DIR, int DIM>
+__device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S, const NetFrag& nf,
+                           WarpSmem<T>* sm, int lane, int lt) {
+  int i0, j0, k0, c0, ncell;
+  decode_task<DIR>(P, lt, i0, j0, k0, c0, ncell);
+  euler_stage_cells<T, DIR>(A, P, sm, lane, i0, j0, k0, c0, ncell);
+  int viol = 0;
+  unsigned long long signv = 0;
+  unsigned checked = 0;
+  euler_faces<T, DIR, DIM>(A, P, nf, sm, lane, ncell, viol, signv, checked);
   // phase D: cells
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
@@ -805,9 +815,71 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
   if (!final_sweep) { smax = 0.0; ent = 0.0; }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  unsigned checked = (P.tecno && valid) ? (DIM == 1 ? 3u : (DIM == 2 ? 4u : 5u)) : 0u;
   warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
   __syncwarp();
+}
+
+// Block-cooperative variant for the y and z sweeps: the 8 warps of the block
+// hold 8 adjacent x-columns of the same line segment.  The staging loads and
+// the cell epilogue run with threads laid out as 4 rows x 8 columns per warp
+// instruction (8 consecutive x per row), instead of one strided cell per lane;
+// the faces are evaluated per warp exactly as in euler_task.
+constexpr int COOP_COLS = WARPS_PER_BLOCK;
+
+template <typename T, int DIR, int DIM>
+__device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbState& S, const NetFrag& nf,
+                                 WarpSmem<T>* sm0, int lt0) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int i0, j0, k0, c0, ncell;
+  decode_task<DIR>(P, lt0, i0, j0, k0, c0, ncell);   // i0 of column 0 (a multiple of 8)
+  const int N = dir_len<DIR>(P);
+  const T G = T(P.gamma);
+  const int col = tid % COOP_COLS;
+  // staging: rows q = tid / 8 and q + 32 of column col
+  for (int q = tid / COOP_COLS; q < ncell + 4; q += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
+    int c = c0 - 2 + q;
+    int side = c < 0 ? 0 : 1;
+    int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
+    T p[5];
+    if (kind == DSPW_BC_DIRICHLET) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) p[v] = T(P.bc_state[2 * DIR + side][v]);
+    } else {
+      int flip;
+      int src = ghost_source(c, N, kind, flip);
+      T u[5];
+      load_cons<T>(A.Uin, A.ctot, cell_index<DIR>(P, i0 + col, j0, k0, src), P.nv, P.dim, u);
+      cons_to_prim<T>(u, G, p);
+      if (flip) p[1 + DIR] = -p[1 + DIR];
+    }
+    T v[5];
+    prim_to_ent<T>(p, G, v);
+    WarpSmem<T>* sc = sm0 + col;
+#pragma unroll
+    for (int w = 0; w < 5; w++) { sc->P[w][q] = p[w]; sc->V[w][q] = v[w]; }
+  }
+  __syncthreads();
+  int viol = 0;
+  unsigned long long signv = 0;
+  unsigned checked = 0;
+  euler_faces<T, DIR, DIM>(A, P, nf, sm0 + warp, lane, ncell, viol, signv, checked);
+  __syncthreads();
+  const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
+  double smax = 0.0, ent = 0.0;
+  unsigned bad_fin = 0, bad_pos = 0;
+  for (int row = tid / COOP_COLS; row < ncell; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
+    WarpSmem<T>* sc = sm0 + col;
+    T Fl[5], Fr[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) { Fl[v] = sc->F[v][row]; Fr[v] = sc->F[v][row + 1]; }
+    long long cell = cell_index<DIR>(P, i0 + col, j0, k0, c0 + row);
+    finish_cell<T>(A, P, S, cell, false, final_sweep, Fl, Fr, P.nv, smax, ent, bad_fin, bad_pos);
+  }
+  if (!final_sweep) { smax = 0.0; ent = 0.0; }
+  SweepArgs<T> A2 = A;
+  A2.final_stage = A.final_stage && final_sweep;
+  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
+  __syncthreads();
 }
 
 // scalar laws: lin_/bur_ fluxes (enflo_scalar/src_scalar/num_flux.cc:12-57,
@@ -888,12 +960,33 @@ template <typename T, int DIR>
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MinBlocks<T>::value)
 k_sweep(SweepArgs<T> A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  WarpSmem<T>* sm = reinterpret_cast<WarpSmem<T>*>(smem_raw) + (threadIdx.x >> 5);
+  WarpSmem<T>* sm0 = reinterpret_cast<WarpSmem<T>*>(smem_raw);
+  WarpSmem<T>* sm = sm0 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   NetFrag nf;
   if (sizeof(T) == 4) net_frag_load(*A.net, lane, nf);
   const int stride = gridDim.x * WARPS_PER_BLOCK;
-  for (int task = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); task < A.ntask; task += stride) {
+  for (int base = blockIdx.x * WARPS_PER_BLOCK; base < A.ntask; base += stride) {
+    if (DIR >= 1 && base + WARPS_PER_BLOCK <= A.ntask) {
+      // block-uniform test: 8 tasks of one Euler problem on 8 adjacent columns
+      const int p = find_problem(A.task_start, A.nprob, base);
+      const int lt0 = base - __ldg(A.task_start + p);
+      const ProbDev& P = A.prob[p];
+      if (!P.is_scalar && base + WARPS_PER_BLOCK <= __ldg(A.task_start + p + 1) && (lt0 % P.nx) % COOP_COLS == 0 &&
+          (lt0 % P.nx) + COOP_COLS <= P.nx) {
+        ProbState& S = A.st[p];
+        if (!A.residual_only && !*((volatile int*)&S.active)) continue;
+        if (DIR == 1) {
+          if (P.dim == 2) euler_coop_block<T, DIR, 2>(A, P, S, nf, sm0, lt0);
+          else euler_coop_block<T, DIR, 3>(A, P, S, nf, sm0, lt0);
+        } else {
+          euler_coop_block<T, DIR, 3>(A, P, S, nf, sm0, lt0);
+        }
+        continue;
+      }
+    }
+    const int task = base + (threadIdx.x >> 5);
+    if (task >= A.ntask) continue;
     const int p = find_problem(A.task_start, A.nprob, task);
     const ProbDev& P = A.prob[p];
     ProbState& S = A.st[p];
