@@ -31,6 +31,7 @@ UNITS = {
     "dspw_fp32.cu": ["--fmad=true"],
     "dspw_capi.cu": ["--fmad=false"],
     "dspw_train.cu": ["--fmad=true"],
+    "dspw_noalloc.cu": ["--fmad=false"],
 }
 
 

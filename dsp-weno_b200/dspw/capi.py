@@ -220,6 +220,7 @@ def lib():
         "dspw_errors": (I, [P, I, I, dp, dp]),
         "dspw_sync": (I, [P]),
         "dspw_reconstruct_batch": (I, [C.POINTER(Desc), dp, LL, dp, dp, C.POINTER(LL)]),
+        "dspw_globals_noalloc": (I, [C.POINTER(Desc), P, LL, I, P, P]),
         "dspw_profile_step": (I, [P, dp, C.c_char_p, I, C.POINTER(I)]),
         "dspw_stream": (P, [P]),
         "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),

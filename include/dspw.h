@@ -202,6 +202,23 @@ DSPW_API int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, i
 DSPW_API int dspw_reconstruct_batch(const dspw_desc* desc, const double* u4, long long n, double* recl,
                                     double* recr, long long* limiter_acts);
 
+/* Global sums of a state the caller owns, with no device allocation.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc: a
+ * driver that keeps every device buffer in its own pool, a component that may
+ * not grow the device footprint, or a loop that must not synchronise the device
+ * through an allocation.  d_cons: conserved component planes on the current
+ * device (stride elements apart, elem_bytes 8 or 4, the layout of
+ * dspw_device_state); d_out: 7 device doubles receiving total entropy, kinetic
+ * energy and the 5 conserved totals (dspw_globals_out order), each times the
+ * cell volume.  Work is enqueued on `stream` (a cudaStream_t, may be NULL); the
+ * call does not synchronise.  Scratch is one fixed 256 KiB device array in the
+ * library, shared by all calls: states above 16,777,216 cells are rejected with
+ * DSPW_ERR_ARG, and calls that overlap on the GPU race on it.  The first call
+ * on each device looks up the array's device address and should not be made
+ * during stream capture. */
+DSPW_API int dspw_globals_noalloc(const dspw_desc* desc, const void* d_cons, long long stride, int elem_bytes,
+                                  double* d_out, void* stream);
+
 /* Synchronise the handle's stream; returns the first error recorded. */
 DSPW_API int dspw_sync(dspw_handle* h);
 
