@@ -123,6 +123,11 @@ struct dspw_handle {
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   double graph_dt = -1.0;
+  // training-pair collection during residual evaluations (trainer only)
+  float* collect_buf = nullptr;
+  unsigned long long* collect_count = nullptr;
+  unsigned long long collect_cap = 0;
+  unsigned collect_stride = 1;
   // profiling: when set, an event is recorded after every launch
   std::vector<cudaEvent_t>* prof_ev = nullptr;
   std::vector<std::string>* prof_names = nullptr;
@@ -329,6 +334,10 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
   a.residual_only = residual_only;
   a.status = h->dstatus;
   a.net = h->dnet;
+  a.collect_buf = residual_only ? h->collect_buf : nullptr;
+  a.collect_count = h->collect_count;
+  a.collect_cap = h->collect_cap;
+  a.collect_stride = h->collect_stride ? h->collect_stride : 1;
   if (h->has_ns) {
     CK(Launch<T>::entvars(h->dprob, h->nprob, h->dcell_start, h->ctot, a.Uin, h->ctot, (T*)h->V, h->stream));
     prof_mark(h, "entvars");
@@ -398,6 +407,19 @@ int check_p(dspw_handle* h, int p) { return (!h || p < 0 || p >= h->nprob) ? DSP
 }  // namespace
 
 namespace dspw {
+int handle_collect(dspw_handle* h, float* buf, unsigned long long* count, unsigned long long cap, unsigned stride) {
+  h->collect_buf = buf;
+  h->collect_count = count;
+  h->collect_cap = cap;
+  h->collect_stride = stride;
+  int r = enqueue_stage_any(h, 0, 1);
+  h->collect_buf = nullptr;
+  h->collect_count = nullptr;
+  if (r) return r;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return DSPW_ERR_CUDA;
+  return DSPW_OK;
+}
+int handle_precision(const dspw_handle* h) { return h->precision; }
 ProbDev make_prob_public(const dspw_desc& d, long long off) { return make_prob(d, off); }
 NetParams make_net_public(const dspw_desc& d) { return make_net(d); }
 }  // namespace dspw

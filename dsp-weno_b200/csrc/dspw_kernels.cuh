@@ -87,7 +87,26 @@ struct SweepArgs {
   int viscous;             // 1: the NS viscous kernel performs the update
   StatusDev* status;
   const NetParams* net;
+  // optional collection of (stencil, reconstruction) pairs for training:
+  // every collect_stride-th reconstruction appends 6 floats (u0..u3, l, r)
+  float* collect_buf;
+  unsigned long long* collect_count;
+  unsigned long long collect_cap;
+  unsigned collect_stride;
 };
+
+// append one training pair (sampled by a hash of the reconstruction's position)
+template <typename T>
+__device__ inline void collect_pair(const SweepArgs<T>& A, unsigned key, T s0, T s1, T s2, T s3, T l, T r) {
+  if (!A.collect_buf) return;
+  unsigned h = key * 2654435761u;
+  h ^= h >> 15;
+  if (h % A.collect_stride) return;
+  unsigned long long i = atomicAdd(A.collect_count, 1ull);
+  if (i >= A.collect_cap) return;
+  float* o = A.collect_buf + 6 * i;
+  o[0] = (float)s0; o[1] = (float)s1; o[2] = (float)s2; o[3] = (float)s3; o[4] = (float)l; o[5] = (float)r;
+}
 
 // ----------------------------------------------------------- small helpers --
 
@@ -528,9 +547,10 @@ __device__ inline void reconstruct_lane(const ProbDev& P, const NetParams& NP, c
 // of the 4 stencil cells, component-wise reconstruction.  Columns of R are
 // built one at a time; Diff[i] accumulates over j in the reference's order.
 template <typename T, int DIR, int DIM>
-__device__ inline void tecno_dissipation(const ProbDev& P, const NetParams& NP, const NetFrag& nf, WarpSmem<T>* sm,
-                                         int lane, bool valid, int q0, const FaceAvg<T>& fa, T flux[5],
-                                         int& viol, unsigned long long& signv) {
+__device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P, const NetParams& NP,
+                                         const NetFrag& nf, WarpSmem<T>* sm, int lane, bool valid, int q0,
+                                         const FaceAvg<T>& fa, T flux[5], int& viol, unsigned long long& signv,
+                                         unsigned collect_salt) {
   typedef Mth<T> m;
   const T G = T(P.gamma);
   const T n0 = T(DIR == 0), n1 = T(DIR == 1), n2 = T(DIR == 2);
@@ -590,6 +610,9 @@ __device__ inline void tecno_dissipation(const ProbDev& P, const NetParams& NP, 
     }
     T zl = T(0), zr = T(0);
     reconstruct_lane<T>(P, NP, nf, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol);
+    if (A.collect_buf && valid)
+      collect_pair<T>(A, (unsigned)(blockIdx.x * 1024 + threadIdx.x) * 8u + (unsigned)j + 977u * collect_salt,
+                      z[0], z[1], z[2], z[3], zl, zr);
     T dZ = zr - zl;
     if (valid && sign_violation<T>(z[0], z[1], z[2], z[3], zl, zr)) signv++;
     T ld = Lam[j];
@@ -733,7 +756,8 @@ __device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int la
 // face central flux, TeCNO dissipation; face fluxes end in sm->F.
 template <typename T, int DIR, int DIM>
 __device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, const NetFrag& nf, WarpSmem<T>* sm,
-                                   int lane, int ncell, int& viol, unsigned long long& signv, unsigned& checked) {
+                                   int lane, int ncell, int& viol, unsigned long long& signv, unsigned& checked,
+                                   unsigned collect_salt = 0) {
   const T G = T(P.gamma), Rg = T(P.gas_const), area = T(P.area[DIR]);
   // phase B: wide two-point flux centred at g = c0 - 1 + lane (cells g-1, g+1)
   if (P.fourth && lane <= ncell + 1) {
@@ -778,7 +802,8 @@ __device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, cons
     const T ra = T(P.rarea[DIR]);
 #pragma unroll
     for (int v = 0; v < 5; v++) flux[v] *= ra;
-    tecno_dissipation<T, DIR, DIM>(P, *A.net, nf, sm, lane, valid, valid ? lane : 0, fa, flux, viol, signv);
+    tecno_dissipation<T, DIR, DIM>(A, P, *A.net, nf, sm, lane, valid, valid ? lane : 0, fa, flux, viol, signv,
+                                   collect_salt);
 #pragma unroll
     for (int v = 0; v < 5; v++) flux[v] *= area;
     checked = valid ? (DIM == 1 ? 3u : (DIM == 2 ? 4u : 5u)) : 0u;
@@ -799,7 +824,7 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
   int viol = 0;
   unsigned long long signv = 0;
   unsigned checked = 0;
-  euler_faces<T, DIR, DIM>(A, P, nf, sm, lane, ncell, viol, signv, checked);
+  euler_faces<T, DIR, DIM>(A, P, nf, sm, lane, ncell, viol, signv, checked, (unsigned)lt);
   // phase D: cells
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
@@ -862,7 +887,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   int viol = 0;
   unsigned long long signv = 0;
   unsigned checked = 0;
-  euler_faces<T, DIR, DIM>(A, P, nf, sm0 + warp, lane, ncell, viol, signv, checked);
+  euler_faces<T, DIR, DIM>(A, P, nf, sm0 + warp, lane, ncell, viol, signv, checked, (unsigned)(lt0 + warp));
   __syncthreads();
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
   double smax = 0.0, ent = 0.0;
@@ -934,6 +959,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
     T l = T(0), r = T(0);
     reconstruct_lane<T>(P, *A.net, nf, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
     if (valid && sign_violation<T>(s0, s1, s2, s3, l, r)) signv++;
+    if (A.collect_buf && valid) collect_pair<T>(A, (unsigned)lt * 32u + (unsigned)lane, s0, s1, s2, s3, l, r);
     flux -= T(0.5) * D * (r - l);
   }
   flux *= T(P.area[DIR]);

@@ -37,6 +37,14 @@ cudaError_t launch_end_step(const ProbDev* prob, ProbState* st, int nprob, cudaS
 // host-side construction shared by the C ABI entry points
 ProbDev make_prob_public(const dspw_desc& d, long long off);
 NetParams make_net_public(const dspw_desc& d);
+}  // namespace dspw
+
+struct dspw_handle;
+namespace dspw {
+// one residual evaluation of the handle's current state with pair collection
+// enabled (used by the trainer); returns a dspw status
+int handle_collect(dspw_handle* h, float* buf, unsigned long long* count, unsigned long long cap, unsigned stride);
+int handle_precision(const dspw_handle* h);
 cudaError_t launch_init_state(const ProbDev* prob, ProbState* st, int p, cudaStream_t s);
 
 }  // namespace dspw

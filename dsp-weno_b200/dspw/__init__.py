@@ -2,6 +2,6 @@
 (include/dspw.h, libdspw.so) and the param.in helpers.  All compute runs in
 libdspw.so; importing this package does not load CUDA."""
 from .capi import (ABI_VERSION, BC, FLUX, MODEL, MU, PRECISION, RECON, TIME, Desc, DspwError,
-                   Globals, Solver, StatusOut, TrainCfg, check, lib, load_network_file, make_desc,
+                   Globals, Solver, StatusOut, TrainCfg, Trainer, check, lib, load_network_file, make_desc,
                    nvar, save_network_file, xavier_network)
 from .paramfile import read_param, write_param

@@ -73,7 +73,8 @@ class StatusOut(C.Structure):
 
 class TrainCfg(C.Structure):
     _fields_ = [("lr", C.c_double), ("beta1", C.c_double), ("beta2", C.c_double),
-                ("weight_decay", C.c_double), ("eps", C.c_double), ("batch", C.c_int), ("seed", C.c_int)]
+                ("weight_decay", C.c_double), ("eps", C.c_double), ("batch", C.c_int), ("seed", C.c_int),
+                ("compute_bf16", C.c_int), ("collect_stride", C.c_int), ("reserved_i", C.c_int * 6)]
 
 
 def load_network_file(path) -> tuple[np.ndarray, np.ndarray]:
@@ -231,6 +232,8 @@ def lib():
         "dspw_trainer_epoch": (I, [P, C.POINTER(D)]),
         "dspw_trainer_loss_grad": (I, [P, dp, dp, I, C.POINTER(D), dp, dp]),
         "dspw_trainer_get_params": (I, [P, dp, dp]),
+        "dspw_trainer_info": (I, [P, C.POINTER(LL), dp]),
+        "dspw_trainer_eval": (I, [P, C.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -250,6 +253,73 @@ def reconstruct_batch(desc: Desc, u4) -> tuple[np.ndarray, np.ndarray, int]:
     check(lib().dspw_reconstruct_batch(C.byref(desc), u.reshape(-1), n, l, r, C.byref(acts)),
           "dspw_reconstruct_batch")
     return l, r, acts.value
+
+
+class Trainer:
+    """Owner of a dspw_trainer: GPU training of the DSP-WENO network.
+    Defaults follow DSP-WENO_trainer/config.py (lr 1e-3, betas (0.5, 0.9),
+    weight decay 1e-5, seed 6008) with batch 8192."""
+
+    def __init__(self, network, lr=1e-3, betas=(0.5, 0.9), weight_decay=1e-5, eps=1e-8, batch=8192, seed=6008,
+                 bf16=True, collect_stride=1):
+        W, b = network
+        cfg = TrainCfg(lr=lr, beta1=betas[0], beta2=betas[1], weight_decay=weight_decay, eps=eps, batch=batch,
+                       seed=seed, compute_bf16=int(bool(bf16)), collect_stride=int(collect_stride))
+        h = C.c_void_p()
+        check(lib().dspw_trainer_create(C.byref(cfg), np.ascontiguousarray(W, dtype=np.float64).reshape(-1),
+                                        np.ascontiguousarray(b, dtype=np.float64).reshape(-1), C.byref(h)),
+              "dspw_trainer_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().dspw_trainer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_data(self, stencils, targets):
+        s = np.ascontiguousarray(stencils, dtype=np.float64).reshape(-1)
+        t = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1)
+        check(lib().dspw_trainer_set_data(self.h, s, t, len(s) // 4), "dspw_trainer_set_data")
+
+    def collect(self, solver, max_pairs):
+        n = C.c_longlong()
+        check(lib().dspw_trainer_collect(self.h, solver.h, int(max_pairs), C.byref(n)), "dspw_trainer_collect")
+        return n.value
+
+    def epoch(self):
+        v = C.c_double()
+        check(lib().dspw_trainer_epoch(self.h, C.byref(v)), "dspw_trainer_epoch")
+        return v.value
+
+    def loss_grad(self, stencils, targets):
+        s = np.ascontiguousarray(stencils, dtype=np.float64).reshape(-1)
+        t = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1)
+        loss = C.c_double()
+        gw, gb = np.zeros(100), np.zeros(20)
+        check(lib().dspw_trainer_loss_grad(self.h, s, t, len(s) // 4, C.byref(loss), gw, gb), "dspw_trainer_loss_grad")
+        return loss.value, gw.reshape(4, 5, 5), gb.reshape(4, 5)
+
+    def eval(self):
+        v = C.c_double()
+        check(lib().dspw_trainer_eval(self.h, C.byref(v)), "dspw_trainer_eval")
+        return v.value
+
+    def params(self):
+        w, b = np.zeros(100), np.zeros(20)
+        check(lib().dspw_trainer_get_params(self.h, w, b), "dspw_trainer_get_params")
+        return w.reshape(4, 5, 5), b.reshape(4, 5)
+
+    def info(self):
+        n = C.c_longlong()
+        fm = np.zeros(5)
+        check(lib().dspw_trainer_info(self.h, C.byref(n), fm), "dspw_trainer_info")
+        return n.value, fm
 
 
 class DspwError(RuntimeError):

@@ -239,6 +239,9 @@ typedef struct dspw_train_cfg {
   double lr, beta1, beta2, weight_decay, eps;
   int batch;
   int seed;
+  int compute_bf16;    /* 1: weights and activations rounded to BF16 before each product (FP32 accumulation) */
+  int collect_stride;  /* dspw_trainer_collect keeps every collect_stride-th reconstruction (>= 1) */
+  int reserved_i[6];
 } dspw_train_cfg;
 
 DSPW_API int dspw_trainer_create(const dspw_train_cfg* cfg, const double* w_init /* 4*25 */,
@@ -258,6 +261,11 @@ DSPW_API int dspw_trainer_epoch(dspw_trainer* t, double* mean_loss);
 DSPW_API int dspw_trainer_loss_grad(dspw_trainer* t, const double* stencils, const double* targets, int n,
                            double* loss, double* grad_w /* 4*25 */, double* grad_b /* 4*5 */);
 DSPW_API int dspw_trainer_get_params(dspw_trainer* t, double* w /* 4*25 */, double* b /* 4*5 */);
+/* Mean loss over the trainer's data set with the current parameters, no update. */
+DSPW_API int dspw_trainer_eval(dspw_trainer* t, double* mean_loss);
+/* Number of samples and the largest |feature| of each of the 5 network inputs
+ * over the valid samples: the training box used for the SP-WENO fallback. */
+DSPW_API int dspw_trainer_info(dspw_trainer* t, long long* nsamples, double* feature_max /* 5 */);
 
 #ifdef __cplusplus
 }
