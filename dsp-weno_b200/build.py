@@ -53,6 +53,24 @@ def compile_unit(name: str, flags: list[str], verbose: bool) -> Path:
     return obj
 
 
+HOST = PKG / "host"
+CLI = Path(os.environ.get("DSPW_CLI_OUT", PKG / "enflo_b200"))
+
+
+def build_cli(lib: Path) -> Path:
+    """The command-line driver (host/*.cc), linked against libdspw.so."""
+    srcs = sorted(HOST.glob("*.cc"))
+    deps = srcs + sorted(HOST.glob("*.h")) + [REPO / "include" / "dspw.h", lib]
+    if CLI.exists() and all(CLI.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return CLI
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", f"-I{REPO / 'include'}", *map(str, srcs),
+           "-o", str(CLI), f"-L{lib.parent}", f"-l:{lib.name}", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host driver build failed:\n{r.stderr}")
+    return CLI
+
+
 def build(verbose: bool = False) -> Path:
     BUILD.mkdir(parents=True, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
@@ -64,6 +82,8 @@ def build(verbose: bool = False) -> Path:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    if LIB == PKG / "libdspw.so":
+        build_cli(LIB)
     return LIB
 
 

@@ -1,0 +1,319 @@
+// enflo_b200.cc -- command-line driver, a drop-in for the reference's
+// `enflo -i param.in` / `enfloS -i param.in` (enflo/src/main.cc:12-29).
+//
+// It reads the same param.in (param.h), evaluates the domain limits, initial
+// condition and exact solution (expr.h), and for every mesh level (all levels
+// when OOC_study is yes, the first otherwise, as FV::run, enflo/src/fv.cc:1231-1324)
+// runs the stage path through the C ABI (include/dspw.h).  It writes the
+// reference's SOLN_FILES_<reconstruction>/ directory: globals.dat, the final
+// solution, and for OOC studies l1_err.dat / l2_err.dat / linf_err.dat with the
+// table layout of compute_OOC (enflo_scalar/src_scalar/compute_ooc.cc:10-141).
+// Errors of systems are those of the density.
+//
+//   enflo_b200 -i param.in [--precision fp64|fp32_bf16] [--chunk K]
+//   enflo_b200 -i param.in --check          parse and print the descriptor, no GPU
+//   enflo_b200 -i param.in --dump-ic FILE   write level 0's initial state (FP64), no GPU
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/dspw.h"
+#include "expr.h"
+#include "param.h"
+
+using dspw_host::Expr;
+using dspw_host::Param;
+using dspw_host::read_param;
+
+namespace {
+
+struct Fail : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+int flux_enum(const std::string& f) {
+  static const std::map<std::string, int> m = {
+      {"lin_ec", DSPW_LIN_EC}, {"lin_ec4", DSPW_LIN_EC4}, {"lin_tecno", DSPW_LIN_TECNO},
+      {"lin_tecno4", DSPW_LIN_TECNO4}, {"bur_ec", DSPW_BUR_EC}, {"bur_ec4", DSPW_BUR_EC4},
+      {"bur_tecno", DSPW_BUR_TECNO}, {"bur_tecno4", DSPW_BUR_TECNO4}, {"roe", DSPW_ROE}, {"kep", DSPW_KEP},
+      {"kep4", DSPW_KEP4}, {"kepec", DSPW_KEPEC}, {"kepec4", DSPW_KEPEC4}, {"roe_ec", DSPW_ROE_EC},
+      {"roe_ec4", DSPW_ROE_EC4}, {"keps", DSPW_KEPS}, {"keps4", DSPW_KEPS4}, {"kep_tecno_roe", DSPW_KEP_TECNO_ROE},
+      {"kepes_tecno_roe", DSPW_KEPES_TECNO_ROE}, {"kepes_tecno_rusanov", DSPW_KEPES_TECNO_RUSANOV},
+      {"roe_tecno_roe", DSPW_ROE_TECNO_ROE}, {"kepes_tecno4_roe", DSPW_KEPES_TECNO4_ROE},
+      {"kepes_tecno4_rusanov", DSPW_KEPES_TECNO4_RUSANOV}, {"roe_tecno4_roe", DSPW_ROE_TECNO4_ROE}};
+  auto it = m.find(f);
+  if (it == m.end()) throw Fail("unknown flux scheme: " + f);
+  return it->second;
+}
+
+int recon_enum(const std::string& r) {
+  static const std::map<std::string, int> m = {{"sp_weno", DSPW_REC_SP_WENO}, {"sp_wenoc", DSPW_REC_SP_WENOC},
+                                               {"sp_weno_corr2", DSPW_REC_SP_WENO_CORR2},
+                                               {"sp_weno_dl", DSPW_REC_SP_WENO_DL}, {"first", DSPW_REC_FIRST},
+                                               {"second", DSPW_REC_SECOND}, {"minmod", DSPW_REC_MINMOD},
+                                               {"minabs", DSPW_REC_MINABS}};
+  auto it = m.find(r);
+  if (it == m.end()) throw Fail("reconstruction not supported by the GPU path: " + r);
+  return it->second;
+}
+
+int bc_enum(const std::string& b) {
+  if (b == "periodic") return DSPW_BC_PERIODIC;
+  if (b == "dirichlet") return DSPW_BC_DIRICHLET;
+  if (b == "neumann") return DSPW_BC_NEUMANN;
+  if (b == "wall") return DSPW_BC_WALL;
+  throw Fail("unknown boundary type: " + b);
+}
+
+// network file in the format of Neural_Network::load_network (enflo/src/neural_network.cc:82-130)
+void load_network(const std::string& path, dspw_desc& d) {
+  std::ifstream in(path);
+  if (!in) throw Fail("DSP-WENO network file does not exist: " + path);
+  std::string line;
+  bool weights = true;
+  int wl = 0, bl = 0;
+  while (std::getline(in, line)) {
+    while (!line.empty() && std::isspace((unsigned char)line.back())) line.pop_back();
+    if (line == "Biases") weights = false;
+    if (line != "BEGIN") continue;
+    int row = 0;
+    while (std::getline(in, line)) {
+      while (!line.empty() && std::isspace((unsigned char)line.back())) line.pop_back();
+      if (line == "END") break;
+      std::istringstream is(line);
+      std::vector<double> v;
+      double x;
+      while (is >> x) v.push_back(x);
+      if (v.empty()) continue;
+      if (weights) {
+        if (wl >= 4 || row >= 5 || v.size() != 5) throw Fail("network file: expected 4 layers of 5x5 weights");
+        for (int k = 0; k < 5; k++) d.nn_w[wl][row][k] = v[k];
+      } else {
+        if (bl >= 4 || row >= 5) throw Fail("network file: expected 4 layers of 5 biases");
+        d.nn_b[bl][row] = v[0];
+      }
+      row++;
+    }
+    if (weights) wl++; else bl++;
+  }
+  if (wl != 4 || bl != 4) throw Fail("network file: expected 4 weight and 4 bias blocks");
+}
+
+struct Level {
+  dspw_desc d;
+  int nvar;
+  long long n;
+  double xmin, xmax, ymin, ymax, zmin, zmax, dx, dy, dz;
+};
+
+Level make_level(const Param& P, int rl, const std::string& precision) {
+  Level L;
+  dspw_desc& d = L.d;
+  memset(&d, 0, sizeof(d));
+  d.abi_version = DSPW_ABI_VERSION;
+  if (P.scalar) d.model = P.model == "linadv" ? DSPW_LINADV : DSPW_BURGERS;
+  else if (P.model == "euler") d.model = DSPW_EULER;
+  else if (P.model == "ns_es") d.model = DSPW_NS_ES;
+  else if (P.model == "ns_kep") d.model = DSPW_NS_KEP;
+  else throw Fail("unknown model: " + P.model);
+  d.flux = flux_enum(P.flux);
+  d.recon = recon_enum(P.reconstruct);
+  if (P.time_scheme == "ssprk3") d.time_scheme = DSPW_SSPRK3;
+  else if (P.time_scheme == "rk1") d.time_scheme = DSPW_RK1;
+  else throw Fail("time scheme not supported by the GPU path: " + P.time_scheme);
+  d.precision = precision == "fp32_bf16" ? DSPW_FP32_BF16 : DSPW_FP64;
+  d.nx = P.nx[rl];
+  d.ny = P.ny[rl];
+  d.nz = P.nz[rl];
+  for (int f = 0; f < 6; f++) d.bc[f] = bc_enum(P.bc[f]);
+  d.ec1_fix = P.ec1_fix;
+  d.mu_model = P.mu_model == "sutherland" ? DSPW_MU_SUTHERLAND : (P.mu_model == "power" ? DSPW_MU_POWER : DSPW_MU_CONSTANT);
+  d.max_iter = P.max_iter;
+  d.t_stamps = P.time_stamps;
+  L.xmin = Expr(P.xmin, P.constants).eval(0, 0, 0, 0);
+  L.xmax = Expr(P.xmax, P.constants).eval(0, 0, 0, 0);
+  L.ymin = Expr(P.ymin, P.constants).eval(0, 0, 0, 0);
+  L.ymax = Expr(P.ymax, P.constants).eval(0, 0, 0, 0);
+  L.zmin = Expr(P.zmin, P.constants).eval(0, 0, 0, 0);
+  L.zmax = Expr(P.zmax, P.constants).eval(0, 0, 0, 0);
+  d.xmin = L.xmin; d.xmax = L.xmax; d.ymin = L.ymin; d.ymax = L.ymax; d.zmin = L.zmin; d.zmax = L.zmax;
+  d.gamma = P.gamma;
+  d.gas_const = P.gas_const;
+  d.prandtl = P.prandtl;
+  d.mu_ref = P.mu_ref;
+  d.T_ref = P.T_ref;
+  d.T_0 = P.T_0;
+  d.omega = P.omega;
+  for (int k = 0; k < 3; k++) d.lin_vel[k] = P.lin_vel[k];
+  d.cfl = P.cfl;
+  d.final_time = P.final_time;
+  if (P.reconstruct == "sp_weno_dl") load_network(P.net_file, d);
+  L.nvar = P.scalar ? 1 : 5;
+  L.n = (long long)d.nx * d.ny * d.nz;
+  L.dx = (L.xmax - L.xmin) / d.nx;   // enflo/src/fv.cc:29-31
+  L.dy = (L.ymax - L.ymin) / d.ny;
+  L.dz = (L.zmax - L.zmin) / d.nz;
+  return L;
+}
+
+// values of expressions at the cell centres xmin + 0.5 dx + i dx (enflo/src/fv.cc:41-43)
+std::vector<double> evaluate(const Level& L, const std::vector<std::string>& exprs,
+                             const std::map<std::string, double>& constants, double t) {
+  std::vector<Expr> ex;
+  for (auto& s : exprs) ex.emplace_back(s, constants);
+  std::vector<double> out(ex.size() * L.n);
+  const dspw_desc& d = L.d;
+  for (int k = 0; k < d.nz; k++)
+    for (int j = 0; j < d.ny; j++)
+      for (int i = 0; i < d.nx; i++) {
+        double x = L.xmin + 0.5 * L.dx + i * L.dx;
+        double y = L.ymin + 0.5 * L.dy + j * L.dy;
+        double z = L.zmin + 0.5 * L.dz + k * L.dz;
+        long long c = ((long long)k * d.ny + j) * d.nx + i;
+        for (size_t v = 0; v < ex.size(); v++) out[v * L.n + c] = ex[v].eval(x, y, z, t);
+      }
+  return out;
+}
+
+void check(int rc, const char* what) {
+  if (rc != DSPW_OK) throw Fail(std::string(what) + ": " + dspw_error_string(rc));
+}
+
+void write_ooc(const std::string& path, const Param& P, const std::vector<double>& err,
+               const std::vector<Level>& levels) {
+  std::ofstream f(path);
+  f << std::left << std::setw(40) << std::setfill('-') << "" << "\n";
+  f << std::left << std::setfill(' ') << std::setw(6) << "Nx" << std::setw(6) << "Ny" << std::setw(6) << "Nz"
+    << std::setw(17) << "ERR" << std::setw(8) << "OOC" << "\n";
+  f << std::left << std::setw(40) << std::setfill('-') << "" << "\n" << std::setfill(' ');
+  for (size_t i = 0; i < err.size(); i++) {
+    const Level& L = levels[i];
+    f << std::left << std::setw(6) << L.d.nx << std::setw(6) << L.d.ny << std::setw(6) << L.d.nz << std::scientific
+      << std::setw(17) << std::setprecision(5) << err[i];
+    if (i == 0) {
+      f << std::setw(8) << " - ";
+    } else {
+      // rate from the mesh-size measure of compute_OOC (problem_dim directions)
+      auto h2 = [&](const Level& M) {
+        double s = M.dx * M.dx;
+        if (P.problem_dim >= 2) s += M.dy * M.dy;
+        if (P.problem_dim >= 3) s += M.dz * M.dz;
+        return s;
+      };
+      double rate = std::log(err[i - 1] / err[i]) / std::log(std::sqrt(h2(levels[i - 1]) / h2(L)));
+      f << std::fixed << std::setprecision(2) << std::setw(8) << rate;
+    }
+    f << "\n";
+  }
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  std::string file, precision = "fp64", dump;
+  bool check_only = false;
+  int chunk = 64;
+  for (int a = 1; a < argc; a++) {
+    std::string s = argv[a];
+    if (s == "-i" && a + 1 < argc) file = argv[++a];
+    else if (s == "--precision" && a + 1 < argc) precision = argv[++a];
+    else if (s == "--chunk" && a + 1 < argc) chunk = std::atoi(argv[++a]);
+    else if (s == "--check") check_only = true;
+    else if (s == "--dump-ic" && a + 1 < argc) dump = argv[++a];
+    else {
+      std::cerr << "usage: enflo_b200 -i param.in [--precision fp64|fp32_bf16] [--chunk K] [--check] "
+                   "[--dump-ic FILE]\n";
+      return 2;
+    }
+  }
+  if (file.empty()) {
+    std::cerr << "enflo_b200: -i param.in is required\n";
+    return 2;
+  }
+  try {
+    Param P = read_param(file);
+    int nlev = P.ooc ? (int)P.nx.size() : 1;
+    std::vector<Level> levels;
+    for (int rl = 0; rl < nlev; rl++) levels.push_back(make_level(P, rl, precision));
+    if (check_only) {
+      // parse every expression so that syntax errors surface without a GPU
+      for (auto& e : P.ic) Expr(e, P.constants);
+      for (auto& e : P.exact) Expr(e, P.constants);
+      const dspw_desc& d = levels[0].d;
+      std::cout << "{\"model\": " << d.model << ", \"flux\": " << d.flux << ", \"recon\": " << d.recon
+                << ", \"nx\": " << d.nx << ", \"ny\": " << d.ny << ", \"nz\": " << d.nz << ", \"bc\": [" << d.bc[0]
+                << ", " << d.bc[1] << ", " << d.bc[2] << ", " << d.bc[3] << ", " << d.bc[4] << ", " << d.bc[5]
+                << "], \"xmin\": " << std::setprecision(17) << d.xmin << ", \"xmax\": " << d.xmax
+                << ", \"cfl\": " << d.cfl << ", \"final_time\": " << d.final_time << ", \"t_stamps\": " << d.t_stamps
+                << ", \"levels\": " << nlev << ", \"nn_w000\": " << d.nn_w[0][0][0] << "}\n";
+      return 0;
+    }
+    if (!dump.empty()) {
+      std::vector<double> ic = evaluate(levels[0], P.ic, P.constants, 0.0);
+      std::ofstream f(dump, std::ios::binary);
+      f.write(reinterpret_cast<const char*>(ic.data()), sizeof(double) * ic.size());
+      return 0;
+    }
+    std::string soln_dir = P.output_path + "/SOLN_FILES_" + P.reconstruct;   // enflo/src/fv.h:28-34
+    std::filesystem::remove_all(soln_dir);
+    std::filesystem::create_directories(soln_dir);
+    std::ofstream glob(soln_dir + "/globals.dat");
+    std::vector<double> l1, l2, linf;
+    for (int rl = 0; rl < nlev; rl++) {
+      Level& L = levels[rl];
+      std::cout << "   Solving on mesh with size " << L.d.nx << "x" << L.d.ny << "x" << L.d.nz << std::endl;
+      std::vector<double> ic = evaluate(L, P.ic, P.constants, 0.0);
+      dspw_handle* h = nullptr;
+      check(dspw_create(&L.d, &h), "dspw_create");
+      int rc = dspw_upload_prim(h, 0, ic.data());
+      if (rc) { dspw_destroy(h); check(rc, "dspw_upload_prim"); }
+      int steps = 0;
+      rc = dspw_run(h, chunk, &steps);
+      dspw_globals_out g;
+      if (rc == DSPW_OK) rc = dspw_globals(h, 0, &g);
+      if (rc) { dspw_destroy(h); check(rc, "dspw_run"); }
+      glob << std::setprecision(10) << g.time << " " << g.total_entropy << " " << g.iter << "\n";
+      std::vector<double> prim(L.nvar * L.n);
+      check(dspw_download_prim(h, 0, prim.data()), "dspw_download_prim");
+      if (P.ooc) {
+        std::vector<std::string> ex = {P.exact[0]};
+        std::vector<double> exact = evaluate(L, ex, P.constants, g.time);
+        double e[3];
+        check(dspw_errors(h, 0, 0, exact.data(), e), "dspw_errors");
+        l1.push_back(e[0]);
+        l2.push_back(e[1]);
+        linf.push_back(e[2]);
+        std::cout << "   L1 error " << std::scientific << std::setprecision(5) << e[0] << " after " << g.iter
+                  << " steps, t = " << std::defaultfloat << g.time << std::endl;
+      } else {
+        std::ofstream sol(soln_dir + "/sol_final.dat");
+        sol << std::setprecision(17);
+        for (long long c = 0; c < L.n; c++) {
+          for (int v = 0; v < L.nvar; v++) sol << prim[v * L.n + c] << (v + 1 < L.nvar ? " " : "\n");
+        }
+        std::cout << "   " << g.iter << " steps, t = " << g.time << std::endl;
+      }
+      dspw_status_out st;
+      dspw_last_status(h, &st);
+      if (st.code) std::cerr << "   device status: " << dspw_error_string(st.code) << std::endl;
+      dspw_destroy(h);
+    }
+    if (P.ooc) {
+      write_ooc(soln_dir + "/l1_err.dat", P, l1, levels);
+      write_ooc(soln_dir + "/l2_err.dat", P, l2, levels);
+      write_ooc(soln_dir + "/linf_err.dat", P, linf, levels);
+    }
+  } catch (const std::exception& e) {
+    std::cerr << "enflo_b200: " << e.what() << std::endl;
+    return 1;
+  }
+  return 0;
+}
