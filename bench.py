@@ -8,11 +8,17 @@ SSPRK3 step of every cell; one cell-update = one physical cell advanced by one
 step.  The FP64 plain form (SP-WENO, no network) is measured beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 2048] [--precision fp32_bf16|fp64] [--recon sp_weno_dl]
+                    [--workload kh|shu_osher|batched|tgv] [--n N]
+                    [--precision fp32_bf16|fp64] [--recon sp_weno_dl]
+
+The other workloads (dspw.workloads) time the remaining problem classes:
+1-D Euler Shu-Osher, the batch of the isentropic-vortex OOC list plus 4096
+Burgers problems, and the 3-D Navier-Stokes Taylor-Green vortex at 256^3.
 
 Under torchrun (N > 1) every rank advances its own 2048^2 problem (weak
 scaling, no data-path collective); NCCL only carries the barrier and the
-max-over-ranks of the device time.
+max-over-ranks of the device time.  The batched workload is one problem list
+shared out over the ranks by cell count (strong scaling, dspw.partition).
 
 `--impl reference` times the reference's own CPU solver (oracle/_ref, built
 from its sources) on bounded samples of the same workload, on all host cores.
@@ -42,22 +48,6 @@ NET_FILE = REPO / "tests" / "golden" / "dsp_weno.txt"
 # per-launch DRAM traffic of the dominant kernel from the committed ncu capture
 # (profiles/sweep_kernels_kh.md); None until measured
 NCU_TRAFFIC_BYTES_PER_CELL = None
-
-
-def kh_prim(n: int, seed: int = 12345) -> np.ndarray:
-    """Kelvin-Helmholtz on [0,1]^2: rho 2 / 1, u 0.5 / -0.5 inside / outside
-    |y-0.5| < 0.25, p 2.5, v = 0.01 sin(4 pi x) + U(-1e-3, 1e-3) seeded noise."""
-    h = 1.0 / n
-    x = (np.arange(n) + 0.5) * h
-    X, Y = np.meshgrid(x, x)
-    inner = np.abs(Y - 0.5) < 0.25
-    rng = np.random.default_rng(seed)
-    p = np.zeros((5, 1, n, n))
-    p[0, 0] = np.where(inner, 2.0, 1.0)
-    p[1, 0] = np.where(inner, 0.5, -0.5)
-    p[2, 0] = 0.01 * np.sin(4 * np.pi * X) + rng.uniform(-1e-3, 1e-3, (n, n))
-    p[4, 0] = 2.5
-    return p
 
 
 # ------------------------------------------------------------------ CPU legs
@@ -158,30 +148,77 @@ class ClockSampler:
 # ------------------------------------------------------------------ GPU legs
 
 
-def algorithmic_bytes(name, stage, ncell, nv, w):
-    """Minimum HBM bytes of one launch: x sweep reads U^k and writes R; the
-    final (y) sweep reads U^k, R and (stages 2-3) U^n and writes U^(k+1)."""
-    if name == "sweep_x":
-        return ncell * nv * w * 2
-    if name in ("sweep_y", "sweep_z"):
-        return ncell * nv * w * (4 if stage > 0 else 3)
-    return 0
+def algorithmic_bytes(name, stage, probs, w):
+    """Minimum HBM bytes of one launch of kernel ``name`` in SSPRK3 stage
+    ``stage`` over problems ``probs`` = [(cells, nv, dim, ns)], nv the stored
+    components, w the word size.  Euler / scalar: the x sweep reads U^k and
+    writes R, middle sweeps read U^k and R and write R, the last sweep reads U^k,
+    R (absent in 1-D) and, in stages 2-3, U^n and writes U^(k+1).  Navier-Stokes:
+    entropy variables read U and write V; node fluxes read V and write 3 nv per
+    node; the sweeps only accumulate R; the viscous update reads the node fluxes,
+    R, U^k (and U^n) and writes U^(k+1)."""
+    tot = 0
+    for cells, nv, dim, ns in probs:
+        upd = 4 if stage > 0 else 3
+        b = 0
+        if ns:
+            b = {"entvars": 2, "visc_nodes": 4, "sweep_x": 2, "sweep_y": 3, "sweep_z": 3,
+                 "visc_update": 3 + upd}.get(name, 0)
+        elif name.startswith("sweep_"):
+            axis = "xyz".index(name[-1])
+            if axis < dim:
+                if axis == dim - 1:
+                    b = upd if dim > 1 else upd - 1
+                else:
+                    b = 2 if axis == 0 else 3
+        tot += cells * nv * w * b
+    return tot
+
+
+def build_workload(args, precision, recon, rank, world):
+    """(descs, prims, cells of this rank, cells of all ranks, scaling)."""
+    from dspw import load_network_file, workloads as W
+    from dspw.partition import partition
+
+    net = load_network_file(NET_FILE)
+    if args.workload == "kh":
+        d, p, c = W.kh(args.n or 2048, precision, recon, net, seed=12345 + rank)
+        return d, p, c, c * world, "weak"
+    if args.workload == "shu_osher":
+        d, p, c = W.shu_osher(args.n or 25600, precision, recon, net)
+        return d, p, c, c * world, "weak"
+    if args.workload == "tgv":
+        d, p, c = W.tgv(args.n or 256, precision, recon, net)
+        return d, p, c, c * world, "weak"
+    # batched: one fixed problem list shared out by cell count (strong scaling)
+    specs = W.batched_specs()
+    cells = [W.spec_cells(s) for s in specs]
+    mine = partition(cells, world)[rank]
+    d, p, c = W.batched(precision, recon, net, select=mine)
+    return d, p, c, sum(cells), "strong"
+
+
+def prob_info(descs):
+    out = []
+    for d in descs:
+        dim = 1 + (d.ny > 1) + (d.nz > 1)
+        nv = 1 if d.model in (0, 1) else dim + 2
+        out.append((d.nx * d.ny * d.nz, nv, dim, d.model == 3))
+    return out
 
 
 def measure_gpu(args, torch, dist, rank, world):
     import dspw
-    from dspw import Solver, load_network_file, make_desc
+    from dspw import Solver
 
-    n = args.n
-    net = load_network_file(NET_FILE)
-    prim = kh_prim(n, seed=12345 + rank)
     dev = torch.device("cuda", torch.cuda.current_device())
+    descs, prims, ncell, ncell_all, scaling = build_workload(args, args.precision, args.recon, rank, world)
+    probs = prob_info(descs)
 
-    def solver(precision, recon):
-        d = make_desc(model="euler", flux="kepes_tecno4_roe", recon=recon, nx=n, ny=n, nz=1, x=(0, 1), y=(0, 1),
-                      bc="periodic", cfl=0.4, final_time=1.0e9, network=net, precision=precision)
+    def solver(d, pr):
         s = Solver(d)
-        s.upload_prim(prim)
+        for p, a in enumerate(pr):
+            s.upload_prim(a, p)
         return s
 
     def timed(s, steps, warmup):
@@ -205,7 +242,7 @@ def measure_gpu(args, torch, dist, rank, world):
             ms = float(t.item())
         return ms
 
-    s = solver(args.precision, args.recon)
+    s = solver(descs, prims)
     if args.profile_only:
         s.step(args.warmup)
         s.step(args.steps)
@@ -216,53 +253,60 @@ def measure_gpu(args, torch, dist, rank, world):
     ms = timed(s, args.steps, args.warmup)
     clk = clocks.stop()
     st = s.status()
-    g = s.globals()
     # per-kernel durations of one (un-graphed) step for the roofline
     prof = s.profile_step()
-    nv, w = 4, (4 if args.precision == "fp32_bf16" else 8)
+    w = 4 if args.precision == "fp32_bf16" else 8
+    first = "entvars" if any(p[3] for p in probs) else "sweep_x"   # the first launch of a stage
     stage, rows = -1, []
     for name, kms in prof:
-        if name == "sweep_x":
+        if name == first:
             stage += 1
         rows.append((name, stage, kms))
     dom = max(rows, key=lambda r: r[2])
-    ncell = n * n
-    dom_bytes = algorithmic_bytes(dom[0], dom[1], ncell, nv, w)
+    dom_bytes = algorithmic_bytes(dom[0], dom[1], probs, w)
     peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text()) if (REPO / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = dom_bytes / (dom[2] * 1e-3) / 1e9
-    # e2e through the C ABI with host buffers: upload (pinned H2D), one step,
-    # download (D2H) per step
-    pinned = torch.empty(prim.size, dtype=torch.float64, pin_memory=True).numpy().reshape(prim.shape)
-    pinned[...] = prim
-    out = torch.empty(prim.size, dtype=torch.float64, pin_memory=True).numpy().reshape(prim.shape)
-    e2e_steps = max(2, min(args.steps, 10))
-    s.upload_prim(pinned)
+    # e2e through the C ABI with host buffers: upload every problem (pinned
+    # H2D), one step, download every problem (D2H) per step
+    pinned, outs = [], []
+    for a in prims:
+        hp = torch.empty(a.size, dtype=torch.float64, pin_memory=True).numpy().reshape(a.shape)
+        hp[...] = a
+        pinned.append(hp)
+        outs.append(torch.empty(a.size, dtype=torch.float64, pin_memory=True).numpy().reshape(a.shape))
+    e2e_steps = max(2, min(args.steps, 10 if len(prims) < 16 else 2))
     lib = dspw.lib()
+    for p, a in enumerate(pinned):
+        s.upload_prim(a, p)
     s.step(1)
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        dspw.check(lib.dspw_upload_prim(s.h, 0, pinned), "upload")
+        for p, a in enumerate(pinned):
+            dspw.check(lib.dspw_upload_prim(s.h, p, a), "upload")
         dspw.check(lib.dspw_step(s.h, 1, 0.0), "step")
-        dspw.check(lib.dspw_download_cons(s.h, 0, out), "download")
+        for p, a in enumerate(outs):
+            dspw.check(lib.dspw_download_cons(s.h, p, a), "download")
     e2e_s = time.perf_counter() - t0
     if dist is not None:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    # FP64 plain form (SP-WENO, no network) on the same grid for the ratio
+    del s
+    # FP64 plain form (SP-WENO, no network) on the same workload for the ratio
     fp64_ms = None
     if args.precision == "fp32_bf16" and not args.no_fp64:
-        s64 = solver("fp64", "sp_weno")
+        d64, p64, _, _, _ = build_workload(args, "fp64", "sp_weno", rank, world)
+        s64 = solver(d64, p64)
         k64 = max(1, args.steps // 4)
         fp64_ms = timed(s64, k64, max(1, args.warmup // 2)) / k64
         del s64
-    launches_per_step = len(prof)
-    return dict(ms=ms, clk=clk, status=st, globals=g, prof=rows, dom=dom, dom_bytes=dom_bytes, achieved=achieved,
-                peak=peak, e2e_s=e2e_s, e2e_steps=e2e_steps, ncell=ncell, launches=launches_per_step,
-                fp64_ms=fp64_ms, h2d=prim.nbytes, d2h=prim.nbytes)
+    nbytes = sum(a.nbytes for a in prims)
+    return dict(ms=ms, clk=clk, status=st, prof=rows, dom=dom, dom_bytes=dom_bytes, achieved=achieved,
+                peak=peak, e2e_s=e2e_s, e2e_steps=e2e_steps, ncell=ncell, ncell_all=ncell_all, scaling=scaling,
+                launches=len(prof), fp64_ms=fp64_ms, h2d=nbytes, d2h=nbytes, nprob=len(descs))
 
 
 def main():
@@ -271,7 +315,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--workload", default="kh", choices=["kh", "shu_osher", "batched", "tgv"],
+                    help="kh: 2-D Euler KH (the headline); shu_osher: 1-D Euler; batched: vortex OOC list plus "
+                         "4096 Burgers problems in one batch (shared out over ranks); tgv: 3-D Navier-Stokes "
+                         "Taylor-Green vortex")
+    ap.add_argument("--n", type=int, default=None, help="grid size (kh 2048, shu_osher 25600, tgv 256)")
     ap.add_argument("--precision", default="fp32_bf16", choices=["fp32_bf16", "fp64"])
     ap.add_argument("--recon", default="sp_weno_dl")
     ap.add_argument("--cpu-sample-n", type=int, default=128)
@@ -285,13 +333,33 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    workload = f"kh{args.n}_{args.precision}_{args.recon}_kepes_tecno4_roe"
-    config = {"workload": workload, "grid": [args.n, args.n], "model": "euler2d", "flux": "kepes_tecno4_roe",
-              "recon": args.recon, "precision": args.precision, "cfl": 0.4,
-              "l2": "no flush: per-step working set (U^n, two stage buffers, residual) exceeds the 126 MB L2"}
+    if args.workload == "kh":
+        n = args.n or 2048
+        config = {"workload": f"kh{n}_{args.precision}_{args.recon}_kepes_tecno4_roe", "grid": [n, n],
+                  "model": "euler2d", "flux": "kepes_tecno4_roe", "recon": args.recon, "precision": args.precision,
+                  "cfl": 0.4}
+    elif args.workload == "shu_osher":
+        n = args.n or 25600
+        config = {"workload": f"shu_osher{n}_{args.precision}_{args.recon}_kepes_tecno4_roe", "grid": [n],
+                  "model": "euler1d", "flux": "kepes_tecno4_roe", "recon": args.recon, "precision": args.precision,
+                  "cfl": 0.4}
+    elif args.workload == "batched":
+        config = {"workload": f"batched_vortex_ooc_burgers4096_{args.precision}_{args.recon}",
+                  "problems": "isentropic vortex at 64..2048^2 (6 levels, kepes_tecno4_roe) + 4096 Burgers "
+                              "Nx~U{100..5000} (bur_tecno4), one batch per rank, shared out by cell count",
+                  "recon": args.recon, "precision": args.precision, "cfl": 0.5}
+    else:
+        n = args.n or 256
+        config = {"workload": f"tgv{n}_ns_es_{args.precision}_{args.recon}_kepes_tecno4_roe", "grid": [n, n, n],
+                  "model": "ns_es", "flux": "kepes_tecno4_roe", "recon": args.recon, "precision": args.precision,
+                  "cfl": 0.4, "Re": 1600, "Mach": 0.1}
+    config["l2"] = "no flush: per-step working set (U^n, two stage buffers, residual) exceeds the 126 MB L2"
 
     if args.impl == "reference":
         if rank != 0:
+            return
+        if args.workload != "kh":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm samples the KH workload only"}))
             return
         procs = cpu_cores()
         pool = RefPool(args.cpu_sample_n, args.recon, procs)
@@ -317,7 +385,10 @@ def main():
 
     # CPU baseline first (spawned processes, before any GPU call)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if args.workload != "kh":
+        cpu = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
+               "sample": "not sampled: the CPU baseline covers the KH workload"}
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             procs = cpu_cores()
             pool = RefPool(args.cpu_sample_n, args.recon, procs)
@@ -352,8 +423,8 @@ def main():
     if rank != 0:
         return
     steps = args.steps
-    value = world * r["ncell"] * steps / (r["ms"] * 1e-3)
-    e2e_v = world * r["ncell"] * r["e2e_steps"] / r["e2e_s"]
+    value = r["ncell_all"] * steps / (r["ms"] * 1e-3)
+    e2e_v = r["ncell_all"] * r["e2e_steps"] / r["e2e_s"]
     dom = r["dom"]
     traffic = None
     if NCU_TRAFFIC_BYTES_PER_CELL is not None:
@@ -361,7 +432,7 @@ def main():
         traffic = traffic * r["ncell"] if traffic else None
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": r["ms"] / steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": r["ms"] / steps, "higher_is_better": True, "scaling": r["scaling"],
         "vs_baseline": None, "dtype": "f32" if args.precision == "fp32_bf16" else "f64", "data": "synthetic",
         "config": config,
         "roofline": {"bound": "hbm", "kernel": dom[0], "stage": dom[1], "achieved": r["achieved"],
@@ -379,7 +450,7 @@ def main():
                    "nonfinite": r["status"].nonfinite_cells, "nonpositive": r["status"].nonpositive_cells},
     }
     if r["fp64_ms"]:
-        line["fp64_plain"] = {"value": world * r["ncell"] / (r["fp64_ms"] * 1e-3), "ms_per_step": r["fp64_ms"],
+        line["fp64_plain"] = {"value": r["ncell_all"] / (r["fp64_ms"] * 1e-3), "ms_per_step": r["fp64_ms"],
                               "recon": "sp_weno", "speedup_fp32_bf16_dl_over_fp64_plain": r["fp64_ms"] / (r["ms"] / steps)}
     print(json.dumps(line))
 

@@ -216,5 +216,6 @@ def test_ooc_study_through_driver(tmp_path, recon):
             # the table carries 6 significant digits
             assert abs(r[1] - ref[i, col]) <= 5e-6 * ref[i, col], (fname, i, r, ref[i, col])
         rate = float(rows[2][2])
-        assert 2.5 < rate < 4.5
+        # L1 converges at third order; L-inf is limited near the extrema of sin^4
+        assert (2.5 < rate < 4.5) if col == 0 else (1.5 < rate < 4.5), (fname, rate)
     assert (soln / "globals.dat").exists()
