@@ -99,6 +99,7 @@ struct dspw_handle {
   int time_scheme = 1;
   int has_ns = 0;
   int maxdim = 1;
+  int spec = 0;                        // sweep kernel specialisation (spec_code), 0 generic
   std::vector<dspw_desc> desc;
   std::vector<ProbDev> hprob;
   std::vector<long long> cell_start;   // nprob + 1
@@ -291,6 +292,17 @@ NetParams make_net(const dspw_desc& dn) {
   return np;
 }
 
+// A batch of Euler / NS problems of one dimension, all with the 4th-order
+// KEPEC central part plus TeCNO dissipation and one reconstruction family,
+// runs the specialised sweep kernels; any other batch the generic ones.
+int choose_spec(const std::vector<ProbDev>& ps) {
+  const int dim = ps[0].dim;
+  const bool dl = ps[0].spw_corr < 0;
+  for (const ProbDev& P : ps)
+    if (P.is_scalar || P.dim != dim || P.central != 0 || !P.fourth || !P.tecno || (P.spw_corr < 0) != dl) return 0;
+  return spec_code(dim, dl ? 2 : 1);
+}
+
 int tasks_for(const ProbDev& P, int dir) {
   if (dir >= P.dim) return 0;
   int N[3] = {P.nx, P.ny, P.nz};
@@ -354,7 +366,7 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
     // NS problems never update in a sweep; mixed batches are not formed with NS
     if (h->has_ns) a.viscous = 1;
     int grid = (nt + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
-    CK(Launch<T>::sweep(dir, a, grid, h->stream));
+    CK(Launch<T>::sweep(dir, a, grid, h->stream, h->spec));
     prof_mark(h, dir == 0 ? "sweep_x" : (dir == 1 ? "sweep_y" : "sweep_z"));
   }
   if (h->has_ns) {
@@ -477,6 +489,7 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
       if (descs[p].model != DSPW_NS_ES) { delete h; return DSPW_ERR_UNSUPPORTED; }
   }
   h->ctot = off;
+  h->spec = choose_spec(h->hprob);
   for (int dir = 0; dir < 3; dir++) {
     h->task_start[dir].push_back(0);
     for (int p = 0; p < nprob; p++) {

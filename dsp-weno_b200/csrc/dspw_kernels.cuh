@@ -18,6 +18,7 @@
 // of inactive directions are identically zero in the reference and are not
 // stored.
 #pragma once
+#include <cstddef>
 #include "dspw_math.cuh"
 #include "../../include/dspw.h"
 
@@ -54,6 +55,27 @@ struct ProbDev {
   double cfl, final_time, t_interval;
   double bc_state[6][5];
 };
+
+// Compile-time specialisation of the sweep kernels.  The generic kernel reads
+// the flux structure and the reconstruction from ProbDev at run time and holds
+// the code of every model, dimension and flux.  A batch whose problems are all
+// Euler / Navier-Stokes of one dimension with the 4th-order KEPEC central part
+// and TeCNO dissipation (kepes_tecno4_roe, kepes_tecno4_rusanov) and one
+// reconstruction family runs a kernel with those choices fixed (Roe / Rusanov,
+// EC1_fix and the SP-WENO correction stay run-time flags).
+struct SpecGeneric {
+  static constexpr bool fixed = false;
+  static constexpr int dim = 0;
+  static constexpr int rec = 0;
+};
+template <int DIM_, int REC_>   // REC_: 1 SP-WENO family, 2 DSP-WENO network
+struct SpecHot {
+  static constexpr bool fixed = true;
+  static constexpr int dim = DIM_;
+  static constexpr int rec = REC_;
+};
+// host-side code of a specialisation: 0 generic, else 10 * dim + rec
+constexpr int spec_code(int dim, int rec) { return 10 * dim + rec; }
 
 struct ProbState {
   double time, dt, t_save, factor;
@@ -293,8 +315,10 @@ DSPW_HD bool sign_violation(T z0, T z1, T z2, T z3, T zl, T zr) {
 // ------------------------------------------------------ warp shared memory --
 
 // staging of the network inputs / outputs of one warp (FP32 form only)
-template <typename T> struct NetScratch { float feat[32][8]; float logit[32][8]; };
-template <> struct NetScratch<double> { float feat[1][8]; float logit[1][8]; };
+// per-warp scratch of the tensor-core network (FP32 form): the staged inputs,
+// the logits, and each lane's B fragments and biases (loaded once per kernel)
+template <typename T> struct NetScratch { float feat[32][8]; float logit[32][8]; uint32_t frag[32][12]; };
+template <> struct NetScratch<double> { float feat[1][8]; float logit[1][8]; uint32_t frag[1][12]; };
 
 template <typename T>
 struct WarpSmem {
@@ -304,6 +328,12 @@ struct WarpSmem {
   T F[5][32];      // face fluxes, face f = c0 + idx
   NetScratch<T> ns;
 };
+// mlp_warp_tiles addresses the scratch by these byte offsets, with 16-byte
+// vector accesses to the rows of every warp's scratch
+static_assert(offsetof(NetScratch<float>, logit) == 1024 && offsetof(NetScratch<float>, frag) == 2048,
+              "NetScratch<float> layout");
+static_assert(offsetof(WarpSmem<float>, ns) % 16 == 0 && sizeof(WarpSmem<float>) % 16 == 0,
+              "WarpSmem<float> alignment");
 
 // ---------------------------------------------------- two-point fluxes ------
 
@@ -435,44 +465,127 @@ __device__ inline void net_frag_load(const NetParams& P, int lane, NetFrag& nf) 
   }
 }
 
-DSPW_HD void mma_bf16_16x8x8(float c[4], uint32_t a0, uint32_t a1, uint32_t b0) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(b0));
-}
-
-// in: feat (this lane's 5 inputs); out: logits (this lane's 5 outputs)
-__device__ inline void warp_mlp_bf16(const NetFrag& nf, float (*fs)[8], float (*ls)[8], const float in[5],
-                                     float out[5], int lane) {
-#pragma unroll
-  for (int k = 0; k < 5; k++) fs[lane][k] = in[k];
-  fs[lane][5] = 0.f; fs[lane][6] = 0.f; fs[lane][7] = 0.f;
-  __syncwarp();
-  int r = lane >> 2, kq = (lane & 3) * 2;
-#pragma unroll
-  for (int t = 0; t < 2; t++) {
-    uint32_t a0 = pack_bf16(fs[16 * t + r][kq], fs[16 * t + r][kq + 1]);
-    uint32_t a1 = pack_bf16(fs[16 * t + r + 8][kq], fs[16 * t + r + 8][kq + 1]);
-    float c[4];
+// each lane stores its fragments into its warp's scratch (once per kernel)
+template <typename T>
+__device__ inline void net_frag_stage(const NetParams& P, int lane, NetScratch<T>& ns) {
+  if constexpr (sizeof(T) == 4) {
+    NetFrag nf;
+    net_frag_load(P, lane, nf);
 #pragma unroll
     for (int l = 0; l < 4; l++) {
-      c[0] = nf.bias0[l]; c[1] = nf.bias1[l]; c[2] = nf.bias0[l]; c[3] = nf.bias1[l];
-      mma_bf16_16x8x8(c, a0, a1, nf.b[l]);
-      if (l < 3) {
-        a0 = pack_bf16(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f));
-        a1 = pack_bf16(fmaxf(c[2], 0.f), fmaxf(c[3], 0.f));
-      }
+      ns.frag[lane][l] = nf.b[l];
+      ns.frag[lane][4 + l] = __float_as_uint(nf.bias0[l]);
+      ns.frag[lane][8 + l] = __float_as_uint(nf.bias1[l]);
     }
-    ls[16 * t + r][kq] = c[0];
-    ls[16 * t + r][kq + 1] = c[1];
-    ls[16 * t + r + 8][kq] = c[2];
-    ls[16 * t + r + 8][kq + 1] = c[3];
+    __syncwarp();
+  }
+}
+
+// The four layers of one 16-row tile as one PTX block: A fragments loaded from
+// the staged inputs (rows r and r + 8, columns kq and kq + 1), bias-initialised
+// FP32 accumulators, m16n8k8 BF16 MMA, ReLU and BF16 repacking of the C
+// fragment as the next layer's A fragment, and the logits stored back to
+// shared memory.
+__device__ inline void mlp_tile_bf16(const NetFrag& nf, unsigned in_lo, unsigned in_hi, unsigned out_lo,
+                                     unsigned out_hi) {
+  asm volatile(
+      "{\n\t"
+      ".reg .f32 %%x<4>, %%c<4>;\n\t"
+      ".reg .b32 %%a<2>;\n\t"
+      "ld.shared.v2.f32 {%%x0, %%x1}, [%0];\n\t"
+      "ld.shared.v2.f32 {%%x2, %%x3}, [%1];\n\t"
+      "cvt.rn.bf16x2.f32 %%a0, %%x1, %%x0;\n\t"
+      "cvt.rn.bf16x2.f32 %%a1, %%x3, %%x2;\n\t"
+      "mov.f32 %%c0, %8;\n\t"
+      "mov.f32 %%c1, %9;\n\t"
+      "mov.f32 %%c2, %8;\n\t"
+      "mov.f32 %%c3, %9;\n\t"
+      "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%%c0,%%c1,%%c2,%%c3}, {%%a0,%%a1}, {%4}, "
+      "{%%c0,%%c1,%%c2,%%c3};\n\t"
+      "max.f32 %%c0, %%c0, 0f00000000;\n\t"
+      "max.f32 %%c1, %%c1, 0f00000000;\n\t"
+      "max.f32 %%c2, %%c2, 0f00000000;\n\t"
+      "max.f32 %%c3, %%c3, 0f00000000;\n\t"
+      "cvt.rn.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
+      "cvt.rn.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
+      "mov.f32 %%c0, %10;\n\t"
+      "mov.f32 %%c1, %11;\n\t"
+      "mov.f32 %%c2, %10;\n\t"
+      "mov.f32 %%c3, %11;\n\t"
+      "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%%c0,%%c1,%%c2,%%c3}, {%%a0,%%a1}, {%5}, "
+      "{%%c0,%%c1,%%c2,%%c3};\n\t"
+      "max.f32 %%c0, %%c0, 0f00000000;\n\t"
+      "max.f32 %%c1, %%c1, 0f00000000;\n\t"
+      "max.f32 %%c2, %%c2, 0f00000000;\n\t"
+      "max.f32 %%c3, %%c3, 0f00000000;\n\t"
+      "cvt.rn.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
+      "cvt.rn.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
+      "mov.f32 %%c0, %12;\n\t"
+      "mov.f32 %%c1, %13;\n\t"
+      "mov.f32 %%c2, %12;\n\t"
+      "mov.f32 %%c3, %13;\n\t"
+      "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%%c0,%%c1,%%c2,%%c3}, {%%a0,%%a1}, {%6}, "
+      "{%%c0,%%c1,%%c2,%%c3};\n\t"
+      "max.f32 %%c0, %%c0, 0f00000000;\n\t"
+      "max.f32 %%c1, %%c1, 0f00000000;\n\t"
+      "max.f32 %%c2, %%c2, 0f00000000;\n\t"
+      "max.f32 %%c3, %%c3, 0f00000000;\n\t"
+      "cvt.rn.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
+      "cvt.rn.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
+      "mov.f32 %%c0, %14;\n\t"
+      "mov.f32 %%c1, %15;\n\t"
+      "mov.f32 %%c2, %14;\n\t"
+      "mov.f32 %%c3, %15;\n\t"
+      "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%%c0,%%c1,%%c2,%%c3}, {%%a0,%%a1}, {%7}, "
+      "{%%c0,%%c1,%%c2,%%c3};\n\t"
+      "st.shared.v2.f32 [%2], {%%c0, %%c1};\n\t"
+      "st.shared.v2.f32 [%3], {%%c2, %%c3};\n\t"
+      "}\n"
+      :
+      : "r"(in_lo), "r"(in_hi), "r"(out_lo), "r"(out_hi), "r"(nf.b[0]), "r"(nf.b[1]), "r"(nf.b[2]), "r"(nf.b[3]),
+        "f"(nf.bias0[0]), "f"(nf.bias1[0]), "f"(nf.bias0[1]), "f"(nf.bias1[1]), "f"(nf.bias0[2]), "f"(nf.bias1[2]),
+        "f"(nf.bias0[3]), "f"(nf.bias1[3])
+      : "memory");
+}
+
+// The warp-wide part of one network evaluation: both tiles, between two warp
+// barriers.  mma.sync.aligned requires every lane of the warp to execute the
+// same instruction.  Inlined into lane-divergent code, the compiler may emit
+// several copies of the MMA sequence and send different lanes through
+// different copies, which yields wrong logits; as a separate function there
+// is exactly one copy that every lane calls.  ns_addr is the shared-memory
+// address of the warp's NetScratch.
+static __device__ __noinline__ void mlp_warp_tiles(unsigned ns_addr) {
+  __syncwarp();
+  unsigned lane;
+  asm("mov.u32 %0, %%laneid;" : "=r"(lane));
+  NetFrag nf;
+  const unsigned fa = ns_addr + 2048u + lane * 48u;   // frag[lane][0..11]
+  asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(nf.b[0]), "=r"(nf.b[1]), "=r"(nf.b[2]), "=r"(nf.b[3]) : "r"(fa));
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(nf.bias0[0]), "=f"(nf.bias0[1]), "=f"(nf.bias0[2]), "=f"(nf.bias0[3]) : "r"(fa + 16u));
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(nf.bias1[0]), "=f"(nf.bias1[1]), "=f"(nf.bias1[2]), "=f"(nf.bias1[3]) : "r"(fa + 32u));
+  const unsigned r = lane >> 2, kq = (lane & 3) * 2;
+#pragma unroll
+  for (unsigned t = 0; t < 2; t++) {
+    const unsigned lo = ((16 * t + r) * 8 + kq) * 4, hi = ((16 * t + r + 8) * 8 + kq) * 4;
+    mlp_tile_bf16(nf, ns_addr + lo, ns_addr + hi, ns_addr + 1024u + lo, ns_addr + 1024u + hi);
   }
   __syncwarp();
-#pragma unroll
-  for (int k = 0; k < 5; k++) out[k] = ls[lane][k];
-  __syncwarp();
+}
+
+// in: this lane's 5 inputs; out: this lane's 5 logits.  Every lane of the
+// warp must call it.
+__device__ inline void warp_mlp_bf16(NetScratch<float>& ns, const float in[5], float out[5], int lane) {
+  float4* f = reinterpret_cast<float4*>(&ns.feat[lane][0]);
+  f[0] = make_float4(in[0], in[1], in[2], in[3]);
+  f[1] = make_float4(in[4], 0.f, 0.f, 0.f);
+  mlp_warp_tiles((unsigned)__cvta_generic_to_shared(&ns));
+  const float4 o = *reinterpret_cast<const float4*>(&ns.logit[lane][0]);
+  out[0] = o.x; out[1] = o.y; out[2] = o.z; out[3] = o.w;
+  out[4] = ns.logit[lane][4];
 }
 
 // DSP-WENO reconstruction of one stencil per lane, warp-cooperative network.
@@ -480,18 +593,18 @@ __device__ inline void warp_mlp_bf16(const NetFrag& nf, float (*fs)[8], float (*
 // lanes whose result is unused.  Returns 1 if the sign-preserving limiter had
 // to act (FP32 form).
 template <typename T>
-__device__ inline int dsp_weno_warp(const NetParams& NP, const NetFrag& nf, WarpSmem<T>* sm, int lane, bool valid,
+__device__ inline int dsp_weno_warp(const NetParams& NP, WarpSmem<T>* sm, int lane, bool valid,
                                     T u0, T u1, T u2, T u3, T& l, T& r);
 
 template <>
-__device__ inline int dsp_weno_warp<double>(const NetParams& NP, const NetFrag&, WarpSmem<double>*, int, bool valid,
+__device__ inline int dsp_weno_warp<double>(const NetParams& NP, WarpSmem<double>*, int, bool valid,
                                             double u0, double u1, double u2, double u3, double& l, double& r) {
   if (valid) dsp_weno_fp64(NP, u0, u1, u2, u3, l, r);
   return 0;
 }
 
 template <>
-__device__ inline int dsp_weno_warp<float>(const NetParams& NP, const NetFrag& nf, WarpSmem<float>* sm, int lane,
+__device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>* sm, int lane,
                                            bool valid, float u0, float u1, float u2, float u3, float& l, float& r) {
   // The reference skips the network when |u2 - u1| < 1e-15 (reconstruct.cc:152);
   // in FP32 the equivalent "no jump" test is a jump of a few ulps of the values,
@@ -511,7 +624,7 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, const NetFrag& n
     for (int k = 0; k < 5; k++) inbox = inbox && feat[k] >= NP.feat_lo[k] && feat[k] <= NP.feat_hi[k];
   }
   float lg[5];
-  warp_mlp_bf16(nf, sm->ns.feat, sm->ns.logit, feat, lg, lane);
+  warp_mlp_bf16(sm->ns, feat, lg, lane);
   if (!valid) return 0;
   if (guard) { l = 0.f; r = 0.f; return 0; }
   if (!finite || !inbox) {   // degenerate features or outside the training range: plain SP-WENO
@@ -530,13 +643,13 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, const NetFrag& n
   return 0;
 }
 
-template <typename T>
-__device__ inline void reconstruct_lane(const ProbDev& P, const NetParams& NP, const NetFrag& nf, WarpSmem<T>* sm,
+template <typename T, typename Sp>
+__device__ inline void reconstruct_lane(const ProbDev& P, const NetParams& NP, WarpSmem<T>* sm,
                                         int lane, bool valid, T s0, T s1, T s2, T s3, T& l, T& r, int& viol) {
-  if (P.spw_corr >= 0) {
+  if (Sp::fixed ? Sp::rec == 1 : P.spw_corr >= 0) {
     if (valid) sp_weno<T>(s0, s1, s2, s3, P.spw_corr, l, r);
   } else {
-    viol += dsp_weno_warp<T>(NP, nf, sm, lane, valid, s0, s1, s2, s3, l, r);
+    viol += dsp_weno_warp<T>(NP, sm, lane, valid, s0, s1, s2, s3, l, r);
   }
 }
 
@@ -546,9 +659,9 @@ __device__ inline void reconstruct_lane(const ProbDev& P, const NetParams& NP, c
 // and the Roe / Rusanov variants), R = eigenvectors scaled by S^(1/2), Z = R^T V
 // of the 4 stencil cells, component-wise reconstruction.  Columns of R are
 // built one at a time; Diff[i] accumulates over j in the reference's order.
-template <typename T, int DIR, int DIM>
+template <typename T, int DIR, int DIM, typename Sp>
 __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P, const NetParams& NP,
-                                         const NetFrag& nf, WarpSmem<T>* sm, int lane, bool valid, int q0,
+                                         WarpSmem<T>* sm, int lane, bool valid, int q0,
                                          const FaceAvg<T>& fa, T flux[5], int& viol, unsigned long long& signv,
                                          unsigned collect_salt) {
   typedef Mth<T> m;
@@ -609,7 +722,7 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
       z[k] = T(0.0) + acc;
     }
     T zl = T(0), zr = T(0);
-    reconstruct_lane<T>(P, NP, nf, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol);
+    reconstruct_lane<T, Sp>(P, NP, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol);
     if (A.collect_buf && valid)
       collect_pair<T>(A, (unsigned)(blockIdx.x * 1024 + threadIdx.x) * 8u + (unsigned)j + 977u * collect_salt,
                       z[0], z[1], z[2], z[3], zl, zr);
@@ -754,17 +867,19 @@ __device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int la
 
 // Faces of one staged line segment (phases B and C): wide two-point fluxes,
 // face central flux, TeCNO dissipation; face fluxes end in sm->F.
-template <typename T, int DIR, int DIM>
-__device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, const NetFrag& nf, WarpSmem<T>* sm,
+template <typename T, int DIR, int DIM, typename Sp>
+__device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, WarpSmem<T>* sm,
                                    int lane, int ncell, int& viol, unsigned long long& signv, unsigned& checked,
                                    unsigned collect_salt = 0) {
   const T G = T(P.gamma), Rg = T(P.gas_const), area = T(P.area[DIR]);
   // phase B: wide two-point flux centred at g = c0 - 1 + lane (cells g-1, g+1)
-  if (P.fourth && lane <= ncell + 1) {
+  const bool fourth = Sp::fixed || P.fourth;
+  if (fourth && lane <= ncell + 1) {
     T Fw[5], Pl[5], Pr[5];
 #pragma unroll
     for (int v = 0; v < 5; v++) { Pl[v] = sm->P[v][lane]; Pr[v] = sm->P[v][lane + 2]; }
-    central_pair<T, DIR>(P.central, Pl, Pr, G, Rg, area, Fw);
+    if (Sp::fixed) kepec_pair<T, DIR>(Pl, Pr, G, Rg, area, Fw);
+    else central_pair<T, DIR>(P.central, Pl, Pr, G, Rg, area, Fw);
 #pragma unroll
     for (int v = 0; v < 5; v++) sm->W[v][lane] = Fw[v];
   }
@@ -780,9 +895,9 @@ __device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, cons
     for (int v = 0; v < 5; v++) { Pl[v] = sm->P[v][ql]; Pr[v] = sm->P[v][ql + 1]; }
     face_avg<T, DIR>(Pl, Pr, Rg, fa);
     T Fn[5];
-    if (P.central == 0) kepec_from_avg<T, DIR>(fa, Pl, Pr, G, area, Fn);
+    if (Sp::fixed || P.central == 0) kepec_from_avg<T, DIR>(fa, Pl, Pr, G, area, Fn);
     else central_pair<T, DIR>(P.central, Pl, Pr, G, Rg, area, Fn);
-    if (P.fourth) {
+    if (fourth) {
       // kepec4 / roe_ec4 / kep4: 4/3 F(1,2) - 1/6 F(0,2) - 1/6 F(1,3) (enflo/src/kepec4.cc:10-38)
       const T fact = T(-1.0 / 6.0);
 #pragma unroll
@@ -798,11 +913,11 @@ __device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, cons
       for (int v = 0; v < 5; v++) flux[v] = Fn[v];
     }
   }
-  if (P.tecno) {
+  if (Sp::fixed || P.tecno) {
     const T ra = T(P.rarea[DIR]);
 #pragma unroll
     for (int v = 0; v < 5; v++) flux[v] *= ra;
-    tecno_dissipation<T, DIR, DIM>(A, P, *A.net, nf, sm, lane, valid, valid ? lane : 0, fa, flux, viol, signv,
+    tecno_dissipation<T, DIR, DIM, Sp>(A, P, *A.net, sm, lane, valid, valid ? lane : 0, fa, flux, viol, signv,
                                    collect_salt);
 #pragma unroll
     for (int v = 0; v < 5; v++) flux[v] *= area;
@@ -815,8 +930,8 @@ __device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, cons
   __syncwarp();
 }
 
-template <typename T, int DIR, int DIM>
-__device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S, const NetFrag& nf,
+template <typename T, int DIR, int DIM, typename Sp>
+__device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S,
                            WarpSmem<T>* sm, int lane, int lt) {
   int i0, j0, k0, c0, ncell;
   decode_task<DIR>(P, lt, i0, j0, k0, c0, ncell);
@@ -824,7 +939,7 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
   int viol = 0;
   unsigned long long signv = 0;
   unsigned checked = 0;
-  euler_faces<T, DIR, DIM>(A, P, nf, sm, lane, ncell, viol, signv, checked, (unsigned)lt);
+  euler_faces<T, DIR, DIM, Sp>(A, P, sm, lane, ncell, viol, signv, checked, (unsigned)lt);
   // phase D: cells
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
@@ -851,8 +966,8 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
 // the faces are evaluated per warp exactly as in euler_task.
 constexpr int COOP_COLS = WARPS_PER_BLOCK;
 
-template <typename T, int DIR, int DIM>
-__device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbState& S, const NetFrag& nf,
+template <typename T, int DIR, int DIM, typename Sp>
+__device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbState& S,
                                  WarpSmem<T>* sm0, int lt0) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int i0, j0, k0, c0, ncell;
@@ -887,7 +1002,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   int viol = 0;
   unsigned long long signv = 0;
   unsigned checked = 0;
-  euler_faces<T, DIR, DIM>(A, P, nf, sm0 + warp, lane, ncell, viol, signv, checked, (unsigned)(lt0 + warp));
+  euler_faces<T, DIR, DIM, Sp>(A, P, sm0 + warp, lane, ncell, viol, signv, checked, (unsigned)(lt0 + warp));
   __syncthreads();
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
   double smax = 0.0, ent = 0.0;
@@ -910,7 +1025,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
 // scalar laws: lin_/bur_ fluxes (enflo_scalar/src_scalar/num_flux.cc:12-57,
 // lin_tecno4.cc:10-31, lin_ec4.cc:10-34, bur_tecno4.cc:10-35, bur_ec4.cc:10-34)
 template <typename T, int DIR>
-__device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S, const NetFrag& nf,
+__device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S,
                             WarpSmem<T>* sm, int lane, int lt) {
   typedef Mth<T> m;
   int i0, j0, k0, c0, ncell;
@@ -957,7 +1072,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   if (P.tecno) {
     T D = (P.model == DSPW_LINADV) ? m::abs(vn) : T(0.5) * (m::abs(s1) + m::abs(s2));
     T l = T(0), r = T(0);
-    reconstruct_lane<T>(P, *A.net, nf, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
+    reconstruct_lane<T, SpecGeneric>(P, *A.net, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
     if (valid && sign_violation<T>(s0, s1, s2, s3, l, r)) signv++;
     if (A.collect_buf && valid) collect_pair<T>(A, (unsigned)lt * 32u + (unsigned)lane, s0, s1, s2, s3, l, r);
     flux -= T(0.5) * D * (r - l);
@@ -981,16 +1096,17 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   __syncwarp();
 }
 
-// One sweep of direction DIR over every problem of the batch.
-template <typename T, int DIR>
+// One sweep of direction DIR over every problem of the batch.  Sp fixes the
+// model, dimension and flux structure (SpecHot) or leaves them to ProbDev
+// (SpecGeneric); a SpecHot kernel is only launched for directions < its dim.
+template <typename T, int DIR, typename Sp>
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MinBlocks<T>::value)
 k_sweep(SweepArgs<T> A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem<T>* sm0 = reinterpret_cast<WarpSmem<T>*>(smem_raw);
   WarpSmem<T>* sm = sm0 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  NetFrag nf;
-  if (sizeof(T) == 4) net_frag_load(*A.net, lane, nf);
+  if (!Sp::fixed || Sp::rec == 2) net_frag_stage<T>(*A.net, lane, sm->ns);
   const int stride = gridDim.x * WARPS_PER_BLOCK;
   for (int base = blockIdx.x * WARPS_PER_BLOCK; base < A.ntask; base += stride) {
     if (DIR >= 1 && base + WARPS_PER_BLOCK <= A.ntask) {
@@ -998,15 +1114,17 @@ k_sweep(SweepArgs<T> A) {
       const int p = find_problem(A.task_start, A.nprob, base);
       const int lt0 = base - __ldg(A.task_start + p);
       const ProbDev& P = A.prob[p];
-      if (!P.is_scalar && base + WARPS_PER_BLOCK <= __ldg(A.task_start + p + 1) && (lt0 % P.nx) % COOP_COLS == 0 &&
-          (lt0 % P.nx) + COOP_COLS <= P.nx) {
+      if ((Sp::fixed || !P.is_scalar) && base + WARPS_PER_BLOCK <= __ldg(A.task_start + p + 1) &&
+          (lt0 % P.nx) % COOP_COLS == 0 && (lt0 % P.nx) + COOP_COLS <= P.nx) {
         ProbState& S = A.st[p];
         if (!A.residual_only && !*((volatile int*)&S.active)) continue;
-        if (DIR == 1) {
-          if (P.dim == 2) euler_coop_block<T, DIR, 2>(A, P, S, nf, sm0, lt0);
-          else euler_coop_block<T, DIR, 3>(A, P, S, nf, sm0, lt0);
+        if constexpr (Sp::fixed) {
+          euler_coop_block<T, DIR, Sp::dim, Sp>(A, P, S, sm0, lt0);
+        } else if (DIR == 1) {
+          if (P.dim == 2) euler_coop_block<T, DIR, 2, Sp>(A, P, S, sm0, lt0);
+          else euler_coop_block<T, DIR, 3, Sp>(A, P, S, sm0, lt0);
         } else {
-          euler_coop_block<T, DIR, 3>(A, P, S, nf, sm0, lt0);
+          euler_coop_block<T, DIR, 3, Sp>(A, P, S, sm0, lt0);
         }
         continue;
       }
@@ -1018,18 +1136,20 @@ k_sweep(SweepArgs<T> A) {
     ProbState& S = A.st[p];
     if (!A.residual_only && !*((volatile int*)&S.active)) continue;
     const int lt = task - __ldg(A.task_start + p);
-    if (P.is_scalar) {
-      scalar_task<T, DIR>(A, P, S, nf, sm, lane, lt);
+    if constexpr (Sp::fixed) {
+      euler_task<T, DIR, Sp::dim, Sp>(A, P, S, sm, lane, lt);
+    } else if (P.is_scalar) {
+      scalar_task<T, DIR>(A, P, S, sm, lane, lt);
     } else {
       if (DIR == 0) {
-        if (P.dim == 1) euler_task<T, DIR, 1>(A, P, S, nf, sm, lane, lt);
-        else if (P.dim == 2) euler_task<T, DIR, 2>(A, P, S, nf, sm, lane, lt);
-        else euler_task<T, DIR, 3>(A, P, S, nf, sm, lane, lt);
+        if (P.dim == 1) euler_task<T, DIR, 1, Sp>(A, P, S, sm, lane, lt);
+        else if (P.dim == 2) euler_task<T, DIR, 2, Sp>(A, P, S, sm, lane, lt);
+        else euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
       } else if (DIR == 1) {
-        if (P.dim == 2) euler_task<T, DIR, 2>(A, P, S, nf, sm, lane, lt);
-        else euler_task<T, DIR, 3>(A, P, S, nf, sm, lane, lt);
+        if (P.dim == 2) euler_task<T, DIR, 2, Sp>(A, P, S, sm, lane, lt);
+        else euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
       } else {
-        euler_task<T, DIR, 3>(A, P, S, nf, sm, lane, lt);
+        euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
       }
     }
   }
@@ -1371,8 +1491,7 @@ k_recon_batch(const ProbDev* prob, const NetParams* net, const double* u4, long 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem<T>* sm = reinterpret_cast<WarpSmem<T>*>(smem_raw) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  NetFrag nf;
-  if (sizeof(T) == 4) net_frag_load(*net, lane, nf);
+  net_frag_stage<T>(*net, lane, sm->ns);
   const long long nchunk = (n + 31) / 32;
   for (long long ch = blockIdx.x * (long long)WARPS_PER_BLOCK + (threadIdx.x >> 5); ch < nchunk;
        ch += (long long)gridDim.x * WARPS_PER_BLOCK) {
@@ -1382,7 +1501,7 @@ k_recon_batch(const ProbDev* prob, const NetParams* net, const double* u4, long 
     T s2 = valid ? T(u4[4 * i + 2]) : T(2), s3 = valid ? T(u4[4 * i + 3]) : T(3);
     T lo = T(0), ro = T(0);
     int viol = 0;
-    reconstruct_lane<T>(*prob, *net, nf, sm, lane, valid, s0, s1, s2, s3, lo, ro, viol);
+    reconstruct_lane<T, SpecGeneric>(*prob, *net, sm, lane, valid, s0, s1, s2, s3, lo, ro, viol);
     if (valid) { l[i] = (double)lo; r[i] = (double)ro; }
     unsigned v = __reduce_add_sync(0xffffffffu, (unsigned)viol);
     if (lane == 0 && v) atomicAdd(acts, (unsigned long long)v);
