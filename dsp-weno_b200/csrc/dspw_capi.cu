@@ -303,12 +303,16 @@ int choose_spec(const std::vector<ProbDev>& ps) {
   return spec_code(dim, dl ? 2 : 1);
 }
 
-int tasks_for(const ProbDev& P, int dir) {
+// Tasks of one problem in direction dir: warp tasks (one line segment each),
+// or, for the y / z sweeps of a specialised batch, block tasks of 8 adjacent
+// columns (decode_group).
+long long tasks_for(const ProbDev& P, int dir, bool groups) {
   if (dir >= P.dim) return 0;
   int N[3] = {P.nx, P.ny, P.nz};
   long long nseg = (N[dir] + SEG_CELLS - 1) / SEG_CELLS;
   long long other = (long long)P.nx * P.ny * P.nz / N[dir];
-  return (int)(nseg * other);
+  if (groups && dir >= 1) return nseg * (other / P.nx) * ((P.nx + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK);
+  return nseg * other;
 }
 
 void* buf(dspw_handle* h, int which) {
@@ -365,7 +369,8 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
     a.viscous = 0;
     // NS problems never update in a sweep; mixed batches are not formed with NS
     if (h->has_ns) a.viscous = 1;
-    int grid = (nt + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+    // one block per 8 warp tasks, or per column group (specialised y / z sweeps)
+    int grid = (h->spec && dir >= 1) ? nt : (nt + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
     CK(Launch<T>::sweep(dir, a, grid, h->stream, h->spec));
     prof_mark(h, dir == 0 ? "sweep_x" : (dir == 1 ? "sweep_y" : "sweep_z"));
   }
@@ -493,7 +498,7 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
   for (int dir = 0; dir < 3; dir++) {
     h->task_start[dir].push_back(0);
     for (int p = 0; p < nprob; p++) {
-      long long nt = (long long)h->task_start[dir].back() + tasks_for(h->hprob[p], dir);
+      long long nt = (long long)h->task_start[dir].back() + tasks_for(h->hprob[p], dir, h->spec != 0);
       if (nt > (1LL << 30)) { delete h; return DSPW_ERR_ARG; }
       h->task_start[dir].push_back((int)nt);
     }

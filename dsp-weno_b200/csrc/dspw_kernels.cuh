@@ -279,6 +279,24 @@ DSPW_HD void decode_task(const ProbDev& P, int lt, int& i0, int& j0, int& k0, in
   ncell = min(SEG_CELLS, N - c0);
 }
 
+// (column group, segment) of a local group task of the specialised y / z
+// sweeps: groups of 8 adjacent x columns (the last of a row may be partial,
+// ncols < 8), then segments, then the remaining direction.
+template <int DIR>
+DSPW_HD void decode_group(const ProbDev& P, int lg, int& i0, int& j0, int& k0, int& c0, int& ncell, int& ncols) {
+  const int N = dir_len<DIR>(P);
+  const int nseg = (N + SEG_CELLS - 1) / SEG_CELLS;
+  const int ngx = (P.nx + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+  const int ig = lg % ngx;
+  lg /= ngx;
+  const int seg = lg % nseg, o = lg / nseg;
+  i0 = ig * WARPS_PER_BLOCK;
+  ncols = min(WARPS_PER_BLOCK, P.nx - i0);
+  if (DIR == 1) { k0 = o; j0 = 0; } else { j0 = o; k0 = 0; }
+  c0 = seg * SEG_CELLS;
+  ncell = min(SEG_CELLS, N - c0);
+}
+
 template <int DIR>
 DSPW_HD long long cell_index(const ProbDev& P, int i0, int j0, int k0, int c) {
   if (DIR == 0) return P.off + ((long long)k0 * P.ny + j0) * P.nx + c;
@@ -482,10 +500,11 @@ __device__ inline void net_frag_stage(const NetParams& P, int lane, NetScratch<T
 }
 
 // The four layers of one 16-row tile as one PTX block: A fragments loaded from
-// the staged inputs (rows r and r + 8, columns kq and kq + 1), bias-initialised
-// FP32 accumulators, m16n8k8 BF16 MMA, ReLU and BF16 repacking of the C
-// fragment as the next layer's A fragment, and the logits stored back to
-// shared memory.
+// the staged inputs (rows r and r + 8, columns kq and kq + 1) and rounded to
+// BF16, m16n8k8 BF16 MMA with the layer's FP32 biases as the C operand, ReLU
+// fused into the BF16 repacking of the result as the next layer's A fragment
+// (cvt.rn.relu: max(x, 0) then round), and the logits stored back to shared
+// memory.
 __device__ inline void mlp_tile_bf16(const NetFrag& nf, unsigned in_lo, unsigned in_hi, unsigned out_lo,
                                      unsigned out_hi) {
   asm volatile(
@@ -496,48 +515,20 @@ __device__ inline void mlp_tile_bf16(const NetFrag& nf, unsigned in_lo, unsigned
       "ld.shared.v2.f32 {%%x2, %%x3}, [%1];\n\t"
       "cvt.rn.bf16x2.f32 %%a0, %%x1, %%x0;\n\t"
       "cvt.rn.bf16x2.f32 %%a1, %%x3, %%x2;\n\t"
-      "mov.f32 %%c0, %8;\n\t"
-      "mov.f32 %%c1, %9;\n\t"
-      "mov.f32 %%c2, %8;\n\t"
-      "mov.f32 %%c3, %9;\n\t"
       "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%%c0,%%c1,%%c2,%%c3}, {%%a0,%%a1}, {%4}, "
-      "{%%c0,%%c1,%%c2,%%c3};\n\t"
-      "max.f32 %%c0, %%c0, 0f00000000;\n\t"
-      "max.f32 %%c1, %%c1, 0f00000000;\n\t"
-      "max.f32 %%c2, %%c2, 0f00000000;\n\t"
-      "max.f32 %%c3, %%c3, 0f00000000;\n\t"
-      "cvt.rn.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
-      "cvt.rn.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
-      "mov.f32 %%c0, %10;\n\t"
-      "mov.f32 %%c1, %11;\n\t"
-      "mov.f32 %%c2, %10;\n\t"
-      "mov.f32 %%c3, %11;\n\t"
+      "{%8,%9,%8,%9};\n\t"
+      "cvt.rn.relu.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
+      "cvt.rn.relu.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
       "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%%c0,%%c1,%%c2,%%c3}, {%%a0,%%a1}, {%5}, "
-      "{%%c0,%%c1,%%c2,%%c3};\n\t"
-      "max.f32 %%c0, %%c0, 0f00000000;\n\t"
-      "max.f32 %%c1, %%c1, 0f00000000;\n\t"
-      "max.f32 %%c2, %%c2, 0f00000000;\n\t"
-      "max.f32 %%c3, %%c3, 0f00000000;\n\t"
-      "cvt.rn.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
-      "cvt.rn.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
-      "mov.f32 %%c0, %12;\n\t"
-      "mov.f32 %%c1, %13;\n\t"
-      "mov.f32 %%c2, %12;\n\t"
-      "mov.f32 %%c3, %13;\n\t"
+      "{%10,%11,%10,%11};\n\t"
+      "cvt.rn.relu.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
+      "cvt.rn.relu.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
       "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%%c0,%%c1,%%c2,%%c3}, {%%a0,%%a1}, {%6}, "
-      "{%%c0,%%c1,%%c2,%%c3};\n\t"
-      "max.f32 %%c0, %%c0, 0f00000000;\n\t"
-      "max.f32 %%c1, %%c1, 0f00000000;\n\t"
-      "max.f32 %%c2, %%c2, 0f00000000;\n\t"
-      "max.f32 %%c3, %%c3, 0f00000000;\n\t"
-      "cvt.rn.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
-      "cvt.rn.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
-      "mov.f32 %%c0, %14;\n\t"
-      "mov.f32 %%c1, %15;\n\t"
-      "mov.f32 %%c2, %14;\n\t"
-      "mov.f32 %%c3, %15;\n\t"
+      "{%12,%13,%12,%13};\n\t"
+      "cvt.rn.relu.bf16x2.f32 %%a0, %%c1, %%c0;\n\t"
+      "cvt.rn.relu.bf16x2.f32 %%a1, %%c3, %%c2;\n\t"
       "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%%c0,%%c1,%%c2,%%c3}, {%%a0,%%a1}, {%7}, "
-      "{%%c0,%%c1,%%c2,%%c3};\n\t"
+      "{%14,%15,%14,%15};\n\t"
       "st.shared.v2.f32 [%2], {%%c0, %%c1};\n\t"
       "st.shared.v2.f32 [%3], {%%c2, %%c3};\n\t"
       "}\n"
@@ -774,6 +765,35 @@ __device__ inline void euler_stage_cells(const SweepArgs<T>& A, const ProbDev& P
   __syncwarp();
 }
 
+// SSPRK stage update of one Euler cell from its residual R, U^(k) (u) and U^n
+// (un): U = b U + (a U^n + R (-factor b)) (enflo/src/fv.cc:1163-1175), stored to
+// Uout, with the CFL speed / entropy / health epilogue on the stage that yields
+// U^(n+1).
+template <typename T>
+__device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
+                                         const T R[5], T u[5], const T un[5], double& smax, double& ent,
+                                         unsigned& bad_fin, unsigned& bad_pos) {
+  const T a = T(A.a_rk), b = T(A.b_rk);
+  const T c2 = T(-S.factor * A.b_rk);
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    u[v] *= b;
+    u[v] += un[v] * a + R[v] * c2;
+  }
+  store_cons<T>(A.Uout, A.ctot, cell, P.nv, u);
+  if (A.final_stage) {
+    T p[5];
+    cons_to_prim<T>(u, T(P.gamma), p);
+    double sp = wave_speed<T>(P, p);
+    if (sp > smax) smax = sp;
+    double rho = p[0], pr = p[4];
+    if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
+    if (!isfinite(rho) || !isfinite(pr) || !isfinite((double)u[1]) || !isfinite((double)u[4])) bad_fin++;
+    double s = ::log(pr) - P.gamma * ::log(rho);
+    ent += -rho * s / (P.gamma - 1.0);
+  }
+}
+
 // final combination for one cell: residual (reference order
 // ((R_prev - F_left) + F_right)) then either store R or apply the SSPRK stage
 // update U = b U + (a U^n + R (-factor b)) (enflo/src/fv.cc:1163-1175), with
@@ -818,24 +838,8 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
   }
   load_cons<T>(A.Uin, A.ctot, cell, P.nv, P.dim, u);
   load_cons<T>(A.Un, A.ctot, cell, P.nv, P.dim, un);
-#pragma unroll
-  for (int v = 0; v < 5; v++) {
-    u[v] *= b;
-    u[v] += un[v] * a + R[v] * c2;
-  }
-  store_cons<T>(A.Uout, A.ctot, cell, P.nv, u);
-  if (A.final_stage) {
-    T p[5];
-    cons_to_prim<T>(u, T(P.gamma), p);
-    double sp = wave_speed<T>(P, p);
-    if (sp > smax) smax = sp;
-    double rho = p[0], pr = p[4];
-    if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
-    if (!isfinite(rho) || !isfinite(pr) || !isfinite((double)u[1]) || !isfinite((double)u[4])) bad_fin++;
-    double s = ::log(pr) - P.gamma * ::log(rho);
-    ent += -rho * s / (P.gamma - 1.0);
-  }
-  (void)nv_eff;
+  update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
+  (void)a; (void)c2; (void)nv_eff;
 }
 
 template <typename T>
@@ -966,29 +970,128 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
 // the faces are evaluated per warp exactly as in euler_task.
 constexpr int COOP_COLS = WARPS_PER_BLOCK;
 
+// Block-wide tiles of the cooperative sweep, behind the per-warp scratch in
+// dynamic shared memory: the staged conserved rows of the 8 columns (ghost rows
+// resolved), and the residual and U^n of the segment's cells for the epilogue.
+// Planes are the stored components 0 .. nv-1.
+template <typename T>
+struct CoopTiles {
+  T U[5][SEG_LOAD][COOP_COLS];
+  T R[5][SEG_CELLS][COOP_COLS];
+  T Un[5][SEG_CELLS][COOP_COLS];
+};
+static_assert(sizeof(WarpSmem<double>) % 16 == 0, "WarpSmem<double> alignment");
+
+// 16-byte global -> shared copy that completes asynchronously (L2 only)
+__device__ inline void cp_async16(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ inline void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// u[5] of one tile entry (plane layout of load_cons)
+template <typename T>
+__device__ inline void tile_cons(const T (*U)[SEG_LOAD][COOP_COLS], int nv, int q, int col, T u[5]) {
+  u[0] = U[0][q][col];
+  u[1] = U[1][q][col];
+  if (nv == 5) { u[2] = U[2][q][col]; u[3] = U[3][q][col]; u[4] = U[4][q][col]; }
+  else if (nv == 4) { u[2] = U[2][q][col]; u[3] = T(0); u[4] = U[3][q][col]; }
+  else { u[2] = T(0); u[3] = T(0); u[4] = U[2][q][col]; }
+}
+template <typename T>
+__device__ inline void tile_cons(const T (*U)[SEG_CELLS][COOP_COLS], int nv, int q, int col, T u[5]) {
+  u[0] = U[0][q][col];
+  u[1] = U[1][q][col];
+  if (nv == 5) { u[2] = U[2][q][col]; u[3] = U[3][q][col]; u[4] = U[4][q][col]; }
+  else if (nv == 4) { u[2] = U[2][q][col]; u[3] = T(0); u[4] = U[3][q][col]; }
+  else { u[2] = T(0); u[3] = T(0); u[4] = U[2][q][col]; }
+}
+
+// Block-cooperative variant for the y and z sweeps: the 8 warps of the block
+// hold 8 adjacent x-columns of the same line segment.  The block first issues
+// asynchronous row copies (8 adjacent x per row and plane) of the staged cells
+// and, as a second group, of the residual and U^n of its cells; it converts the
+// staged rows once the first group has landed, evaluates the faces per warp as
+// in euler_task while the second group is in flight, and runs the cell
+// epilogue from shared memory.  When the rows are not 16-byte aligned in
+// global memory (nx, the problem offset or the plane stride not a multiple of
+// 16 bytes) the same tiles are filled by plain loads.
 template <typename T, int DIR, int DIM, typename Sp>
 __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbState& S,
-                                 WarpSmem<T>* sm0, int lt0) {
+                                 WarpSmem<T>* sm0, int lt0, bool group) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int i0, j0, k0, c0, ncell;
-  decode_task<DIR>(P, lt0, i0, j0, k0, c0, ncell);   // i0 of column 0 (a multiple of 8)
+  int i0, j0, k0, c0, ncell, ncols = COOP_COLS;
+  // i0 of column 0 (a multiple of 8); group tasks may end in a partial group
+  if (group) decode_group<DIR>(P, lt0, i0, j0, k0, c0, ncell, ncols);
+  else decode_task<DIR>(P, lt0, i0, j0, k0, c0, ncell);
   const int N = dir_len<DIR>(P);
   const T G = T(P.gamma);
   const int col = tid % COOP_COLS;
-  // staging: rows q = tid / 8 and q + 32 of column col
-  for (int q = tid / COOP_COLS; q < ncell + 4; q += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
-    int c = c0 - 2 + q;
-    int side = c < 0 ? 0 : 1;
-    int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
+  const int nv = P.nv;
+  CoopTiles<T>& tl = *reinterpret_cast<CoopTiles<T>*>(sm0 + WARPS_PER_BLOCK);
+  const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
+  constexpr int VEC = 16 / (int)sizeof(T);           // elements per 16-byte copy
+  constexpr int CH = COOP_COLS / VEC;                 // copies per row and plane
+  const bool aligned = ncols == COOP_COLS && (A.ctot % VEC) == 0 && (P.off % VEC) == 0 && (P.nx % VEC) == 0;
+  // group 1: staged rows q = 0 .. ncell+3 (cells c0-2 .. c0+ncell+1)
+  const int nrow = ncell + 4;
+  if (aligned) {
+    for (int idx = tid; idx < nv * nrow * CH; idx += WARPS_PER_BLOCK * 32) {
+      const int comp = idx / (nrow * CH), rem = idx - comp * nrow * CH, q = rem / CH, ch = rem - q * CH;
+      const int c = c0 - 2 + q;
+      const int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + (c < 0 ? 0 : 1)];
+      if (kind == DSPW_BC_DIRICHLET) continue;
+      int flip;
+      const int src = ghost_source(c, N, kind, flip);
+      cp_async16(&tl.U[comp][q][ch * VEC], A.Uin + comp * A.ctot + cell_index<DIR>(P, i0 + ch * VEC, j0, k0, src));
+    }
+    cp_async_commit();
+    // group 2: residual (the previous sweep's) and U^n of the cells
+    for (int idx = tid; idx < nv * ncell * CH; idx += WARPS_PER_BLOCK * 32) {
+      const int comp = idx / (ncell * CH), rem = idx - comp * ncell * CH, q = rem / CH, ch = rem - q * CH;
+      const long long off = comp * A.ctot + cell_index<DIR>(P, i0 + ch * VEC, j0, k0, c0 + q);
+      cp_async16(&tl.R[comp][q][ch * VEC], A.R + off);
+      if (final_sweep) cp_async16(&tl.Un[comp][q][ch * VEC], A.Un + off);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+  } else {
+    for (int idx = tid; idx < nv * nrow * COOP_COLS; idx += WARPS_PER_BLOCK * 32) {
+      const int comp = idx / (nrow * COOP_COLS), rem = idx - comp * nrow * COOP_COLS, q = rem / COOP_COLS,
+                cc = rem - q * COOP_COLS;
+      const int c = c0 - 2 + q;
+      const int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + (c < 0 ? 0 : 1)];
+      if (kind == DSPW_BC_DIRICHLET || cc >= ncols) continue;
+      int flip;
+      const int src = ghost_source(c, N, kind, flip);
+      tl.U[comp][q][cc] = A.Uin[comp * A.ctot + cell_index<DIR>(P, i0 + cc, j0, k0, src)];
+    }
+    for (int idx = tid; idx < nv * ncell * COOP_COLS; idx += WARPS_PER_BLOCK * 32) {
+      const int comp = idx / (ncell * COOP_COLS), rem = idx - comp * ncell * COOP_COLS, q = rem / COOP_COLS,
+                cc = rem - q * COOP_COLS;
+      if (cc >= ncols) continue;
+      const long long off = comp * A.ctot + cell_index<DIR>(P, i0 + cc, j0, k0, c0 + q);
+      tl.R[comp][q][cc] = A.R[off];
+      if (final_sweep) tl.Un[comp][q][cc] = A.Un[off];
+    }
+  }
+  __syncthreads();
+  // conversion of the staged rows: row q = tid / 8 (+ 32) of column col
+  for (int q = tid / COOP_COLS; q < nrow && col < ncols; q += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
+    const int c = c0 - 2 + q;
+    const int side = c < 0 ? 0 : 1;
+    const int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
     T p[5];
     if (kind == DSPW_BC_DIRICHLET) {
 #pragma unroll
       for (int v = 0; v < 5; v++) p[v] = T(P.bc_state[2 * DIR + side][v]);
     } else {
       int flip;
-      int src = ghost_source(c, N, kind, flip);
+      ghost_source(c, N, kind, flip);
       T u[5];
-      load_cons<T>(A.Uin, A.ctot, cell_index<DIR>(P, i0 + col, j0, k0, src), P.nv, P.dim, u);
+      tile_cons<T>(tl.U, nv, q, col, u);
       cons_to_prim<T>(u, G, p);
       if (flip) p[1 + DIR] = -p[1 + DIR];
     }
@@ -1002,18 +1105,27 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   int viol = 0;
   unsigned long long signv = 0;
   unsigned checked = 0;
-  euler_faces<T, DIR, DIM, Sp>(A, P, sm0 + warp, lane, ncell, viol, signv, checked, (unsigned)(lt0 + warp));
+  if (warp < ncols)   // warp-uniform: the network inside needs every lane of the warp
+    euler_faces<T, DIR, DIM, Sp>(A, P, sm0 + warp, lane, ncell, viol, signv, checked, (unsigned)(lt0 + warp));
+  if (aligned) cp_async_wait<0>();
   __syncthreads();
-  const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
   double smax = 0.0, ent = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
-  for (int row = tid / COOP_COLS; row < ncell; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
+  for (int row = tid / COOP_COLS; row < ncell && col < ncols; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
     WarpSmem<T>* sc = sm0 + col;
-    T Fl[5], Fr[5];
+    T R[5], r0[5];
+    tile_cons<T>(tl.R, nv, row, col, r0);
 #pragma unroll
-    for (int v = 0; v < 5; v++) { Fl[v] = sc->F[v][row]; Fr[v] = sc->F[v][row + 1]; }
-    long long cell = cell_index<DIR>(P, i0 + col, j0, k0, c0 + row);
-    finish_cell<T>(A, P, S, cell, false, final_sweep, Fl, Fr, P.nv, smax, ent, bad_fin, bad_pos);
+    for (int v = 0; v < 5; v++) R[v] = (r0[v] - sc->F[v][row]) + sc->F[v][row + 1];
+    const long long cell = cell_index<DIR>(P, i0 + col, j0, k0, c0 + row);
+    if (!final_sweep) {
+      store_cons<T>(A.R, A.ctot, cell, nv, R);
+    } else {
+      T u[5], un[5];
+      tile_cons<T>(tl.U, nv, row + 2, col, u);
+      tile_cons<T>(tl.Un, nv, row, col, un);
+      update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
+    }
   }
   if (!final_sweep) { smax = 0.0; ent = 0.0; }
   SweepArgs<T> A2 = A;
@@ -1107,49 +1219,60 @@ k_sweep(SweepArgs<T> A) {
   WarpSmem<T>* sm = sm0 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (!Sp::fixed || Sp::rec == 2) net_frag_stage<T>(*A.net, lane, sm->ns);
-  const int stride = gridDim.x * WARPS_PER_BLOCK;
-  for (int base = blockIdx.x * WARPS_PER_BLOCK; base < A.ntask; base += stride) {
-    if (DIR >= 1 && base + WARPS_PER_BLOCK <= A.ntask) {
-      // block-uniform test: 8 tasks of one Euler problem on 8 adjacent columns
-      const int p = find_problem(A.task_start, A.nprob, base);
-      const int lt0 = base - __ldg(A.task_start + p);
+  if constexpr (Sp::fixed && DIR >= 1) {
+    // specialised y / z sweeps: every task is one block-cooperative column group
+    for (int g = blockIdx.x; g < A.ntask; g += gridDim.x) {
+      const int p = find_problem(A.task_start, A.nprob, g);
       const ProbDev& P = A.prob[p];
-      if ((Sp::fixed || !P.is_scalar) && base + WARPS_PER_BLOCK <= __ldg(A.task_start + p + 1) &&
-          (lt0 % P.nx) % COOP_COLS == 0 && (lt0 % P.nx) + COOP_COLS <= P.nx) {
-        ProbState& S = A.st[p];
-        if (!A.residual_only && !*((volatile int*)&S.active)) continue;
-        if constexpr (Sp::fixed) {
-          euler_coop_block<T, DIR, Sp::dim, Sp>(A, P, S, sm0, lt0);
-        } else if (DIR == 1) {
-          if (P.dim == 2) euler_coop_block<T, DIR, 2, Sp>(A, P, S, sm0, lt0);
-          else euler_coop_block<T, DIR, 3, Sp>(A, P, S, sm0, lt0);
-        } else {
-          euler_coop_block<T, DIR, 3, Sp>(A, P, S, sm0, lt0);
-        }
-        continue;
-      }
+      ProbState& S = A.st[p];
+      if (!A.residual_only && !*((volatile int*)&S.active)) continue;
+      euler_coop_block<T, DIR, Sp::dim, Sp>(A, P, S, sm0, g - __ldg(A.task_start + p), true);
     }
-    const int task = base + (threadIdx.x >> 5);
-    if (task >= A.ntask) continue;
-    const int p = find_problem(A.task_start, A.nprob, task);
-    const ProbDev& P = A.prob[p];
-    ProbState& S = A.st[p];
-    if (!A.residual_only && !*((volatile int*)&S.active)) continue;
-    const int lt = task - __ldg(A.task_start + p);
-    if constexpr (Sp::fixed) {
-      euler_task<T, DIR, Sp::dim, Sp>(A, P, S, sm, lane, lt);
-    } else if (P.is_scalar) {
-      scalar_task<T, DIR>(A, P, S, sm, lane, lt);
-    } else {
-      if (DIR == 0) {
-        if (P.dim == 1) euler_task<T, DIR, 1, Sp>(A, P, S, sm, lane, lt);
-        else if (P.dim == 2) euler_task<T, DIR, 2, Sp>(A, P, S, sm, lane, lt);
-        else euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
-      } else if (DIR == 1) {
-        if (P.dim == 2) euler_task<T, DIR, 2, Sp>(A, P, S, sm, lane, lt);
-        else euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
+  } else {
+    const int stride = gridDim.x * WARPS_PER_BLOCK;
+    for (int base = blockIdx.x * WARPS_PER_BLOCK; base < A.ntask; base += stride) {
+      if (DIR >= 1 && base + WARPS_PER_BLOCK <= A.ntask) {
+        // block-uniform test: 8 tasks of one Euler problem on 8 adjacent columns
+        const int p = find_problem(A.task_start, A.nprob, base);
+        const int lt0 = base - __ldg(A.task_start + p);
+        const ProbDev& P = A.prob[p];
+        if ((Sp::fixed || !P.is_scalar) && base + WARPS_PER_BLOCK <= __ldg(A.task_start + p + 1) &&
+            (lt0 % P.nx) % COOP_COLS == 0 && (lt0 % P.nx) + COOP_COLS <= P.nx) {
+          ProbState& S = A.st[p];
+          if (!A.residual_only && !*((volatile int*)&S.active)) continue;
+          if constexpr (Sp::fixed) {
+            euler_coop_block<T, DIR, Sp::dim, Sp>(A, P, S, sm0, lt0, false);
+          } else if (DIR == 1) {
+            if (P.dim == 2) euler_coop_block<T, DIR, 2, Sp>(A, P, S, sm0, lt0, false);
+            else euler_coop_block<T, DIR, 3, Sp>(A, P, S, sm0, lt0, false);
+          } else {
+            euler_coop_block<T, DIR, 3, Sp>(A, P, S, sm0, lt0, false);
+          }
+          continue;
+        }
+      }
+      const int task = base + (threadIdx.x >> 5);
+      if (task >= A.ntask) continue;
+      const int p = find_problem(A.task_start, A.nprob, task);
+      const ProbDev& P = A.prob[p];
+      ProbState& S = A.st[p];
+      if (!A.residual_only && !*((volatile int*)&S.active)) continue;
+      const int lt = task - __ldg(A.task_start + p);
+      if constexpr (Sp::fixed) {
+        euler_task<T, DIR, Sp::dim, Sp>(A, P, S, sm, lane, lt);
+      } else if (P.is_scalar) {
+        scalar_task<T, DIR>(A, P, S, sm, lane, lt);
       } else {
-        euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
+        if (DIR == 0) {
+          if (P.dim == 1) euler_task<T, DIR, 1, Sp>(A, P, S, sm, lane, lt);
+          else if (P.dim == 2) euler_task<T, DIR, 2, Sp>(A, P, S, sm, lane, lt);
+          else euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
+        } else if (DIR == 1) {
+          if (P.dim == 2) euler_task<T, DIR, 2, Sp>(A, P, S, sm, lane, lt);
+          else euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
+        } else {
+          euler_task<T, DIR, 3, Sp>(A, P, S, sm, lane, lt);
+        }
       }
     }
   }

@@ -148,17 +148,34 @@ DSPW_HD void nn_features(T u0, T u1, T u2, T u3, T feat[5], T vx[5], T vy[5]) {
   T mx = T(1.0);
   mx = m::max(mx, m::abs(u0)); mx = m::max(mx, m::abs(u1));
   mx = m::max(mx, m::abs(u2)); mx = m::max(mx, m::abs(u3));
-  T c0 = m::div(u0, mx), c1 = m::div(u1, mx), c2 = m::div(u2, mx), c3 = m::div(u3, mx);
-  T tm = m::div(c3 - c2, c2 - c1);
-  T tp = m::div(c1 - c0, c2 - c1);
+  T c0, c1, c2, c3, tm, tp;
+  if constexpr (sizeof(T) == 4) {
+    // FP32 form: one reciprocal per divisor, shared by its quotients
+    const T rm = m::div(T(1), mx);
+    c0 = u0 * rm; c1 = u1 * rm; c2 = u2 * rm; c3 = u3 * rm;
+    const T r21 = m::div(T(1), c2 - c1);
+    tm = (c3 - c2) * r21;
+    tp = (c1 - c0) * r21;
+  } else {
+    c0 = m::div(u0, mx); c1 = m::div(u1, mx); c2 = m::div(u2, mx); c3 = m::div(u3, mx);
+    tm = m::div(c3 - c2, c2 - c1);
+    tp = m::div(c1 - c0, c2 - c1);
+  }
   T d1 = m::abs(c1 - c0), d2 = m::abs(c2 - c1), d3 = m::abs(c3 - c2);
   T md = m::max(m::max(d1, d2), d3);
   feat[0] = m::tanh(tm); feat[1] = m::tanh(tp);
   feat[2] = d1; feat[3] = d2; feat[4] = d3;
 
   const T thr = T(1e-8);
-  T psi_p = m::div(T(1) - tm, T(1) - tp);
-  T psi_m = m::div(T(1), psi_p);
+  T psi_p, psi_m;
+  if constexpr (sizeof(T) == 4) {
+    const T a = T(1) - tm, b = T(1) - tp;
+    psi_p = a * m::div(T(1), b);
+    psi_m = b * m::div(T(1), a);
+  } else {
+    psi_p = m::div(T(1) - tm, T(1) - tp);
+    psi_m = m::div(T(1), psi_p);
+  }
   T g1 = m::min(md, T(1.0 / 8.0));
   T g2 = -m::min(md, T(3.0 / 8.0));
   T x1 = T(1.0 / 8.0) * (T(1) + psi_p) - g1 * psi_p;
@@ -220,11 +237,20 @@ DSPW_HD void nn_finish(const T lg[5], const T vx[5], const T vy[5], T u0, T u1, 
   T sum = T(0);
 #pragma unroll
   for (int i = 0; i < 5; i++) { s[i] = m::exp(lg[i] - mxv); sum += s[i]; }
-#pragma unroll
-  for (int i = 0; i < 5; i++) s[i] = m::div(s[i], sum);
   T C1 = T(0.0), C2 = T(0.0);
+  if constexpr (sizeof(T) == 4) {
+    // FP32 form: normalise the two weighted sums instead of the five weights
 #pragma unroll
-  for (int i = 0; i < 5; i++) { C1 += s[i] * vx[i]; C2 += s[i] * vy[i]; }
+    for (int i = 0; i < 5; i++) { C1 += s[i] * vx[i]; C2 += s[i] * vy[i]; }
+    const T rs = m::div(T(1), sum);
+    C1 *= rs;
+    C2 *= rs;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 5; i++) s[i] = m::div(s[i], sum);
+#pragma unroll
+    for (int i = 0; i < 5; i++) { C1 += s[i] * vx[i]; C2 += s[i] * vy[i]; }
+  }
   T w1 = T(1.0 / 4.0) - T(2) * C1;
   T tw0 = T(1.0 / 4.0) - T(2) * C2;
   T wt0 = T(1.0) - w1, wt3 = T(1.0) - tw0;
