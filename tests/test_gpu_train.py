@@ -138,3 +138,42 @@ def test_collect_train_and_gain():
     assert np.isfinite(l1_trained) and l1_trained < 2 * l1_untrained
     print(f"train loss {losses[0]:.3e} -> {losses[-1]:.3e}")
     print(f"gain: held-out loss {l_before:.3e} -> {l_after:.3e}; config-1 L1 {l1_untrained:.3e} -> {l1_trained:.3e}")
+
+
+def test_retrain_on_two_million_pairs():
+    """The retraining set of the north-star size: 2 M (stencil, SP-WENO target)
+    pairs collected on the GPU from plain SP-WENO runs of the scalar, 1-D and
+    2-D problems, trained with FP32 master weights, BF16 compute, Adam and
+    batch 8192.  Epoch time is reported; the loss must fall."""
+    import time
+    from dspw import workloads as W
+
+    W0, b0 = xavier_network(6008)
+    tr = Trainer((W0, b0), batch=8192, bf16=True, collect_stride=1)
+    total = 0
+    nx = 4000
+    x = -np.pi + (np.arange(nx) + 0.5) * 2 * np.pi / nx
+    s = Solver(make_desc(model="linadv", flux="lin_tecno4", recon="sp_weno", nx=nx, x=(-np.pi, np.pi), cfl=0.5,
+                         final_time=0.5))
+    s.upload_prim((np.sin(x) ** 4).reshape(1, 1, 1, nx))
+    total += tr.collect(s, 100_000)
+    d, p, _ = W.shu_osher(25600, "fp64", "sp_weno", None)
+    s = Solver(d)
+    s.upload_prim(p[0])
+    for _ in range(4):
+        s.step(200)
+        total += tr.collect(s, 100_000)
+    d, p, _ = W.kh(512, "fp64", "sp_weno", None)
+    s = Solver(d)
+    s.upload_prim(p[0])
+    s.step(100)
+    total += tr.collect(s, 2_000_000 - total)
+    assert total >= 1_900_000, total
+    losses, times = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        losses.append(tr.epoch())
+        times.append(time.perf_counter() - t0)
+    assert losses[-1] < losses[0], losses
+    print(f"2M-pair retraining: {total} pairs, epoch {min(times) * 1e3:.1f} ms "
+          f"({total / min(times) / 1e6:.1f} M samples/s), loss {losses[0]:.3e} -> {losses[-1]:.3e}")
