@@ -150,15 +150,20 @@ class ClockSampler:
 
 def algorithmic_bytes(name, stage, probs, w):
     """Minimum HBM bytes of one launch of kernel ``name`` in SSPRK3 stage
-    ``stage`` over problems ``probs`` = [(cells, nv, dim, ns)], nv the stored
-    components, w the word size.  Euler / scalar: the x sweep reads U^k and
+    ``stage`` over problems ``probs`` = [(cells, nv, dim, ns, kernel class)], nv
+    the stored components, w the word size.  A sweep launch of a mixed batch is
+    named ``sweep_<d>.c<class>`` and covers the problems of that class only.  Euler / scalar: the x sweep reads U^k and
     writes R, middle sweeps read U^k and R and write R, the last sweep reads U^k,
     R (absent in 1-D) and, in stages 2-3, U^n and writes U^(k+1).  Navier-Stokes:
     entropy variables read U and write V; node fluxes read V and write 3 nv per
     node; the sweeps only accumulate R; the viscous update reads the node fluxes,
     R, U^k (and U^n) and writes U^(k+1)."""
+    base, _, cls = name.partition(".c")
+    name = base
     tot = 0
-    for cells, nv, dim, ns in probs:
+    for cells, nv, dim, ns, kcls in probs:
+        if cls and int(cls) != kcls:
+            continue
         upd = 4 if stage > 0 else 3
         b = 0
         if ns:
@@ -198,12 +203,22 @@ def build_workload(args, precision, recon, rank, world):
     return d, p, c, sum(cells), "strong"
 
 
+def kernel_class(d, dim):
+    """Sweep kernel class of a problem (the library's spec_of): Euler / NS with a
+    kepes_tecno4 flux run the kernels specialised for their dimension and
+    reconstruction family (10 * dim + 1 SP-WENO, + 2 DSP-WENO), others class 0."""
+    from dspw import FLUX, RECON
+    if d.model in (0, 1) or d.flux not in (FLUX["kepes_tecno4_roe"], FLUX["kepes_tecno4_rusanov"]):
+        return 0
+    return 10 * dim + (2 if d.recon == RECON["sp_weno_dl"] else 1)
+
+
 def prob_info(descs):
     out = []
     for d in descs:
         dim = 1 + (d.ny > 1) + (d.nz > 1)
         nv = 1 if d.model in (0, 1) else dim + 2
-        out.append((d.nx * d.ny * d.nz, nv, dim, d.model == 3))
+        out.append((d.nx * d.ny * d.nz, nv, dim, d.model == 3, kernel_class(d, dim)))
     return out
 
 
@@ -257,10 +272,12 @@ def measure_gpu(args, torch, dist, rank, world):
     prof = s.profile_step()
     w = 4 if args.precision == "fp32_bf16" else 8
     first = "entvars" if any(p[3] for p in probs) else "sweep_x"   # the first launch of a stage
-    stage, rows = -1, []
+    stage, rows, prev = -1, [], None
     for name, kms in prof:
-        if name == first:
+        base = name.partition(".c")[0]
+        if base == first and prev != first:   # one x launch per kernel class
             stage += 1
+        prev = base
         rows.append((name, stage, kms))
     dom = max(rows, key=lambda r: r[2])
     dom_bytes = algorithmic_bytes(dom[0], dom[1], probs, w)

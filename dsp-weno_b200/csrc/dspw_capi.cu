@@ -92,6 +92,18 @@ cudaError_t launch_init_state(const ProbDev* prob, ProbState* st, int p, cudaStr
 
 // ------------------------------------------------------------------ handle --
 
+// Problems of a batch that run the same sweep kernels: one launch per
+// direction and class, over the class's own task prefix sums; pmap maps the
+// class's entries to the batch's problem indices (null when the class is the
+// whole batch in order).
+struct SweepClass {
+  int spec = 0;                        // spec_code of the class's kernels, 0 generic
+  std::vector<int> probs;
+  std::vector<int> task_start[3];
+  int* dtask[3] = {nullptr, nullptr, nullptr};
+  int* dpmap = nullptr;
+};
+
 struct dspw_handle {
   int nprob = 0;
   int precision = 0;
@@ -99,18 +111,16 @@ struct dspw_handle {
   int time_scheme = 1;
   int has_ns = 0;
   int maxdim = 1;
-  int spec = 0;                        // sweep kernel specialisation (spec_code), 0 generic
+  std::vector<SweepClass> classes;
   std::vector<dspw_desc> desc;
   std::vector<ProbDev> hprob;
   std::vector<long long> cell_start;   // nprob + 1
-  std::vector<int> task_start[3];
   long long ctot = 0;
   long long maxcells = 0;
   ProbDev* dprob = nullptr;
   ProbState* dst = nullptr;
   StatusDev* dstatus = nullptr;
   NetParams* dnet = nullptr;
-  int* dtask[3] = {nullptr, nullptr, nullptr};
   long long* dcell_start = nullptr;
   int* dnactive = nullptr;
   void* Un = nullptr;
@@ -292,15 +302,13 @@ NetParams make_net(const dspw_desc& dn) {
   return np;
 }
 
-// A batch of Euler / NS problems of one dimension, all with the 4th-order
-// KEPEC central part plus TeCNO dissipation and one reconstruction family,
-// runs the specialised sweep kernels; any other batch the generic ones.
-int choose_spec(const std::vector<ProbDev>& ps) {
-  const int dim = ps[0].dim;
-  const bool dl = ps[0].spw_corr < 0;
-  for (const ProbDev& P : ps)
-    if (P.is_scalar || P.dim != dim || P.central != 0 || !P.fourth || !P.tecno || (P.spw_corr < 0) != dl) return 0;
-  return spec_code(dim, dl ? 2 : 1);
+// Sweep kernels of one problem: Euler / NS problems with the 4th-order KEPEC
+// central part plus TeCNO dissipation run the kernels specialised for their
+// dimension and reconstruction family; every other problem the generic ones.
+int spec_of(const ProbDev& P, const dspw_desc& d) {
+  if (d.reserved_i[1] == 1) return 0;   // generic kernels requested
+  if (P.is_scalar || P.central != 0 || !P.fourth || !P.tecno) return 0;
+  return spec_code(P.dim, P.spw_corr < 0 ? 2 : 1);
 }
 
 // Tasks of one problem in direction dir: warp tasks (one line segment each),
@@ -362,17 +370,23 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
     prof_mark(h, "visc_nodes");
   }
   for (int dir = 0; dir < h->maxdim; dir++) {
-    int nt = h->task_start[dir][h->nprob];
-    if (nt == 0) continue;
-    a.task_start = h->dtask[dir];
-    a.ntask = nt;
-    a.viscous = 0;
-    // NS problems never update in a sweep; mixed batches are not formed with NS
-    if (h->has_ns) a.viscous = 1;
-    // one block per 8 warp tasks, or per column group (specialised y / z sweeps)
-    int grid = (h->spec && dir >= 1) ? nt : (nt + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
-    CK(Launch<T>::sweep(dir, a, grid, h->stream, h->spec));
-    prof_mark(h, dir == 0 ? "sweep_x" : (dir == 1 ? "sweep_y" : "sweep_z"));
+    for (const SweepClass& c : h->classes) {
+      int nt = c.task_start[dir].back();
+      if (nt == 0) continue;
+      a.task_start = c.dtask[dir];
+      a.pmap = c.dpmap;
+      a.nprob = (int)c.probs.size();
+      a.ntask = nt;
+      a.viscous = 0;
+      // NS problems never update in a sweep; mixed batches are not formed with NS
+      if (h->has_ns) a.viscous = 1;
+      // one block per 8 warp tasks, or per column group (specialised y / z sweeps)
+      int grid = (c.spec && dir >= 1) ? nt : (nt + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+      CK(Launch<T>::sweep(dir, a, grid, h->stream, c.spec));
+      std::string name = dir == 0 ? "sweep_x" : (dir == 1 ? "sweep_y" : "sweep_z");
+      if (h->classes.size() > 1) name += ".c" + std::to_string(c.spec);
+      prof_mark(h, name.c_str());
+    }
   }
   if (h->has_ns) {
     CK(Launch<T>::visc_update(a, h->dcell_start, h->ctot, (const T*)h->node, h->stream));
@@ -494,13 +508,27 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
       if (descs[p].model != DSPW_NS_ES) { delete h; return DSPW_ERR_UNSUPPORTED; }
   }
   h->ctot = off;
-  h->spec = choose_spec(h->hprob);
-  for (int dir = 0; dir < 3; dir++) {
-    h->task_start[dir].push_back(0);
-    for (int p = 0; p < nprob; p++) {
-      long long nt = (long long)h->task_start[dir].back() + tasks_for(h->hprob[p], dir, h->spec != 0);
-      if (nt > (1LL << 30)) { delete h; return DSPW_ERR_ARG; }
-      h->task_start[dir].push_back((int)nt);
+  // classes of problems sharing sweep kernels, in order of first appearance
+  for (int p = 0; p < nprob; p++) {
+    const int sc = spec_of(h->hprob[p], descs[p]);
+    SweepClass* c = nullptr;
+    for (SweepClass& k : h->classes)
+      if (k.spec == sc) c = &k;
+    if (!c) {
+      h->classes.emplace_back();
+      c = &h->classes.back();
+      c->spec = sc;
+    }
+    c->probs.push_back(p);
+  }
+  for (SweepClass& c : h->classes) {
+    for (int dir = 0; dir < 3; dir++) {
+      c.task_start[dir].push_back(0);
+      for (int p : c.probs) {
+        long long nt = (long long)c.task_start[dir].back() + tasks_for(h->hprob[p], dir, c.spec != 0);
+        if (nt > (1LL << 30)) { delete h; return DSPW_ERR_ARG; }
+        c.task_start[dir].push_back((int)nt);
+      }
     }
   }
   // network parameters (shared by the batch; taken from the first DL problem)
@@ -526,7 +554,11 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
     CKC(cudaMalloc(&h->dnet, sizeof(NetParams)));
     CKC(cudaMalloc(&h->dcell_start, sizeof(long long) * (nprob + 1)));
     CKC(cudaMalloc(&h->dnactive, sizeof(int)));
-    for (int dir = 0; dir < 3; dir++) CKC(cudaMalloc(&h->dtask[dir], sizeof(int) * (nprob + 1)));
+    for (SweepClass& c : h->classes) {
+      const size_t n = c.probs.size();
+      for (int dir = 0; dir < 3; dir++) CKC(cudaMalloc(&c.dtask[dir], sizeof(int) * (n + 1)));
+      if (h->classes.size() > 1) CKC(cudaMalloc(&c.dpmap, sizeof(int) * n));
+    }
     CKC(cudaMalloc(&h->Un, state_bytes));
     CKC(cudaMalloc(&h->Ua, state_bytes));
     CKC(cudaMalloc(&h->Ub, state_bytes));
@@ -542,8 +574,12 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
     CKC(cudaMemset(h->dstatus, 0, sizeof(StatusDev)));
     CKC(cudaMemcpy(h->dnet, &np, sizeof(NetParams), cudaMemcpyHostToDevice));
     CKC(cudaMemcpy(h->dcell_start, h->cell_start.data(), sizeof(long long) * (nprob + 1), cudaMemcpyHostToDevice));
-    for (int dir = 0; dir < 3; dir++)
-      CKC(cudaMemcpy(h->dtask[dir], h->task_start[dir].data(), sizeof(int) * (nprob + 1), cudaMemcpyHostToDevice));
+    for (SweepClass& c : h->classes) {
+      const size_t n = c.probs.size();
+      for (int dir = 0; dir < 3; dir++)
+        CKC(cudaMemcpy(c.dtask[dir], c.task_start[dir].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+      if (c.dpmap) CKC(cudaMemcpy(c.dpmap, c.probs.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    }
     CKC(cudaMemset(h->Un, 0, state_bytes));
     CKC(cudaMemset(h->Ua, 0, state_bytes));
     CKC(cudaMemset(h->Ub, 0, state_bytes));
@@ -569,10 +605,15 @@ int dspw_destroy(dspw_handle* h) {
   if (!h) return DSPW_ERR_ARG;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
-  void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive, h->dtask[0], h->dtask[1],
-                  h->dtask[2], h->Un, h->Ua, h->Ub, h->R, h->V, h->node, h->dstage, h->dscratch};
+  void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive,
+                  h->Un, h->Ua, h->Ub, h->R, h->V, h->node, h->dstage, h->dscratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (SweepClass& c : h->classes) {
+    for (int dir = 0; dir < 3; dir++)
+      if (c.dtask[dir]) cudaFree(c.dtask[dir]);
+    if (c.dpmap) cudaFree(c.dpmap);
+  }
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return DSPW_OK;

@@ -95,7 +95,8 @@ template <typename T>
 struct SweepArgs {
   const ProbDev* prob;
   ProbState* st;
-  const int* task_start;   // nprob + 1 prefix of warp tasks in this direction
+  const int* task_start;   // nprob + 1 prefix of tasks in this direction
+  const int* pmap;         // problem index of each entry of task_start (null: identity)
   int nprob, ntask;
   const T* Uin;            // U^(k), stage input
   const T* Un;             // U^n
@@ -1223,8 +1224,9 @@ k_sweep(SweepArgs<T> A) {
     // specialised y / z sweeps: every task is one block-cooperative column group
     for (int g = blockIdx.x; g < A.ntask; g += gridDim.x) {
       const int p = find_problem(A.task_start, A.nprob, g);
-      const ProbDev& P = A.prob[p];
-      ProbState& S = A.st[p];
+      const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+      const ProbDev& P = A.prob[pp];
+      ProbState& S = A.st[pp];
       if (!A.residual_only && !*((volatile int*)&S.active)) continue;
       euler_coop_block<T, DIR, Sp::dim, Sp>(A, P, S, sm0, g - __ldg(A.task_start + p), true);
     }
@@ -1234,11 +1236,12 @@ k_sweep(SweepArgs<T> A) {
       if (DIR >= 1 && base + WARPS_PER_BLOCK <= A.ntask) {
         // block-uniform test: 8 tasks of one Euler problem on 8 adjacent columns
         const int p = find_problem(A.task_start, A.nprob, base);
+        const int pp = A.pmap ? __ldg(A.pmap + p) : p;
         const int lt0 = base - __ldg(A.task_start + p);
-        const ProbDev& P = A.prob[p];
+        const ProbDev& P = A.prob[pp];
         if ((Sp::fixed || !P.is_scalar) && base + WARPS_PER_BLOCK <= __ldg(A.task_start + p + 1) &&
             (lt0 % P.nx) % COOP_COLS == 0 && (lt0 % P.nx) + COOP_COLS <= P.nx) {
-          ProbState& S = A.st[p];
+          ProbState& S = A.st[pp];
           if (!A.residual_only && !*((volatile int*)&S.active)) continue;
           if constexpr (Sp::fixed) {
             euler_coop_block<T, DIR, Sp::dim, Sp>(A, P, S, sm0, lt0, false);
@@ -1254,8 +1257,9 @@ k_sweep(SweepArgs<T> A) {
       const int task = base + (threadIdx.x >> 5);
       if (task >= A.ntask) continue;
       const int p = find_problem(A.task_start, A.nprob, task);
-      const ProbDev& P = A.prob[p];
-      ProbState& S = A.st[p];
+      const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+      const ProbDev& P = A.prob[pp];
+      ProbState& S = A.st[pp];
       if (!A.residual_only && !*((volatile int*)&S.active)) continue;
       const int lt = task - __ldg(A.task_start + p);
       if constexpr (Sp::fixed) {

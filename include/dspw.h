@@ -108,7 +108,9 @@ typedef struct dspw_desc {
   int mu_model;              /* enum dspw_mu */
   int max_iter;
   int t_stamps;              /* output time_stamps; dt is clipped to them like FV::run */
-  int reserved_i[8];
+  int reserved_i[8];          /* [0]: the network carries a training box of its inputs (bounds in
+                                reserved_d[2..4]); [1]: 1 = run this problem on the generic sweep
+                                kernels even when specialised ones exist (validation) */
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double gamma, gas_const, prandtl, mu_ref, T_ref, T_0, omega;
   double lin_vel[3];         /* linadv velocity */

@@ -200,11 +200,12 @@ def test_batch_equals_single():
 @pytest.mark.parametrize("recon", ["sp_wenoc", "sp_weno_dl"])
 @pytest.mark.parametrize("dims", [(40, 1, 1), (24, 40, 1), (16, 12, 10), (12, 12, 10)])
 def test_specialised_kernels_equal_generic(precision, recon, dims):
-    """A kepes_tecno4 problem alone runs the compile-time specialised sweep
-    kernels; batched with a Burgers problem it runs the generic ones.  FP64
-    gives the same bits; FP32 (built with FMA contraction, whose choices may
-    differ between the two instantiations, and with BF16 network layers whose
-    roundings then flip now and then) agrees to rounding."""
+    """A kepes_tecno4 problem runs the compile-time specialised sweep kernels;
+    with descriptor reserved_i[1] = 1 it runs the generic ones (here batched
+    with a Burgers problem, a second kernel class).  FP64 gives the same bits;
+    FP32 (built with FMA contraction, whose choices may differ between the two
+    instantiations, and with BF16 network layers whose roundings then flip now
+    and then) agrees to rounding."""
     nx, ny, nz = dims
     rng = np.random.default_rng(17)
     d = make_desc(model="euler", flux="kepes_tecno4_roe", recon=recon, nx=nx, ny=ny, nz=nz, bc="periodic",
@@ -214,7 +215,10 @@ def test_specialised_kernels_equal_generic(precision, recon, dims):
     a = Solver(d)
     a.upload_prim(st)
     a.step(5)
-    b = Solver([d, dummy])
+    dg = make_desc(model="euler", flux="kepes_tecno4_roe", recon=recon, nx=nx, ny=ny, nz=nz, bc="periodic",
+                   network=net(), precision=precision, ec1_fix=True)
+    dg.reserved_i[1] = 1
+    b = Solver([dg, dummy])
     b.upload_prim(st, 0)
     b.upload_prim(np.sin(np.linspace(0, 6, 33)).reshape(1, 1, 1, 33), 1)
     b.step(5)
