@@ -234,7 +234,10 @@ def measure_gpu(args, torch, dist, rank, world):
         s = Solver(d)
         for p, a in enumerate(pr):
             s.upload_prim(a, p)
+        tuned["ms"] = s.tune(reps=3)   # launch grids picked by timing (dspw_tune), before any timed step
         return s
+
+    tuned = {}
 
     def timed(s, steps, warmup):
         stream = torch.cuda.ExternalStream(s.stream_ptr(), device=dev)
@@ -321,7 +324,8 @@ def measure_gpu(args, torch, dist, rank, world):
         fp64_ms = timed(s64, k64, max(1, args.warmup // 2)) / k64
         del s64
     nbytes = sum(a.nbytes for a in prims)
-    return dict(ms=ms, clk=clk, status=st, prof=rows, dom=dom, dom_bytes=dom_bytes, achieved=achieved,
+    tune_ms = tuned.get("ms")
+    return dict(tune_ms=tune_ms, ms=ms, clk=clk, status=st, prof=rows, dom=dom, dom_bytes=dom_bytes, achieved=achieved,
                 peak=peak, e2e_s=e2e_s, e2e_steps=e2e_steps, ncell=ncell, ncell_all=ncell_all, scaling=scaling,
                 launches=len(prof), fp64_ms=fp64_ms, h2d=nbytes, d2h=nbytes, nprob=len(descs))
 
@@ -460,6 +464,8 @@ def main():
         "e2e": {"value": e2e_v, "unit": "cell-updates/s", "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "api": "dspw_upload_prim + dspw_step(1) + dspw_download_cons"},
         "gpu_launches": r["launches"] * steps,
+        "tuner": {"sweeps_ms_default_grid": r["tune_ms"][0], "sweeps_ms_tuned": r["tune_ms"][1]}
+        if r.get("tune_ms") else None,
         "clocks": r["clk"],
         "kernels_ms_one_step": [[a, b, round(c, 4)] for a, b, c in r["prof"]],
         "health": {"code": r["status"].code, "sign_violations": r["status"].sign_violations,

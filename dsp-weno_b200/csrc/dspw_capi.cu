@@ -102,6 +102,7 @@ struct SweepClass {
   std::vector<int> task_start[3];
   int* dtask[3] = {nullptr, nullptr, nullptr};
   int* dpmap = nullptr;
+  int grid[3] = {0, 0, 0};             // launch grid chosen by dspw_tune (0: one block per block-worth of tasks)
 };
 
 struct dspw_handle {
@@ -331,8 +332,9 @@ void* buf(dspw_handle* h, int which) {
   }
 }
 
+// sweep arguments of stage rk (residual_only: write R in every sweep)
 template <typename T>
-int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
+SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
   SweepArgs<T> a;
   memset(&a, 0, sizeof(a));
   a.prob = h->dprob;
@@ -362,6 +364,31 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
   a.collect_count = h->collect_count;
   a.collect_cap = h->collect_cap;
   a.collect_stride = h->collect_stride ? h->collect_stride : 1;
+  // NS problems never update in a sweep; mixed batches are not formed with NS
+  a.viscous = h->has_ns ? 1 : 0;
+  return a;
+}
+
+// grid of one class's sweep: the tuned one, else one block per 8 warp tasks or
+// per column group (specialised y / z sweeps)
+int default_grid(const SweepClass& c, int dir) {
+  int nt = c.task_start[dir].back();
+  return (c.spec && dir >= 1) ? nt : (nt + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+}
+
+template <typename T>
+cudaError_t launch_class_sweep(dspw_handle* h, SweepArgs<T> a, const SweepClass& c, int dir) {
+  a.task_start = c.dtask[dir];
+  a.pmap = c.dpmap;
+  a.nprob = (int)c.probs.size();
+  a.ntask = c.task_start[dir].back();
+  int grid = c.grid[dir] ? c.grid[dir] : default_grid(c, dir);
+  return Launch<T>::sweep(dir, a, grid, h->stream, c.spec);
+}
+
+template <typename T>
+int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
+  SweepArgs<T> a = stage_args<T>(h, rk, residual_only);
   if (h->has_ns) {
     CK(Launch<T>::entvars(h->dprob, h->nprob, h->dcell_start, h->ctot, a.Uin, h->ctot, (T*)h->V, h->stream));
     prof_mark(h, "entvars");
@@ -371,18 +398,8 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
   }
   for (int dir = 0; dir < h->maxdim; dir++) {
     for (const SweepClass& c : h->classes) {
-      int nt = c.task_start[dir].back();
-      if (nt == 0) continue;
-      a.task_start = c.dtask[dir];
-      a.pmap = c.dpmap;
-      a.nprob = (int)c.probs.size();
-      a.ntask = nt;
-      a.viscous = 0;
-      // NS problems never update in a sweep; mixed batches are not formed with NS
-      if (h->has_ns) a.viscous = 1;
-      // one block per 8 warp tasks, or per column group (specialised y / z sweeps)
-      int grid = (c.spec && dir >= 1) ? nt : (nt + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
-      CK(Launch<T>::sweep(dir, a, grid, h->stream, c.spec));
+      if (c.task_start[dir].back() == 0) continue;
+      CK(launch_class_sweep<T>(h, a, c, dir));
       std::string name = dir == 0 ? "sweep_x" : (dir == 1 ? "sweep_y" : "sweep_z");
       if (h->classes.size() > 1) name += ".c" + std::to_string(c.spec);
       prof_mark(h, name.c_str());
@@ -395,6 +412,65 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
   if (h->nrk == 1 && !residual_only)
     CK(cudaMemcpyAsync(h->Un, h->Ua, h->elem * h->ctot * 5, cudaMemcpyDeviceToDevice, h->stream));
   return DSPW_OK;
+}
+
+// Launch-grid autotuner: for every kernel class and direction, time the sweep
+// (residual evaluation of the current state, which writes only the residual
+// buffer) with its default grid and with persistent grids of 1, 2 and 4 times
+// the resident blocks of the whole GPU, and keep the fastest.
+template <typename T>
+int tune_grids(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
+  int dev = 0, nsm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  StatusDev saved;
+  CK(cudaMemcpy(&saved, h->dstatus, sizeof(saved), cudaMemcpyDeviceToHost));
+  SweepArgs<T> a = stage_args<T>(h, 0, 1);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double tot_before = 0.0, tot_after = 0.0;
+  int ret = DSPW_OK;
+  for (SweepClass& c : h->classes) {
+    for (int dir = 0; dir < h->maxdim; dir++) {
+      if (c.task_start[dir].back() == 0) continue;
+      const int g0 = default_grid(c, dir);
+      const int bpsm = Launch<T>::sweep_blocks_per_sm(dir, c.spec);
+      std::vector<int> cand = {0};
+      for (int k : {1, 2, 4})
+        if (bpsm > 0 && (long long)nsm * bpsm * k < g0) cand.push_back(nsm * bpsm * k);
+      double best = 1e300;
+      int best_grid = 0;
+      for (int g : cand) {
+        c.grid[dir] = g;
+        std::vector<float> t(reps);
+        for (int r = 0; r < reps && ret == DSPW_OK; r++) {
+          if (cudaEventRecord(e0, h->stream) != cudaSuccess ||
+              launch_class_sweep<T>(h, a, c, dir) != cudaSuccess ||
+              cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+              cudaEventElapsedTime(&t[r], e0, e1) != cudaSuccess)
+            ret = DSPW_ERR_CUDA;
+        }
+        if (ret) break;
+        std::sort(t.begin(), t.end());
+        const double med = t[reps / 2];
+        if (g == 0) tot_before += med;
+        if (med < best) { best = med; best_grid = g; }
+      }
+      c.grid[dir] = best_grid;
+      if (ret) break;
+      tot_after += best;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ret) { for (SweepClass& c : h->classes) c.grid[0] = c.grid[1] = c.grid[2] = 0; }
+  // the timing runs counted faces; the status is the solver's, not the tuner's
+  if (cudaMemcpy(h->dstatus, &saved, sizeof(saved), cudaMemcpyHostToDevice) != cudaSuccess) ret = DSPW_ERR_CUDA;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  if (before_ms) *before_ms = tot_before;
+  if (after_ms) *after_ms = tot_after;
+  return ret;
 }
 
 int enqueue_stage_any(dspw_handle* h, int rk, int residual_only) {
@@ -798,6 +874,12 @@ int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, double err
   err[1] = std::sqrt(acc[1] * (P.dx * P.dy * P.dz));
   err[2] = acc[2];
   return DSPW_OK;
+}
+
+int dspw_tune(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
+  if (!h || reps < 1 || reps > 1000) return DSPW_ERR_ARG;
+  return h->precision == DSPW_FP64 ? tune_grids<double>(h, reps, before_ms, after_ms)
+                                   : tune_grids<float>(h, reps, before_ms, after_ms);
 }
 
 int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k, int* nk) {

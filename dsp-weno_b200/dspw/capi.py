@@ -223,6 +223,7 @@ def lib():
         "dspw_reconstruct_batch": (I, [C.POINTER(Desc), dp, LL, dp, dp, C.POINTER(LL)]),
         "dspw_globals_noalloc": (I, [C.POINTER(Desc), P, LL, I, P, P]),
         "dspw_profile_step": (I, [P, dp, C.c_char_p, I, C.POINTER(I)]),
+        "dspw_tune": (I, [P, I, C.POINTER(D), C.POINTER(D)]),
         "dspw_stream": (P, [P]),
         "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),
         "dspw_trainer_create": (I, [C.POINTER(TrainCfg), dp, dp, C.POINTER(P)]),
@@ -408,6 +409,13 @@ class Solver:
         a = np.ascontiguousarray(exact, dtype=np.float64)
         check(lib().dspw_errors(self.h, p, comp, a, e), "dspw_errors")
         return e
+
+    def tune(self, reps=5):
+        """Pick the launch grid of every sweep by timing (dspw_tune); returns
+        the summed sweep times (ms) with the default and the chosen grids."""
+        b, a = C.c_double(), C.c_double()
+        check(lib().dspw_tune(self.h, int(reps), C.byref(b), C.byref(a)), "dspw_tune")
+        return b.value, a.value
 
     def profile_step(self):
         """Durations (ms) of every kernel launch of one un-graphed step."""

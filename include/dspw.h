@@ -194,6 +194,18 @@ DSPW_API int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, d
  * milliseconds (kernel_ms, up to max_k entries, launch order: begin-step,
  * per stage the sweeps x/y/z [and the viscous kernels], end-step) and a short
  * name per launch (names: max_k rows of 16 chars).  For measurement only. */
+/* Launch-grid autotuner (no counterpart in the reference, whose loops are
+   serial): for every kernel class and sweep direction of the handle, times the
+   sweep on the current state (a residual evaluation, which writes only the
+   residual buffer) with its default grid and with persistent grids of 1, 2 and
+   4 times the resident blocks of the GPU, keeps the fastest, and drops the
+   step graph so that the next step is captured with the chosen grids.  The
+   state, the problems' clocks and the status counters are unchanged.  reps:
+   timed launches per candidate (their median is compared, 1..1000).
+   before_ms / after_ms (nullable): summed sweep times with the default and the
+   chosen grids. */
+DSPW_API int dspw_tune(dspw_handle* h, int reps, double* before_ms, double* after_ms);
+
 DSPW_API int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k, int* nk);
 
 /* Reconstruct n independent 4-cell stencils u4[4*i..4*i+3] at their middle

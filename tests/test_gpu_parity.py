@@ -240,3 +240,29 @@ def test_conservation_periodic():
     for v in (0, 1, 2, 4):
         assert abs(g1.conserved[v] - g0.conserved[v]) <= 1e-12 * max(1.0, abs(g0.conserved[v]))
     assert g1.total_entropy <= g0.total_entropy * (1 + 1e-13)
+
+
+def test_tune_keeps_results_and_state():
+    """dspw_tune times launch grids on the current state: afterwards the state,
+    the clock and the status are unchanged, and steps give the same bits as
+    with the default grids (grid-stride loops visit the same tasks)."""
+    rng = np.random.default_rng(8)
+    ds = [make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=96, ny=80, nz=1, bc="periodic"),
+          make_desc(model="burgers", flux="bur_tecno4", recon="sp_weno", nx=300, ny=1, nz=1, x=(-np.pi, np.pi))]
+    states = [random_state(rng, 96, 80, 1), np.sin(np.linspace(-np.pi, np.pi, 300, endpoint=False)).reshape(1, 1, 1, 300)]
+    a, b = Solver(ds), Solver(ds)
+    for p, st in enumerate(states):
+        a.upload_prim(st, p)
+        b.upload_prim(st, p)
+    a.step(2)
+    b.step(2)
+    before = b.cons(0), b.globals(0).time
+    t0, t1 = b.tune(reps=3)
+    assert t0 > 0 and 0 < t1 <= t0 * 1.0001
+    assert np.array_equal(b.cons(0), before[0]) and b.globals(0).time == before[1]
+    a.step(4)
+    b.step(4)
+    for p in range(2):
+        assert np.array_equal(a.cons(p), b.cons(p)), p
+    # the timing runs leave the status counters (read-and-clear) untouched
+    assert a.status().faces_checked == b.status().faces_checked
