@@ -330,16 +330,86 @@ def measure_gpu(args, torch, dist, rank, world):
                 launches=len(prof), fp64_ms=fp64_ms, h2d=nbytes, d2h=nbytes, nprob=len(descs))
 
 
+def matched_error(torch):
+    """Time to a given L1 density error: FP64 plain SP-WENO against FP32 + BF16
+    DSP-WENO, on a shock problem (Shu-Osher, error against a 51200-cell FP64
+    solution averaged to each grid) and a smooth one (isentropic vortex to
+    t = 2, error against the exact advected vortex).  Each form runs a grid
+    sequence to the final time; device time per run is measured with CUDA
+    events around dspw_run.  The FP64 cost of reaching each FP32 error is
+    interpolated in log-log along the FP64 sequence."""
+    from dspw import Solver, load_network_file, workloads as W
+
+    net = load_network_file(NET_FILE)
+
+    def run(descs, prims):
+        s = Solver(descs)
+        for p, a in enumerate(prims):
+            s.upload_prim(a, p)
+        st = torch.cuda.ExternalStream(s.stream_ptr())
+        s.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        steps = s.run(chunk=256)
+        e1.record(st)
+        e1.synchronize()
+        return s, e0.elapsed_time(e1), steps
+
+    def interp_cost(err64, ms64, e):
+        le, lt = np.log(err64), np.log(ms64)
+        order = np.argsort(le)
+        return float(np.exp(np.interp(np.log(e), le[order], lt[order])))
+
+    out = {}
+    d, p, _ = W.shu_osher(51200, "fp64", "sp_weno", net)
+    s, _, _ = run(d, p)
+    ref = s.prim()[0, 0, 0]
+    del s
+    rows = {}
+    for prec, rec, ns in (("fp64", "sp_weno", (400, 800, 1600, 3200, 6400)),
+                          ("fp32_bf16", "sp_weno_dl", (400, 800, 1600))):
+        for n in ns:
+            d, p, _ = W.shu_osher(n, prec, rec, net)
+            s, ms, steps = run(d, p)
+            e = float(np.mean(np.abs(s.prim()[0, 0, 0] - ref.reshape(n, -1).mean(axis=1))))
+            rows.setdefault(prec, []).append((n, e, ms, steps))
+    out["shu_osher"] = rows
+    rows = {}
+    t_end = 2.0
+    for prec, rec, ns in (("fp64", "sp_weno", (64, 128, 256, 512, 1024)),
+                          ("fp32_bf16", "sp_weno_dl", (64, 128, 256, 512))):
+        for n in ns:
+            d, p, _ = W.batched(prec, rec, net, levels=(n,), nburgers=0, vortex_time=t_end)
+            s, ms, steps = run(d, p)
+            e = float(s.errors(W.vortex_exact_density(n, s.globals().time), comp=0)[0])
+            rows.setdefault(prec, []).append((n, e, ms, steps))
+    out["vortex_t2"] = rows
+    summary = {}
+    for case, rows in out.items():
+        e64 = np.array([r[1] for r in rows["fp64"]])
+        t64 = np.array([r[2] for r in rows["fp64"]])
+        summary[case] = [{"n": n, "fp32_dl_err": e, "fp32_dl_ms": ms, "fp64_plain_ms_at_same_err": interp_cost(e64, t64, e),
+                          "speedup": interp_cost(e64, t64, e) / ms,
+                          "inside_fp64_range": bool(e64.min() <= e <= e64.max())}
+                         for n, e, ms, _ in rows["fp32_bf16"]]
+    print(json.dumps({"metric": "time to matched L1 density error, FP64 plain SP-WENO / FP32+BF16 DSP-WENO",
+                      "unit": "ratio", "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+                      "runs": {c: {k: [list(r) for r in v] for k, v in rows.items()} for c, rows in out.items()},
+                      "columns": ["n", "l1_err", "device_ms_per_run", "steps"], "summary": summary}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="kh", choices=["kh", "shu_osher", "batched", "tgv"],
+    ap.add_argument("--workload", default="kh", choices=["kh", "shu_osher", "batched", "tgv", "matched_error"],
                     help="kh: 2-D Euler KH (the headline); shu_osher: 1-D Euler; batched: vortex OOC list plus "
                          "4096 Burgers problems in one batch (shared out over ranks); tgv: 3-D Navier-Stokes "
-                         "Taylor-Green vortex")
+                         "Taylor-Green vortex; matched_error: time to equal L1 error of the two forms on "
+                         "Shu-Osher and the isentropic vortex (its own JSON line)")
     ap.add_argument("--n", type=int, default=None, help="grid size (kh 2048, shu_osher 25600, tgv 256)")
     ap.add_argument("--precision", default="fp32_bf16", choices=["fp32_bf16", "fp64"])
     ap.add_argument("--recon", default="sp_weno_dl")
@@ -354,6 +424,13 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "matched_error":
+        if args.impl == "reference" or rank != 0:
+            return
+        import torch
+        torch.cuda.set_device(0)
+        matched_error(torch)
+        return
     if args.workload == "kh":
         n = args.n or 2048
         config = {"workload": f"kh{n}_{args.precision}_{args.recon}_kepes_tecno4_roe", "grid": [n, n],
