@@ -605,9 +605,13 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>*
   bool guard = fabsf(u2 - u1) < fmaxf(1e-15f, 4.0f * 1.1920929e-07f * mag);
   float feat[5], vx[5], vy[5];
   nn_features<float>(u0, u1, u2, u3, feat, vx, vy);
-  bool finite = true;
+  // one finiteness test of the sum: a NaN or infinity anywhere propagates into
+  // it (an overflow of the sum of huge finite vertices also lands on the
+  // SP-WENO fallback, which is a valid reconstruction)
+  float sum = 0.f;
 #pragma unroll
-  for (int k = 0; k < 5; k++) finite = finite && isfinite(feat[k]) && isfinite(vx[k]) && isfinite(vy[k]);
+  for (int k = 0; k < 5; k++) sum += (feat[k] + vx[k]) + vy[k];
+  const bool finite = isfinite(sum);
   bool use = valid && !guard && finite;
   if (!use) { feat[0] = feat[1] = feat[2] = feat[3] = feat[4] = 0.f; }
   bool inbox = true;
