@@ -218,7 +218,7 @@ def prob_info(descs):
     for d in descs:
         dim = 1 + (d.ny > 1) + (d.nz > 1)
         nv = 1 if d.model in (0, 1) else dim + 2
-        out.append((d.nx * d.ny * d.nz, nv, dim, d.model == 3, kernel_class(d, dim)))
+        out.append((d.nx * d.ny * d.nz, nv, dim, d.model in (3, 4), kernel_class(d, dim)))
     return out
 
 

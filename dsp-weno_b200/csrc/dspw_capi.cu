@@ -176,7 +176,6 @@ int problem_dim(const dspw_desc& d) {
 int validate(const dspw_desc& d) {
   if (d.abi_version != DSPW_ABI_VERSION) return DSPW_ERR_ARG;
   if (d.model < 0 || d.model > 4) return DSPW_ERR_ARG;
-  if (d.model == DSPW_NS_KEP) return DSPW_ERR_UNSUPPORTED;
   if (d.nx < 1 || d.ny < 1 || d.nz < 1) return DSPW_ERR_ARG;
   int dim = problem_dim(d);
   int N[3] = {d.nx, d.ny, d.nz};
@@ -199,7 +198,7 @@ int validate(const dspw_desc& d) {
       default: return DSPW_ERR_UNSUPPORTED;
     }
     if (!(d.gamma > 1.0) || !(d.gas_const > 0.0)) return DSPW_ERR_ARG;
-    if (d.model == DSPW_NS_ES) {
+    if (d.model == DSPW_NS_ES || d.model == DSPW_NS_KEP) {
       if (dim != 3) return DSPW_ERR_UNSUPPORTED;
       for (int f = 0; f < 6; f++)
         if (d.bc[f] != DSPW_BC_PERIODIC) return DSPW_ERR_UNSUPPORTED;   // enflo/src/parameter.cc:564-568
@@ -577,11 +576,11 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
     h->cell_start.push_back(off);
     h->maxcells = std::max(h->maxcells, ncells(descs[p]));
     h->maxdim = std::max(h->maxdim, h->hprob.back().dim);
-    if (descs[p].model == DSPW_NS_ES) h->has_ns = 1;
+    if (descs[p].model == DSPW_NS_ES || descs[p].model == DSPW_NS_KEP) h->has_ns = 1;
   }
-  if (h->has_ns) {
+  if (h->has_ns) {   // the viscous kernels run over the whole batch: Navier-Stokes problems only
     for (int p = 0; p < nprob; p++)
-      if (descs[p].model != DSPW_NS_ES) { delete h; return DSPW_ERR_UNSUPPORTED; }
+      if (descs[p].model != DSPW_NS_ES && descs[p].model != DSPW_NS_KEP) { delete h; return DSPW_ERR_UNSUPPORTED; }
   }
   h->ctot = off;
   // classes of problems sharing sweep kernels, in order of first appearance

@@ -1438,10 +1438,14 @@ __global__ void k_entvars(const ProbDev* prob, int nprob, const long long* cell_
     int lo = 0, hi = nprob - 1;
     while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_start[mid] <= g) lo = mid; else hi = mid - 1; }
     const ProbDev& P = prob[lo];
-    if (P.model != DSPW_NS_ES) continue;
+    if (P.model != DSPW_NS_ES && P.model != DSPW_NS_KEP) continue;
     T u[5], pr[5], v[5];
     load_cons<T>(U, ctot, g, P.nv, P.dim, u);
     cons_to_prim<T>(u, T(P.gamma), pr);
+    if (P.model == DSPW_NS_KEP) {   // the KE viscous flux works on primitive variables
+      for (int c = 0; c < 5; c++) Vout[c * ctot + g] = pr[c];
+      continue;
+    }
     prim_to_ent<T>(pr, T(P.gamma), v);
     for (int c = 0; c < 5; c++) Vout[c * ctot + g] = v[c];
   }
@@ -1451,6 +1455,72 @@ __global__ void k_entvars(const ProbDev* prob, int nprob, const long long* cell_
 // (i..i+1, j..j+1, k..k+1), periodic; writes 15 values (x, y, z fluxes).
 // The y flux keeps only its K22,K23 terms and the z flux only K33 because the
 // reference overwrites the earlier accumulations.
+// nodal_vlux_KE (enflo/src/vflux_KE.cc:15-96) of the node whose lower cell is
+// (i, j, k), from the primitive variables P of the 8 cells around it: node
+// average and velocity derivatives as nodal_avg_and_vel_derivatives
+// (enflo/src/nodal_avg_and_der.cc:16-82, derivative factor 1/(4 dx)), the
+// temperature derivatives with the factor 1/4/dx, stresses and heat flux.
+template <typename T>
+__device__ inline void visc_node_ke(const ProbDev& P, const T* V, long long ctot, T* node, long long g, int i,
+                                    int j, int k, int i1, int j1, int k1) {
+  typedef Mth<T> m;
+#define VC(c, ii, jj, kk) V[(c) * ctot + P.off + ((long long)(kk) * P.ny + (jj)) * P.nx + (ii)]
+  const T f1 = T(1.0 / 8.0);
+  T avg[5], Tx[3], Ty[3], Tz[3];
+#pragma unroll
+  for (int c = 0; c < 5; c++) {
+    avg[c] = VC(c, i1, j1, k1) * f1 + VC(c, i, j1, k1) * f1 + VC(c, i1, j, k1) * f1 + VC(c, i1, j1, k) * f1;
+    avg[c] += VC(c, i, j, k1) * f1 + VC(c, i, j1, k) * f1 + VC(c, i1, j, k) * f1 + VC(c, i, j, k) * f1;
+  }
+  const T vx = m::div(T(1.0), T(4.0) * T(P.dx)), vy = m::div(T(1.0), T(4.0) * T(P.dy)),
+          vz = m::div(T(1.0), T(4.0) * T(P.dz));
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int v = 1 + c;
+    const T v111 = VC(v, i1, j1, k1), v011 = VC(v, i, j1, k1), v101 = VC(v, i1, j, k1), v110 = VC(v, i1, j1, k);
+    const T v001 = VC(v, i, j, k1), v010 = VC(v, i, j1, k), v100 = VC(v, i1, j, k), v000 = VC(v, i, j, k);
+    Tx[c] = v111 * vx + v110 * vx + v101 * vx + v100 * vx;
+    Tx[c] += v011 * -vx + v010 * -vx + v001 * -vx + v000 * -vx;
+    Ty[c] = v111 * vy + v110 * vy + v011 * vy + v010 * vy;
+    Ty[c] += v101 * -vy + v100 * -vy + v001 * -vy + v000 * -vy;
+    Tz[c] = v111 * vz + v101 * vz + v011 * vz + v001 * vz;
+    Tz[c] += v110 * -vz + v100 * -vz + v010 * -vz + v000 * -vz;
+  }
+  const T Rg = T(P.gas_const);
+  auto tmp = [&](int ii, int jj, int kk) { return m::div(VC(4, ii, jj, kk), Rg * VC(0, ii, jj, kk)); };
+  const T t111 = tmp(i1, j1, k1), t110 = tmp(i1, j1, k), t101 = tmp(i1, j, k1), t100 = tmp(i1, j, k);
+  const T t011 = tmp(i, j1, k1), t010 = tmp(i, j1, k), t001 = tmp(i, j, k1), t000 = tmp(i, j, k);
+#undef VC
+  const double T_avg = (double)avg[4] / (P.gas_const * (double)avg[0]);
+  const T mu = T(viscosity(P, T_avg));
+  const T kappa = m::div(mu * T(P.Cp), T(P.prandtl));
+  const T fx = m::div(T(1.0 / 4.0), T(P.dx)), fy = m::div(T(1.0 / 4.0), T(P.dy)), fz = m::div(T(1.0 / 4.0), T(P.dz));
+  const T Tt_x = fx * (t111 + t110 + t101 + t100 - t011 - t010 - t001 - t000);
+  const T Tt_y = fy * (t111 + t110 + t011 + t010 - t101 - t100 - t001 - t000);
+  const T Tt_z = fz * (t111 + t101 + t011 + t001 - t110 - t100 - t010 - t000);
+  const T grad = Tx[0] + Ty[1] + Tz[2];
+  const T txx = mu * (T(2) * Tx[0] - T(2.0 / 3.0) * grad);
+  const T tyy = mu * (T(2) * Ty[1] - T(2.0 / 3.0) * grad);
+  const T tzz = mu * (T(2) * Tz[2] - T(2.0 / 3.0) * grad);
+  const T txy = mu * (Ty[0] + Tx[1]);
+  const T txz = mu * (Tx[2] + Tz[0]);
+  const T tyz = mu * (Ty[2] + Tz[1]);
+  T xf[5], yf[5], zf[5];
+  xf[0] = T(0); xf[1] = txx; xf[2] = txy; xf[3] = txz;
+  xf[4] = (avg[1] * txx + avg[2] * txy + avg[3] * txz) + kappa * Tt_x;
+  yf[0] = T(0); yf[1] = txy; yf[2] = tyy; yf[3] = tyz;
+  yf[4] = (avg[1] * txy + avg[2] * tyy + avg[3] * tyz) + kappa * Tt_y;
+  zf[0] = T(0); zf[1] = txz; zf[2] = tyz; zf[3] = tzz;
+  zf[4] = (avg[1] * txz + avg[2] * tyz + avg[3] * tzz) + kappa * Tt_z;
+  const T ax = -(T(P.dy) * T(P.dz)), ay = -(T(P.dx) * T(P.dz)), az = -(T(P.dx) * T(P.dy));
+#pragma unroll
+  for (int c = 0; c < 5; c++) {
+    node[(0 + c) * ctot + g] = xf[c] * ax;
+    node[(5 + c) * ctot + g] = yf[c] * ay;
+    node[(10 + c) * ctot + g] = zf[c] * az;
+  }
+}
+
 template <typename T>
 __global__ void k_visc_nodes(const ProbDev* prob, int nprob, const long long* cell_start, const T* V, long long ctot,
                              T* node) {
@@ -1460,10 +1530,14 @@ __global__ void k_visc_nodes(const ProbDev* prob, int nprob, const long long* ce
     int lo = 0, hi = nprob - 1;
     while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_start[mid] <= g) lo = mid; else hi = mid - 1; }
     const ProbDev& P = prob[lo];
-    if (P.model != DSPW_NS_ES) continue;
+    if (P.model != DSPW_NS_ES && P.model != DSPW_NS_KEP) continue;
     long long l = g - P.off;
     int i = (int)(l % P.nx), j = (int)((l / P.nx) % P.ny), k = (int)(l / ((long long)P.nx * P.ny));
     int i1 = (i + 1) % P.nx, j1 = (j + 1) % P.ny, k1 = (k + 1) % P.nz;
+    if (P.model == DSPW_NS_KEP) {
+      visc_node_ke<T>(P, V, ctot, node, g, i, j, k, i1, j1, k1);
+      continue;
+    }
 #define VC(c, ii, jj, kk) V[(c) * ctot + P.off + ((long long)(kk) * P.ny + (jj)) * P.nx + (ii)]
     const T f1 = T(1.0 / 8.0);
     const T fx = m::div(T(1.0 / 4.0), T(P.dx)), fy = m::div(T(1.0 / 4.0), T(P.dy)), fz = m::div(T(1.0 / 4.0), T(P.dz));
@@ -1540,7 +1614,7 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
     int lo = 0, hi = A.nprob - 1;
     while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_start[mid] <= g) lo = mid; else hi = mid - 1; }
     const ProbDev& P = A.prob[lo];
-    if (P.model != DSPW_NS_ES) continue;
+    if (P.model != DSPW_NS_ES && P.model != DSPW_NS_KEP) continue;
     ProbState& S = A.st[lo];
     if (!A.residual_only && !S.active) continue;
     pcur = lo;

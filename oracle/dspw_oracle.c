@@ -901,11 +901,68 @@ static void nodal_flux_es(or_state* s, int i, int j, int k, double* xf, double* 
   for (int c = 0; c < 5; c++) { xf[c] *= ax; yf[c] *= ay; zf[c] *= az; }
 }
 
-/* scatter one node's fluxes into its interior cells with weights +-1/4 */
+/* nodal_vlux_KE, enflo/src/vflux_KE.cc:15-96, with the node average and the
+ * velocity derivatives of nodal_avg_and_vel_derivatives
+ * (enflo/src/nodal_avg_and_der.cc:16-82; note its 1/(4 dx) against the
+ * 1/4/dx of the temperature derivatives) and Temperature (enflo/src/fv.cc:1329-1332). */
+static double temp_of(const or_state* s, const double* P) { return P[4] / (s->d.gas_const * P[0]); }
+
+static void nodal_flux_ke(or_state* s, int i, int j, int k, double* xf, double* yf, double* zf) {
+  const dspw_desc* d = &s->d;
+#define PP(a, b, c) (s->P + 5 * pidx(s, NG + i + (a), NG + j + (b), NG + k + (c)))
+  const double f1 = 1.0 / 8.0;
+  double avg[5], Tx[3], Ty[3], Tz[3];
+  for (int c = 0; c < 5; c++) {
+    avg[c] = PP(1, 1, 1)[c] * f1 + PP(0, 1, 1)[c] * f1 + PP(1, 0, 1)[c] * f1 + PP(1, 1, 0)[c] * f1;
+    avg[c] += PP(0, 0, 1)[c] * f1 + PP(0, 1, 0)[c] * f1 + PP(1, 0, 0)[c] * f1 + PP(0, 0, 0)[c] * f1;
+  }
+  const double vx = 1.0 / (4.0 * s->dx), vy = 1.0 / (4.0 * s->dy), vz = 1.0 / (4.0 * s->dz);
+  for (int c = 0; c < 3; c++) {
+    const int v = 1 + c;
+    Tx[c] = PP(1, 1, 1)[v] * vx + PP(1, 1, 0)[v] * vx + PP(1, 0, 1)[v] * vx + PP(1, 0, 0)[v] * vx;
+    Tx[c] += PP(0, 1, 1)[v] * -vx + PP(0, 1, 0)[v] * -vx + PP(0, 0, 1)[v] * -vx + PP(0, 0, 0)[v] * -vx;
+    Ty[c] = PP(1, 1, 1)[v] * vy + PP(1, 1, 0)[v] * vy + PP(0, 1, 1)[v] * vy + PP(0, 1, 0)[v] * vy;
+    Ty[c] += PP(1, 0, 1)[v] * -vy + PP(1, 0, 0)[v] * -vy + PP(0, 0, 1)[v] * -vy + PP(0, 0, 0)[v] * -vy;
+    Tz[c] = PP(1, 1, 1)[v] * vz + PP(1, 0, 1)[v] * vz + PP(0, 1, 1)[v] * vz + PP(0, 0, 1)[v] * vz;
+    Tz[c] += PP(1, 1, 0)[v] * -vz + PP(1, 0, 0)[v] * -vz + PP(0, 1, 0)[v] * -vz + PP(0, 0, 0)[v] * -vz;
+  }
+  const double T_avg = avg[4] / (d->gas_const * avg[0]);
+  const double mu = viscosity(d, T_avg);
+  const double Cp = d->gamma * d->gas_const / (d->gamma - 1.0);
+  const double kappa = mu * Cp / d->prandtl;
+  const double fx = 1.0 / 4.0 / s->dx, fy = 1.0 / 4.0 / s->dy, fz = 1.0 / 4.0 / s->dz;
+  const double t111 = temp_of(s, PP(1, 1, 1)), t110 = temp_of(s, PP(1, 1, 0)), t101 = temp_of(s, PP(1, 0, 1));
+  const double t100 = temp_of(s, PP(1, 0, 0)), t011 = temp_of(s, PP(0, 1, 1)), t010 = temp_of(s, PP(0, 1, 0));
+  const double t001 = temp_of(s, PP(0, 0, 1)), t000 = temp_of(s, PP(0, 0, 0));
+#undef PP
+  const double Tt_x = fx * (t111 + t110 + t101 + t100 - t011 - t010 - t001 - t000);
+  const double Tt_y = fy * (t111 + t110 + t011 + t010 - t101 - t100 - t001 - t000);
+  const double Tt_z = fz * (t111 + t101 + t011 + t001 - t110 - t100 - t010 - t000);
+  const double grad = Tx[0] + Ty[1] + Tz[2];
+  const double txx = mu * (2 * Tx[0] - (2.0 / 3.0) * grad);
+  const double tyy = mu * (2 * Ty[1] - (2.0 / 3.0) * grad);
+  const double tzz = mu * (2 * Tz[2] - (2.0 / 3.0) * grad);
+  const double txy = mu * (Ty[0] + Tx[1]);
+  const double txz = mu * (Tx[2] + Tz[0]);
+  const double tyz = mu * (Ty[2] + Tz[1]);
+  const double* u = avg + 1;
+  xf[0] = 0.0; xf[1] = txx; xf[2] = txy; xf[3] = txz;
+  xf[4] = (u[0] * txx + u[1] * txy + u[2] * txz) + kappa * Tt_x;
+  yf[0] = 0.0; yf[1] = txy; yf[2] = tyy; yf[3] = tyz;
+  yf[4] = (u[0] * txy + u[1] * tyy + u[2] * tyz) + kappa * Tt_y;
+  zf[0] = 0.0; zf[1] = txz; zf[2] = tyz; zf[3] = tzz;
+  zf[4] = (u[0] * txz + u[1] * tyz + u[2] * tzz) + kappa * Tt_z;
+  double ax = -(s->dy * s->dz), ay = -(s->dx * s->dz), az = -(s->dx * s->dy);
+  for (int c = 0; c < 5; c++) { xf[c] *= ax; yf[c] *= ay; zf[c] *= az; }
+}
+
+/* scatter one node's fluxes into its interior cells with weights +-1/4
+ * (nodal_vlux, enflo/src/fv.cc:773-780: ES for ns_es, KE otherwise) */
 static void scatter_node(or_state* s, int i, int j, int k) {
   const int Nx = s->nx, Ny = s->ny, Nz = s->nz;
   double xf[5], yf[5], zf[5];
-  nodal_flux_es(s, i, j, k, xf, yf, zf);
+  if (s->d.model == DSPW_NS_ES) nodal_flux_es(s, i, j, k, xf, yf, zf);
+  else nodal_flux_ke(s, i, j, k, xf, yf, zf);
   for (int l = 0; l < 2; ++l)
     for (int m = 0; m < 2; ++m)
       for (int n = 0; n < 2; ++n) {
@@ -968,7 +1025,7 @@ void or_residual(or_state* s, int rk, double* res) {
   (void)rk;
   if (!s->scalar) prim_to_ent(s);
   inviscid_residual(s);
-  if (s->d.model == DSPW_NS_ES) viscous_residual(s);
+  if (s->d.model == DSPW_NS_ES || s->d.model == DSPW_NS_KEP) viscous_residual(s);
   if (res) {
     size_t nc = (size_t)s->nx * s->ny * s->nz;
     for (size_t c = 0; c < nc; c++)

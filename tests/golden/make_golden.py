@@ -208,6 +208,12 @@ def run_cases():
     cases.append(("tgv_ns", "E", euler_cfg("kepes_tecno4_roe", "sp_weno_dl", model="ns_es", x=(0, "2*pi"),
                   y=(0, "2*pi"), z=(0, "2*pi"), Nx=8, Ny=8, Nz=8, ic=TGV_IC, dim=3, constants={"M": 0.1},
                   mu_ref=1 / 1600, prandtl=0.71, final_time=10.0), 3, 0.0))
+    cases.append(("tgv_ns_kep", "E", euler_cfg("kep4", "sp_weno", model="ns_kep", x=(0, "2*pi"), y=(0, "2*pi"),
+                  z=(0, "2*pi"), Nx=8, Ny=8, Nz=8, ic=TGV_IC, dim=3, constants={"M": 0.2}, mu_ref=0.02,
+                  prandtl=0.71, final_time=10.0), 4, 0.0))
+    cases.append(("tgv_ns_kep_tecno", "E", euler_cfg("kepes_tecno4_roe", "sp_weno_dl", model="ns_kep", x=(0, "2*pi"),
+                  y=(0, "2*pi"), z=(0, "2*pi"), Nx=8, Ny=8, Nz=8, ic=TGV_IC, dim=3, constants={"M": 0.1},
+                  mu_ref=1 / 1600, prandtl=0.71, final_time=10.0), 3, 0.0))
     cases.append(("tgv_ns_fixed", "E", euler_cfg("kepes_tecno4_roe", "sp_weno", model="ns_es", x=(0, "2*pi"),
                   y=(0, "2*pi"), z=(0, "2*pi"), Nx=6, Ny=6, Nz=6, ic=TGV_IC, dim=3, constants={"M": 0.3},
                   mu_ref=0.05, prandtl=0.71, final_time=10.0), 3, 0.01))
