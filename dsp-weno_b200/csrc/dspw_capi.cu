@@ -184,7 +184,7 @@ int validate(const dspw_desc& d) {
   if (!(d.xmax > d.xmin) || !(d.ymax > d.ymin) || !(d.zmax > d.zmin)) return DSPW_ERR_ARG;
   if (d.precision != DSPW_FP64 && d.precision != DSPW_FP32_BF16) return DSPW_ERR_ARG;
   if (d.time_scheme != DSPW_SSPRK3 && d.time_scheme != DSPW_RK1) return DSPW_ERR_UNSUPPORTED;
-  if (d.recon < DSPW_REC_SP_WENO || d.recon > DSPW_REC_SP_WENO_DL) return DSPW_ERR_UNSUPPORTED;
+  if (d.recon < DSPW_REC_SP_WENO || d.recon > DSPW_REC_MINABS) return DSPW_ERR_UNSUPPORTED;
   bool scalar = d.model <= DSPW_BURGERS;
   if (scalar) {
     if (d.model == DSPW_LINADV && !(d.flux >= DSPW_LIN_EC && d.flux <= DSPW_LIN_TECNO4)) return DSPW_ERR_ARG;
@@ -307,7 +307,7 @@ NetParams make_net(const dspw_desc& dn) {
 // dimension and reconstruction family; every other problem the generic ones.
 int spec_of(const ProbDev& P, const dspw_desc& d) {
   if (d.reserved_i[1] == 1) return 0;   // generic kernels requested
-  if (P.is_scalar || P.central != 0 || !P.fourth || !P.tecno) return 0;
+  if (P.is_scalar || P.central != 0 || !P.fourth || !P.tecno || P.recon >= DSPW_REC_FIRST) return 0;
   return spec_code(P.dim, P.spw_corr < 0 ? 2 : 1);
 }
 
@@ -918,7 +918,7 @@ int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k,
 int dspw_reconstruct_batch(const dspw_desc* d, const double* u4, long long n, double* recl, double* recr,
                            long long* limiter_acts) {
   if (!d || !u4 || !recl || !recr || n < 0) return DSPW_ERR_ARG;
-  if (d->recon < DSPW_REC_SP_WENO || d->recon > DSPW_REC_SP_WENO_DL) return DSPW_ERR_UNSUPPORTED;
+  if (d->recon < DSPW_REC_SP_WENO || d->recon > DSPW_REC_MINABS) return DSPW_ERR_UNSUPPORTED;
   if (d->precision != DSPW_FP64 && d->precision != DSPW_FP32_BF16) return DSPW_ERR_ARG;
   if (n == 0) return DSPW_OK;
   ProbDev P = make_prob(*d, 0);

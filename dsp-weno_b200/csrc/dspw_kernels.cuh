@@ -642,7 +642,9 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>*
 template <typename T, typename Sp>
 __device__ inline void reconstruct_lane(const ProbDev& P, const NetParams& NP, WarpSmem<T>* sm,
                                         int lane, bool valid, T s0, T s1, T s2, T s3, T& l, T& r, int& viol) {
-  if (Sp::fixed ? Sp::rec == 1 : P.spw_corr >= 0) {
+  if (!Sp::fixed && P.recon >= DSPW_REC_FIRST) {
+    if (valid) simple_recon<T>(P.recon, s0, s1, s2, s3, l, r);
+  } else if (Sp::fixed ? Sp::rec == 1 : P.spw_corr >= 0) {
     if (valid) sp_weno<T>(s0, s1, s2, s3, P.spw_corr, l, r);
   } else {
     viol += dsp_weno_warp<T>(NP, sm, lane, valid, s0, s1, s2, s3, l, r);

@@ -100,6 +100,34 @@ DSPW_HD void spw_cp(T t0, T t1, T del1, T scale, T& C, T& corr) {
   }
 }
 
+// The reference's lower-order reconstructions of one component
+// (enflo/src/reconstruct.cc): kind 4 first order (:14-30), 5 unlimited MUSCL
+// with kappa = 1/3 (:35-56), 6 / 7 MUSCL with the minmod / minabs limited slope
+// 0.5 * limiter(outer jump, face jump) (:61-79, limited_slope :162-186,
+// minmod / minabs enflo/src/limiter.h:22-57).
+template <typename T>
+DSPW_HD void simple_recon(int kind, T s0, T s1, T s2, T s3, T& recl, T& recr) {
+  typedef Mth<T> m;
+  if (kind == 4) { recl = s1; recr = s2; return; }
+  const T ds = s2 - s1, dl = s1 - s0, dr = s3 - s2;
+  if (kind == 5) {
+    const T K = T(1.0 / 3.0);
+    recl = s1 + (dl * (T(1.0) - K) + ds * (T(1.0) + K)) * T(0.25);
+    recr = s2 - (dr * (T(1.0) - K) + ds * (T(1.0) + K)) * T(0.25);
+    return;
+  }
+  T sl, sr;
+  if (kind == 6) {
+    sl = (dl * ds > T(0.0)) ? m::min(m::abs(dl), m::abs(ds)) * ((dl < T(0)) ? T(-1) : T(1)) : T(0.0);
+    sr = (dr * ds > T(0.0)) ? m::min(m::abs(dr), m::abs(ds)) * ((dr < T(0)) ? T(-1) : T(1)) : T(0.0);
+  } else {
+    sl = (m::abs(dl) > m::abs(ds)) ? ds : dl;
+    sr = (m::abs(dr) > m::abs(ds)) ? ds : dr;
+  }
+  recl = s1 + T(0.5) * sl;
+  recr = s2 - T(0.5) * sr;
+}
+
 // sp_weno_rec, enflo/src/limiter.h:193-252.  corr: 0 sp_weno, 1 sp_wenoc, 2 sp_weno_corr2
 template <typename T>
 DSPW_HD void sp_weno(T s0, T s1, T s2, T s3, int corr, T& recl, T& recr) {

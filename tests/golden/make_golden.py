@@ -124,6 +124,49 @@ def gen_faces_scalar(rng):
     np.savez_compressed(OUT / "faces_scalar.npz", **out)
 
 
+SIMPLE_RECONS = ["first", "second", "minmod", "minabs"]
+
+
+def gen_faces_simple(rng):
+    """Face fluxes with the reference's first-order, unlimited MUSCL and
+    minmod / minabs limited reconstructions (reconstruct.cc:14-79, 162-186)
+    inside the TeCNO fluxes, Euler and scalar."""
+    out = {}
+    for flux in ("kepes_tecno4_roe", "kepes_tecno_roe", "kepes_tecno4_rusanov", "roe_tecno_roe"):
+        for recon in SIMPLE_RECONS:
+            R = O.RefEuler(euler_cfg(flux, recon, EC1_fix="yes" if "roe" in flux else "no", y=(0, 0.5), z=(0, 0.25)))
+            n = 120
+            P = random_prim_stencils(rng, n)
+            dirs = np.arange(n) % 3
+            F = np.zeros((n, 5)); V = np.zeros((n, 4, 5))
+            for t in range(n):
+                F[t], V[t] = R.face_flux(P[t], int(dirs[t]))
+            key = f"E|{flux}|{recon}|{int('roe' in flux)}"
+            out[key + "|P"] = P
+            out[key + "|dir"] = dirs
+            out[key + "|F"] = F
+            out[key + "|V"] = V
+            out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
+    for model, flux in (("linadv", "lin_tecno4"), ("linadv", "lin_tecno"), ("burgers", "bur_tecno4"),
+                        ("burgers", "bur_tecno")):
+        for recon in SIMPLE_RECONS:
+            cfg = dict(model=model, x=("-pi", "pi"), y=(0, 0.5), z=(0, 0.25), Nx=16, Ny=2, Nz=2, cfl=0.5,
+                       final_time=0.5, reconstruct=recon, net_file=NET, flux=flux, ic="sin(x)",
+                       vel=(1.0, -0.5, 0.25), bc="periodic")
+            R = O.RefScalar(cfg)
+            n = 200
+            U = rng.normal(0, 1, (n, 4))
+            U[: n // 3] = np.sin(rng.uniform(0, 6.3, (n // 3, 1)) + 0.05 * np.arange(4)[None, :])
+            dirs = np.arange(n) % 3
+            F = np.array([R.face_flux(U[t], int(dirs[t])) for t in range(n)])
+            key = f"S|{flux}|{recon}"
+            out[key + "|U"] = U
+            out[key + "|dir"] = dirs
+            out[key + "|F"] = F
+            out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
+    np.savez_compressed(OUT / "faces_simple.npz", **out)
+
+
 def structured_stencils(rng):
     """Stencils that hit the special branches: flat, linear (theta = 1), theta
     = -1 (psi = -1), extrema, jumps, tiny jumps, large magnitudes."""
@@ -260,6 +303,7 @@ def main():
     gen_recon(rng)
     gen_runs()
     gen_ooc()
+    gen_faces_simple(np.random.default_rng(20240612))
 
 
 if __name__ == "__main__":

@@ -100,7 +100,8 @@ def random_state(rng, nx, ny, nz, smooth=True):
 
 
 @pytest.mark.parametrize("flux", FLUXES)
-@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_corr2", "sp_weno_dl"])
+@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_corr2", "sp_weno_dl", "first", "second", "minmod",
+                                   "minabs"])
 @pytest.mark.parametrize("dims", [(24, 1, 1), (16, 12, 1), (8, 6, 5)])
 def test_residual_vs_oracle(flux, recon, dims):
     if "tecno" not in flux and recon != "sp_weno":
@@ -146,7 +147,7 @@ def test_residual_rough_vs_oracle(recon):
 
 @pytest.mark.parametrize("model,flux", [("linadv", "lin_tecno4"), ("linadv", "lin_tecno"), ("linadv", "lin_ec4"),
                                         ("burgers", "bur_tecno4"), ("burgers", "bur_tecno"), ("burgers", "bur_ec")])
-@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_dl"])
+@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_dl", "first", "second", "minmod", "minabs"])
 @pytest.mark.parametrize("bc", ["periodic", "wall", "neumann"])
 def test_scalar_residual_vs_oracle(model, flux, recon, bc):
     nx = 40
