@@ -192,6 +192,7 @@ int validate(const dspw_desc& d) {
   } else {
     switch (d.flux) {
       case DSPW_KEPEC: case DSPW_KEPEC4: case DSPW_KEP: case DSPW_KEP4: case DSPW_ROE_EC: case DSPW_ROE_EC4:
+      case DSPW_KEPS: case DSPW_KEPS4: case DSPW_ROE:
       case DSPW_KEP_TECNO_ROE: case DSPW_KEPES_TECNO_ROE: case DSPW_KEPES_TECNO_RUSANOV:
       case DSPW_ROE_TECNO_ROE: case DSPW_KEPES_TECNO4_ROE: case DSPW_KEPES_TECNO4_RUSANOV:
       case DSPW_ROE_TECNO4_ROE: break;
@@ -265,6 +266,9 @@ ProbDev make_prob(const dspw_desc& d, long long off) {
     case DSPW_KEP4: P.central = 1; P.fourth = 1; break;
     case DSPW_ROE_EC: P.central = 2; break;
     case DSPW_ROE_EC4: P.central = 2; P.fourth = 1; break;
+    case DSPW_KEPS: P.central = 3; break;
+    case DSPW_KEPS4: P.central = 3; P.fourth = 1; break;
+    case DSPW_ROE: P.central = 4; break;
     case DSPW_KEP_TECNO_ROE: P.central = 1; P.tecno = 1; P.ec1 = 0; break;   // no EC1_fix (kep_tecno_roe.cc)
     case DSPW_KEPES_TECNO_ROE: P.tecno = 1; break;
     case DSPW_KEPES_TECNO_RUSANOV: P.tecno = 1; P.rusanov = 1; P.ec1 = 0; break;

@@ -42,7 +42,7 @@ struct ProbDev {
   int nx, ny, nz;
   int bc[6];
   int ec1, mu_model, max_iter, is_scalar;
-  int central;        // 0 kepec, 1 kep, 2 roe_ec (TeCNO central part)
+  int central;        // 0 kepec, 1 kep, 2 roe_ec, 3 keps, 4 roe (two-point flux; TeCNO central part)
   int fourth;         // 1: 4th-order central combination
   int tecno;          // 1: entropy-stable dissipation added
   int rusanov;        // 1: Rusanov Lambda, 0: Roe Lambda
@@ -450,11 +450,88 @@ DSPW_HD void roe_ec_pair(const T* Pl, const T* Pr, T gamma, T area, T F[5]) {
   for (int c = 0; c < 5; c++) F[c] *= area;
 }
 
+// keps_flux, enflo/src/keps.cc:10-48 (arithmetic means of rho and beta)
+template <typename T, int DIR>
+DSPW_HD void keps_pair(const T* Pl, const T* Pr, T gamma, T Rg, T area, T F[5]) {
+  typedef Mth<T> m;
+  T rhol = Pl[0], rhor = Pr[0];
+  T rho = T(0.5) * (rhol + rhor);
+  T templ = m::div(Pl[4], Rg * rhol);
+  T tempr = m::div(Pr[4], Rg * rhor);
+  T vel2 = T(0.5) * ((Pl[1] * Pl[1] + Pl[2] * Pl[2] + Pl[3] * Pl[3]) + (Pr[1] * Pr[1] + Pr[2] * Pr[2] + Pr[3] * Pr[3]));
+  T betal = m::div(T(0.5), Rg * templ);
+  T betar = m::div(T(0.5), Rg * tempr);
+  T beta = T(0.5) * (betal + betar);
+  T p = m::div(T(0.5) * rho, beta);
+  T vel[3] = {Pl[1] * T(0.5) + Pr[1] * T(0.5), Pl[2] * T(0.5) + Pr[2] * T(0.5), Pl[3] * T(0.5) + Pr[3] * T(0.5)};
+  T vn = vel[0] * T(DIR == 0) + vel[1] * T(DIR == 1) + vel[2] * T(DIR == 2);
+  F[0] = rho * vn;
+  F[1] = T(DIR == 0) * p + vel[0] * F[0];
+  F[2] = T(DIR == 1) * p + vel[1] * F[0];
+  F[3] = T(DIR == 2) * p + vel[2] * F[0];
+  F[4] = T(0.5) * (m::div(T(1.0), (gamma - T(1.0)) * beta) - vel2) * F[0] +
+         (F[1] * vel[0] + F[2] * vel[1] + F[3] * vel[2]);
+#pragma unroll
+  for (int c = 0; c < 5; c++) F[c] *= area;
+}
+
+// roe_flux (Roe's flux without entropy fix), enflo/src/roe.cc:10-86
+template <typename T, int DIR>
+DSPW_HD void roe_pair(const T* Pl, const T* Pr, T gamma, T area, T F[5]) {
+  typedef Mth<T> m;
+  const T n[3] = {T(DIR == 0), T(DIR == 1), T(DIR == 2)};
+  T rhol = Pl[0], rhor = Pr[0], pl = Pl[4], pr = Pr[4];
+  T hl = m::div(m::div(gamma * pl, rhol), gamma - T(1.0)) + T(0.5) * (Pl[1] * Pl[1] + Pl[2] * Pl[2] + Pl[3] * Pl[3]);
+  T hr = m::div(m::div(gamma * pr, rhor), gamma - T(1.0)) + T(0.5) * (Pr[1] * Pr[1] + Pr[2] * Pr[2] + Pr[3] * Pr[3]);
+  T rls = m::sqrt(rhol), rrs = m::sqrt(rhor);
+  T fl = m::div(rls, rls + rrs);
+  T fr = T(1.0) - fl;
+  T rho = rls * rrs;
+  T vel[3] = {Pl[1] * fl + Pr[1] * fr, Pl[2] * fl + Pr[2] * fr, Pl[3] * fl + Pr[3] * fr};
+  T h = hl * fl + hr * fr;
+  T vn = vel[0] * n[0] + vel[1] * n[1] + vel[2] * n[2];
+  T a = m::sqrt((gamma - T(1.0)) * (h - T(0.5) * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2])));
+  T dp = pr - pl;
+  T vln = Pl[1] * n[0] + Pl[2] * n[1] + Pl[3] * n[2];
+  T vrn = Pr[1] * n[0] + Pr[2] * n[1] + Pr[3] * n[2];
+  T dV = vrn - vln;
+  if (vn >= T(0.0)) {
+    T lambda = vn - a;
+    T coeff = m::div(T(0.5) * (dp - rho * a * dV), a * a);
+    T factor = ((T(0.0) < lambda) ? T(0.0) : lambda) * coeff;   // std::min(lambda, 0.0)
+    F[0] = rhol * vln;
+#pragma unroll
+    for (int c = 0; c < 3; c++) F[1 + c] = n[c] * pl + Pl[1 + c] * (rhol * vln);
+    F[4] = hl * F[0];
+    F[0] += factor;
+#pragma unroll
+    for (int c = 0; c < 3; c++) F[1 + c] += vel[c] * factor + n[c] * (-a * factor);
+    F[4] += (h - a * vn) * factor;
+  } else {
+    T lambda = vn + a;
+    T coeff = m::div(T(0.5) * (dp + rho * a * dV), a * a);
+    T factor = ((lambda < T(0.0)) ? T(0.0) : lambda) * coeff;   // std::max(lambda, 0.0)
+    F[0] = rhor * vrn;
+#pragma unroll
+    for (int c = 0; c < 3; c++) F[1 + c] = n[c] * pr + Pr[1 + c] * (rhor * vrn);
+    F[4] = hr * F[0];
+    F[0] -= factor;
+#pragma unroll
+    for (int c = 0; c < 3; c++) F[1 + c] += vel[c] * (-factor) + n[c] * (-a * factor);
+    F[4] -= (h + a * vn) * factor;
+  }
+#pragma unroll
+  for (int c = 0; c < 5; c++) F[c] *= area;
+}
+
+// two-point flux of kind 0 kepec, 1 kep, 2 roe_ec, 3 keps, 4 roe
 template <typename T, int DIR>
 DSPW_HD void central_pair(int kind, const T* Pl, const T* Pr, T gamma, T Rg, T area, T F[5]) {
   if (kind == 0) kepec_pair<T, DIR>(Pl, Pr, gamma, Rg, area, F);
   else if (kind == 1) kep_pair<T, DIR>(Pl, Pr, gamma, area, F);
-  else roe_ec_pair<T, DIR>(Pl, Pr, gamma, area, F);
+  else if (kind == 2) roe_ec_pair<T, DIR>(Pl, Pr, gamma, area, F);
+  else if (kind == 3) keps_pair<T, DIR>(Pl, Pr, gamma, Rg, area, F);
+  else roe_pair<T, DIR>(Pl, Pr, gamma, area, F);
 }
 
 // ------------------------------------------------- BF16 tensor-core network --

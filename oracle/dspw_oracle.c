@@ -325,6 +325,69 @@ static void roe_ec_flux(const dspw_desc* d, const double* Pl, const double* Pr, 
   for (int c = 0; c < 5; c++) F[c] *= area;
 }
 
+/* keps_flux, enflo/src/keps.cc:10-48: arithmetic means of rho and beta */
+static void keps_flux(const dspw_desc* d, const double* Pl, const double* Pr, const double* n,
+                      double area, double* F) {
+  double R = d->gas_const, G = d->gamma;
+  double rhol = Pl[0], rhor = Pr[0];
+  double rho = 0.5 * (rhol + rhor);
+  double templ = Pl[4] / (R * rhol);
+  double tempr = Pr[4] / (R * rhor);
+  double vel2 = 0.5 * (sq3(Pl + 1) + sq3(Pr + 1));
+  double betal = 0.5 / (R * templ);
+  double betar = 0.5 / (R * tempr);
+  double beta = 0.5 * (betal + betar);
+  double p = 0.5 * rho / beta;
+  double vel[3] = {Pl[1] * 0.5 + Pr[1] * 0.5, Pl[2] * 0.5 + Pr[2] * 0.5, Pl[3] * 0.5 + Pr[3] * 0.5};
+  double vn = dot3(vel, n);
+  F[0] = rho * vn;
+  for (int c = 0; c < 3; c++) F[1 + c] = n[c] * p + vel[c] * F[0];
+  F[4] = 0.5 * (1.0 / ((G - 1.0) * beta) - vel2) * F[0] + dot3(F + 1, vel);
+  for (int c = 0; c < 5; c++) F[c] *= area;
+}
+
+/* roe_flux (Roe's flux without entropy fix), enflo/src/roe.cc:10-86 */
+static void roe_flux(const dspw_desc* d, const double* Pl, const double* Pr, const double* n,
+                     double area, double* F) {
+  double G = d->gamma;
+  double rhol = Pl[0], rhor = Pr[0], pl = Pl[4], pr = Pr[4];
+  double hl = G * pl / rhol / (G - 1.0) + 0.5 * sq3(Pl + 1);
+  double hr = G * pr / rhor / (G - 1.0) + 0.5 * sq3(Pr + 1);
+  double rls = sqrt(rhol), rrs = sqrt(rhor);
+  double fl = rls / (rls + rrs);
+  double fr = 1.0 - fl;
+  double rho = rls * rrs;
+  double vel[3] = {Pl[1] * fl + Pr[1] * fr, Pl[2] * fl + Pr[2] * fr, Pl[3] * fl + Pr[3] * fr};
+  double h = hl * fl + hr * fr;
+  double vn = dot3(vel, n);
+  double a = sqrt((G - 1.0) * (h - 0.5 * sq3(vel)));
+  double dp = pr - pl;
+  double vln = dot3(Pl + 1, n), vrn = dot3(Pr + 1, n);
+  double dV = vrn - vln;
+  if (vn >= 0.0) {
+    double lambda = vn - a;
+    double coeff = 0.5 * (dp - rho * a * dV) / (a * a);
+    double factor = ((0.0 < lambda) ? 0.0 : lambda) * coeff;   /* std::min(lambda, 0.0) */
+    F[0] = rhol * vln;
+    for (int c = 0; c < 3; c++) F[1 + c] = n[c] * pl + Pl[1 + c] * (rhol * vln);
+    F[4] = hl * F[0];
+    F[0] += factor;
+    for (int c = 0; c < 3; c++) F[1 + c] += vel[c] * factor + n[c] * (-a * factor);
+    F[4] += (h - a * vn) * factor;
+  } else {
+    double lambda = vn + a;
+    double coeff = 0.5 * (dp + rho * a * dV) / (a * a);
+    double factor = ((lambda < 0.0) ? 0.0 : lambda) * coeff;   /* std::max(lambda, 0.0) */
+    F[0] = rhor * vrn;
+    for (int c = 0; c < 3; c++) F[1 + c] = n[c] * pr + Pr[1 + c] * (rhor * vrn);
+    F[4] = hr * F[0];
+    F[0] -= factor;
+    for (int c = 0; c < 3; c++) F[1 + c] += vel[c] * (-factor) + n[c] * (-a * factor);
+    F[4] -= (h + a * vn) * factor;
+  }
+  for (int c = 0; c < 5; c++) F[c] *= area;
+}
+
 typedef void (*two_point_fn)(const dspw_desc*, const double*, const double*, const double*, double, double*);
 
 /* kepec4 / roe_ec4 / kep4 combination, enflo/src/kepec4.cc:10-38, roe_ec4.cc:10-34 */
@@ -461,6 +524,9 @@ static void euler_num_flux(const dspw_desc* d, const double* P, const double* V,
     case DSPW_KEP4: four_point(d, kep_flux, P, n, area, F); break;
     case DSPW_ROE_EC: roe_ec_flux(d, P + 5, P + 10, n, area, F); break;
     case DSPW_ROE_EC4: four_point(d, roe_ec_flux, P, n, area, F); break;
+    case DSPW_KEPS: keps_flux(d, P + 5, P + 10, n, area, F); break;
+    case DSPW_KEPS4: four_point(d, keps_flux, P, n, area, F); break;
+    case DSPW_ROE: roe_flux(d, P + 5, P + 10, n, area, F); break;
     default: tecno_flux(d, P, V, n, area, h, F);
   }
 }

@@ -164,6 +164,21 @@ def gen_faces_simple(rng):
             out[key + "|dir"] = dirs
             out[key + "|F"] = F
             out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
+    # the standalone keps, keps4 and roe fluxes (keps.cc, keps4.cc, roe.cc)
+    for flux in ("keps", "keps4", "roe"):
+        R = O.RefEuler(euler_cfg(flux, "sp_weno", y=(0, 0.5), z=(0, 0.25)))
+        n = 150
+        P = random_prim_stencils(rng, n)
+        dirs = np.arange(n) % 3
+        F = np.zeros((n, 5)); V = np.zeros((n, 4, 5))
+        for t in range(n):
+            F[t], V[t] = R.face_flux(P[t], int(dirs[t]))
+        key = f"E|{flux}|sp_weno|0"
+        out[key + "|P"] = P
+        out[key + "|dir"] = dirs
+        out[key + "|F"] = F
+        out[key + "|V"] = V
+        out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
     np.savez_compressed(OUT / "faces_simple.npz", **out)
 
 

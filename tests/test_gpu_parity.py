@@ -83,7 +83,8 @@ def test_reduced_layout_vs_oracle(name):
 
 
 FLUXES = ["kepes_tecno4_roe", "kepes_tecno_roe", "kepes_tecno4_rusanov", "kepes_tecno_rusanov", "kep_tecno_roe",
-          "roe_tecno_roe", "roe_tecno4_roe", "kepec4", "kepec", "kep", "kep4", "roe_ec", "roe_ec4"]
+          "roe_tecno_roe", "roe_tecno4_roe", "kepec4", "kepec", "kep", "kep4", "roe_ec", "roe_ec4", "keps", "keps4",
+          "roe"]
 
 
 def random_state(rng, nx, ny, nz, smooth=True):
