@@ -184,7 +184,7 @@ int validate(const dspw_desc& d) {
   if (!(d.xmax > d.xmin) || !(d.ymax > d.ymin) || !(d.zmax > d.zmin)) return DSPW_ERR_ARG;
   if (d.precision != DSPW_FP64 && d.precision != DSPW_FP32_BF16) return DSPW_ERR_ARG;
   if (d.time_scheme != DSPW_SSPRK3 && d.time_scheme != DSPW_RK1) return DSPW_ERR_UNSUPPORTED;
-  if (d.recon < DSPW_REC_SP_WENO || d.recon > DSPW_REC_MINABS) return DSPW_ERR_UNSUPPORTED;
+  if (d.recon < DSPW_REC_SP_WENO || d.recon > DSPW_REC_ENO2) return DSPW_ERR_UNSUPPORTED;
   bool scalar = d.model <= DSPW_BURGERS;
   if (scalar) {
     if (d.model == DSPW_LINADV && !(d.flux >= DSPW_LIN_EC && d.flux <= DSPW_LIN_TECNO4)) return DSPW_ERR_ARG;
@@ -922,7 +922,7 @@ int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k,
 int dspw_reconstruct_batch(const dspw_desc* d, const double* u4, long long n, double* recl, double* recr,
                            long long* limiter_acts) {
   if (!d || !u4 || !recl || !recr || n < 0) return DSPW_ERR_ARG;
-  if (d->recon < DSPW_REC_SP_WENO || d->recon > DSPW_REC_MINABS) return DSPW_ERR_UNSUPPORTED;
+  if (d->recon < DSPW_REC_SP_WENO || d->recon > DSPW_REC_ENO2) return DSPW_ERR_UNSUPPORTED;
   if (d->precision != DSPW_FP64 && d->precision != DSPW_FP32_BF16) return DSPW_ERR_ARG;
   if (n == 0) return DSPW_OK;
   ProbDev P = make_prob(*d, 0);

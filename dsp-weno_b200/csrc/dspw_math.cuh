@@ -104,11 +104,29 @@ DSPW_HD void spw_cp(T t0, T t1, T del1, T scale, T& C, T& corr) {
 // (enflo/src/reconstruct.cc): kind 4 first order (:14-30), 5 unlimited MUSCL
 // with kappa = 1/3 (:35-56), 6 / 7 MUSCL with the minmod / minabs limited slope
 // 0.5 * limiter(outer jump, face jump) (:61-79, limited_slope :162-186,
-// minmod / minabs enflo/src/limiter.h:22-57).
+// minmod / minabs enflo/src/limiter.h:22-57), 8 point-wise ENO of level 2
+// (:84-110).
+template <typename T>
+DSPW_HD T eno2_side(T q0, T q1, T q2) {
+  // eno_pw with eno_level 2 (enflo/src/limiter.h:63-96, ENO2_COEF :8-9): the
+  // stencil shifts left when the right divided difference is larger
+  typedef Mth<T> m;
+  T res = T(0);
+  if (m::abs(q2 - q1) > m::abs(q1 - q0)) {
+    res += T(-0.5) * q0;
+    res += T(1.5) * q1;
+  } else {
+    res += T(0.5) * q1;
+    res += T(0.5) * q2;
+  }
+  return res;
+}
+
 template <typename T>
 DSPW_HD void simple_recon(int kind, T s0, T s1, T s2, T s3, T& recl, T& recr) {
   typedef Mth<T> m;
   if (kind == 4) { recl = s1; recr = s2; return; }
+  if (kind == 8) { recl = eno2_side<T>(s0, s1, s2); recr = eno2_side<T>(s3, s2, s1); return; }
   const T ds = s2 - s1, dl = s1 - s0, dr = s3 - s2;
   if (kind == 5) {
     const T K = T(1.0 / 3.0);

@@ -133,6 +133,7 @@ Param read_param(const std::string& path) {
   t.entry("final_time"); P.final_time = t.number();
   t.entry("min_residue"); P.min_residue = t.number();
   t.entry("reconstruct"); P.reconstruct = t.word();
+  if (P.reconstruct == "eno") P.reconstruct += std::to_string(t.integer());   // "eno <level>", :178-184
   t.entry("net_file"); P.net_file = t.word();
   t.entry("}");
   // material: scalar files start with 'model', system files with 'gamma'

@@ -63,7 +63,8 @@ enum dspw_flux {
  * enflo/src/reconstruct.cc:14-110 */
 enum dspw_recon {
   DSPW_REC_SP_WENO = 0, DSPW_REC_SP_WENOC = 1, DSPW_REC_SP_WENO_CORR2 = 2, DSPW_REC_SP_WENO_DL = 3,
-  DSPW_REC_FIRST = 4, DSPW_REC_SECOND = 5, DSPW_REC_MINMOD = 6, DSPW_REC_MINABS = 7
+  DSPW_REC_FIRST = 4, DSPW_REC_SECOND = 5, DSPW_REC_MINMOD = 6, DSPW_REC_MINABS = 7,
+  DSPW_REC_ENO2 = 8          /* point-wise ENO, eno_level 2 (param.in "reconstruct eno 2") */
 };
 
 /* boundary conditions (enflo/src/ext_constants.h:25).  DIRICHLET is parsed but

@@ -257,6 +257,22 @@ static void reconstruct1(const dspw_desc* d, const double s[4], double* l, doubl
       *r = s[2] - 0.5 * sr;
       break;
     }
+    case DSPW_REC_ENO2: {           /* reconstruct_eno_pw + eno_pw, eno_level 2 (limiter.h:63-96) */
+      const double c[2][2] = {{-0.5, 1.5}, {0.5, 0.5}};   /* ENO2_COEF, limiter.h:8-9 */
+      const double L[3] = {s[0], s[1], s[2]}, Rr[3] = {s[3], s[2], s[1]};
+      const double* st[2] = {L, Rr};
+      double out[2];
+      for (int side = 0; side < 2; side++) {
+        const double* q = st[side];
+        int r = 0;
+        if (fabs(q[2] - q[1]) > fabs(q[1] - q[0])) r++;
+        double res = 0;
+        for (int i = 0; i < 2; i++) res += c[1 - r][i] * q[1 - r + i];
+        out[side] = res;
+      }
+      *l = out[0]; *r = out[1];
+      break;
+    }
     default: *l = s[1]; *r = s[2];
   }
 }

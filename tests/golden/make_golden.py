@@ -179,6 +179,35 @@ def gen_faces_simple(rng):
         out[key + "|F"] = F
         out[key + "|V"] = V
         out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
+    # point-wise ENO of level 2 (param.in "reconstruct eno 2", reconstruct.cc:84-110)
+    for flux in ("kepes_tecno4_roe", "kepes_tecno_roe"):
+        R = O.RefEuler(euler_cfg(flux, "eno 2", EC1_fix="yes", y=(0, 0.5), z=(0, 0.25)))
+        n = 150
+        P = random_prim_stencils(rng, n)
+        dirs = np.arange(n) % 3
+        F = np.zeros((n, 5)); V = np.zeros((n, 4, 5))
+        for t in range(n):
+            F[t], V[t] = R.face_flux(P[t], int(dirs[t]))
+        key = f"E|{flux}|eno2|1"
+        out[key + "|P"] = P
+        out[key + "|dir"] = dirs
+        out[key + "|F"] = F
+        out[key + "|V"] = V
+        out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
+    for model, flux in (("linadv", "lin_tecno4"), ("burgers", "bur_tecno4")):
+        cfg = dict(model=model, x=("-pi", "pi"), y=(0, 0.5), z=(0, 0.25), Nx=16, Ny=2, Nz=2, cfl=0.5,
+                   final_time=0.5, reconstruct="eno 2", net_file=NET, flux=flux, ic="sin(x)",
+                   vel=(1.0, -0.5, 0.25), bc="periodic")
+        R = O.RefScalar(cfg)
+        n = 200
+        U = rng.normal(0, 1, (n, 4))
+        dirs = np.arange(n) % 3
+        F = np.array([R.face_flux(U[t], int(dirs[t])) for t in range(n)])
+        key = f"S|{flux}|eno2"
+        out[key + "|U"] = U
+        out[key + "|dir"] = dirs
+        out[key + "|F"] = F
+        out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
     np.savez_compressed(OUT / "faces_simple.npz", **out)
 
 

