@@ -128,6 +128,7 @@ struct dspw_handle {
   void* Ua = nullptr;
   void* Ub = nullptr;
   void* R = nullptr;
+  void* R2 = nullptr;                  // classic RK4 only
   void* V = nullptr;
   void* node = nullptr;
   double* dstage = nullptr;
@@ -183,7 +184,7 @@ int validate(const dspw_desc& d) {
     if (N[k] < 2) return DSPW_ERR_UNSUPPORTED;   // a swept direction needs >= 2 cells
   if (!(d.xmax > d.xmin) || !(d.ymax > d.ymin) || !(d.zmax > d.zmin)) return DSPW_ERR_ARG;
   if (d.precision != DSPW_FP64 && d.precision != DSPW_FP32_BF16) return DSPW_ERR_ARG;
-  if (d.time_scheme != DSPW_SSPRK3 && d.time_scheme != DSPW_RK1) return DSPW_ERR_UNSUPPORTED;
+  if (d.time_scheme < DSPW_RK1 || d.time_scheme > DSPW_RK4) return DSPW_ERR_UNSUPPORTED;
   if (d.recon < DSPW_REC_SP_WENO || d.recon > DSPW_REC_ENO2) return DSPW_ERR_UNSUPPORTED;
   bool scalar = d.model <= DSPW_BURGERS;
   if (scalar) {
@@ -214,6 +215,11 @@ int validate(const dspw_desc& d) {
   return DSPW_OK;
 }
 
+// stages per time step (enflo/src/fv.cc:1268-1310)
+int stages_of(int time_scheme) {
+  return time_scheme == DSPW_RK1 ? 1 : (time_scheme == DSPW_SSPRK3 ? 3 : 4);
+}
+
 ProbDev make_prob(const dspw_desc& d, long long off) {
   ProbDev P;
   memset(&P, 0, sizeof(P));
@@ -223,7 +229,7 @@ ProbDev make_prob(const dspw_desc& d, long long off) {
   P.dim = problem_dim(d);
   P.is_scalar = d.model <= DSPW_BURGERS;
   P.nv = P.is_scalar ? 1 : P.dim + 2;
-  P.nrk = d.time_scheme == DSPW_RK1 ? 1 : 3;
+  P.nrk = stages_of(d.time_scheme);
   P.nx = d.nx; P.ny = d.ny; P.nz = d.nz;
   for (int f = 0; f < 6; f++) P.bc[f] = d.bc[f];
   P.ec1 = d.ec1_fix;
@@ -343,11 +349,15 @@ SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
   a.prob = h->dprob;
   a.st = h->dst;
   a.nprob = h->nprob;
-  // SSPRK3 ping-pong: U^n -> Ua -> Ub -> U^n (the last stage writes in place:
-  // every cell reads its own U^n entry before overwriting it)
+  // stage buffers: SSPRK3 U^n -> Ua -> Ub -> U^n, the four-stage schemes
+  // U^n -> Ua -> Ub -> Ua -> U^n (the last stage writes in place: every cell
+  // reads its own U^n entry before overwriting it, and no sweep of that stage
+  // reads U^n); RK1 U^n -> Ua, copied back after the stage
+  static const int in4[4] = {0, 1, 2, 1}, out4[4] = {1, 2, 1, 0};
   int in, out;
   if (h->nrk == 1) { in = 0; out = 1; }
-  else { in = rk == 0 ? 0 : (rk == 1 ? 1 : 2); out = rk == 0 ? 1 : (rk == 1 ? 2 : 0); }
+  else if (h->nrk == 3) { in = rk == 0 ? 0 : (rk == 1 ? 1 : 2); out = rk == 0 ? 1 : (rk == 1 ? 2 : 0); }
+  else { in = in4[rk]; out = out4[rk]; }
   if (residual_only) { in = 0; out = 1; }
   a.Uin = (const T*)buf(h, in);
   a.Un = (const T*)h->Un;
@@ -355,10 +365,12 @@ SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
   a.R = (T*)h->R;
   a.ctot = h->ctot;
   a.rk = rk;
+  a.scheme = h->time_scheme;
+  a.R2 = (T*)h->R2;
   static const double ark[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};   // enflo/src/ext_constants.h:7-8
   static const double brk[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
-  a.a_rk = ark[rk];
-  a.b_rk = brk[rk];
+  a.a_rk = rk < 3 ? ark[rk] : 0.0;
+  a.b_rk = rk < 3 ? brk[rk] : 0.0;
   a.final_stage = (rk == h->nrk - 1) && !residual_only;
   a.residual_only = residual_only;
   a.status = h->dstatus;
@@ -569,7 +581,7 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
   h->nprob = nprob;
   h->precision = descs[0].precision;
   h->time_scheme = descs[0].time_scheme;
-  h->nrk = h->time_scheme == DSPW_RK1 ? 1 : 3;
+  h->nrk = stages_of(h->time_scheme);
   h->elem = h->precision == DSPW_FP64 ? 8 : 4;
   h->desc.assign(descs, descs + nprob);
   long long off = 0;
@@ -642,6 +654,7 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
     CKC(cudaMalloc(&h->Ua, state_bytes));
     CKC(cudaMalloc(&h->Ub, state_bytes));
     CKC(cudaMalloc(&h->R, state_bytes));
+    if (h->time_scheme == DSPW_RK4) CKC(cudaMalloc(&h->R2, state_bytes));
     if (h->has_ns) {
       CKC(cudaMalloc(&h->V, state_bytes));
       CKC(cudaMalloc(&h->node, state_bytes * 3));
@@ -685,7 +698,7 @@ int dspw_destroy(dspw_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
   void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive,
-                  h->Un, h->Ua, h->Ub, h->R, h->V, h->node, h->dstage, h->dscratch};
+                  h->Un, h->Ua, h->Ub, h->R, h->R2, h->V, h->node, h->dstage, h->dscratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (SweepClass& c : h->classes) {

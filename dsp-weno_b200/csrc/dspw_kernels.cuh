@@ -104,7 +104,9 @@ struct SweepArgs {
   T* R;                    // residual accumulator (non-final sweeps)
   long long ctot;
   int rk;
-  double a_rk, b_rk;
+  int scheme;              // enum dspw_time
+  double a_rk, b_rk;       // SSPRK3 / RK1 stage coefficients
+  T* R2;                   // classic RK4: weighted sum of the stage residuals
   int final_stage;         // 1: this stage produces U^(n+1)
   int residual_only;       // 1: write R in every sweep, never update
   int viscous;             // 1: the NS viscous kernel performs the update
@@ -853,17 +855,55 @@ __device__ inline void euler_stage_cells(const SweepArgs<T>& A, const ProbDev& P
 // (un): U = b U + (a U^n + R (-factor b)) (enflo/src/fv.cc:1163-1175), stored to
 // Uout, with the CFL speed / entropy / health epilogue on the stage that yields
 // U^(n+1).
+// stage coefficients of the four-stage schemes (enflo/src/ext_constants.h:9-10)
+DSPW_HD double jameson_coef(int rk) { return rk == 0 ? 1.0 / 4.0 : (rk == 1 ? 1.0 / 3.0 : (rk == 2 ? 1.0 / 2.0 : 1.0)); }
+DSPW_HD double rk4_coef(int rk) { return (rk == 1 || rk == 2) ? 1.0 / 2.0 : 1.0; }
+
+// stage update of one cell of a system (u holds the stage input on entry):
+// SSPRK3 / RK1  U = b U + (a U^n + R (-factor b))        enflo/src/fv.cc:1163-1175
+// Jameson RK4   U = U^n + R (-factor alpha_k)             enflo/src/fv.cc:1176-1184
+// classic RK4   R2 += R / c_k; U = U^n + R (-factor c_(k+1)),
+//               last stage U = U^n + R2 (-factor / 6)     enflo/src/fv.cc:1185-1197
+// (R2 starts every step at zero: stage 0 does not read it)
+template <typename T>
+__device__ inline void stage_combine(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
+                                     const T R[5], T u[5], const T un[5]) {
+  if (A.scheme == DSPW_JAMESON_RK4) {
+    const T c = T(-S.factor * jameson_coef(A.rk));
+#pragma unroll
+    for (int v = 0; v < 5; v++) u[v] = un[v] * T(1.0) + R[v] * c;
+  } else if (A.scheme == DSPW_RK4) {
+    T r2[5] = {T(0), T(0), T(0), T(0), T(0)};
+    if (A.rk > 0) load_cons<T>(A.R2, A.ctot, cell, P.nv, P.dim, r2);
+    const T inv = T(1.0 / rk4_coef(A.rk));
+#pragma unroll
+    for (int v = 0; v < 5; v++) r2[v] += R[v] * inv;
+    if (A.rk < 3) {
+      store_cons<T>(A.R2, A.ctot, cell, P.nv, r2);
+      const T c = T(-S.factor * rk4_coef(A.rk + 1));
+#pragma unroll
+      for (int v = 0; v < 5; v++) u[v] = un[v] * T(1.0) + R[v] * c;
+    } else {
+      const T c = T(-S.factor / 6.0);
+#pragma unroll
+      for (int v = 0; v < 5; v++) u[v] = un[v] * T(1.0) + r2[v] * c;
+    }
+  } else {
+    const T a = T(A.a_rk), b = T(A.b_rk);
+    const T c2 = T(-S.factor * A.b_rk);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      u[v] *= b;
+      u[v] += un[v] * a + R[v] * c2;
+    }
+  }
+}
+
 template <typename T>
 __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
                                          const T R[5], T u[5], const T un[5], double& smax, double& ent,
                                          unsigned& bad_fin, unsigned& bad_pos) {
-  const T a = T(A.a_rk), b = T(A.b_rk);
-  const T c2 = T(-S.factor * A.b_rk);
-#pragma unroll
-  for (int v = 0; v < 5; v++) {
-    u[v] *= b;
-    u[v] += un[v] * a + R[v] * c2;
-  }
+  stage_combine<T>(A, P, S, cell, R, u, un);
   store_cons<T>(A.Uout, A.ctot, cell, P.nv, u);
   if (A.final_stage) {
     T p[5];
@@ -908,8 +948,21 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
   if (P.is_scalar) {
     u[0] = A.Uin[cell];
     un[0] = A.Un[cell];
-    T x = u[0] * b;
-    x = x + (un[0] * a - T(S.factor * A.b_rk) * R[0]);
+    T x;
+    if (A.scheme == DSPW_JAMESON_RK4) {   // enflo_scalar/src_scalar/fv.cc:477-486
+      x = un[0] - T(S.factor * jameson_coef(A.rk)) * R[0];
+    } else if (A.scheme == DSPW_RK4) {    // enflo_scalar/src_scalar/fv.cc:487-499
+      T r2 = (A.rk > 0 ? A.R2[cell] : T(0)) + R[0] / T(rk4_coef(A.rk));
+      if (A.rk < 3) {
+        A.R2[cell] = r2;
+        x = un[0] - T(S.factor * rk4_coef(A.rk + 1)) * R[0];
+      } else {
+        x = un[0] - (T(S.factor) * r2) / T(6.0);
+      }
+    } else {
+      x = u[0] * b;
+      x = x + (un[0] * a - T(S.factor * A.b_rk) * R[0]);
+    }
     A.Uout[cell] = x;
     if (A.final_stage) {
       T pp[5] = {x, T(0), T(0), T(0), T(0)};
@@ -1724,12 +1777,7 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
     T u[5], un[5];
     load_cons<T>(A.Uin, A.ctot, g, P.nv, P.dim, u);
     load_cons<T>(A.Un, A.ctot, g, P.nv, P.dim, un);
-    const T a = T(A.a_rk), b = T(A.b_rk), c2 = T(-S.factor * A.b_rk);
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-      u[v] *= b;
-      u[v] += un[v] * a + R[v] * c2;
-    }
+    stage_combine<T>(A, P, S, g, R, u, un);
     store_cons<T>(A.Uout, A.ctot, g, P.nv, u);
     if (A.final_stage) {
       T p[5];

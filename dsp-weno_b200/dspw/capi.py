@@ -30,7 +30,7 @@ FLUX = {
 RECON = {"sp_weno": 0, "sp_wenoc": 1, "sp_weno_corr2": 2, "sp_weno_dl": 3,
          "first": 4, "second": 5, "minmod": 6, "minabs": 7, "eno2": 8}
 BC = {"periodic": 0, "dirichlet": 1, "neumann": 2, "wall": 3}
-TIME = {"rk1": 0, "ssprk3": 1}
+TIME = {"rk1": 0, "ssprk3": 1, "jameson_rk4": 2, "rk4": 3}
 MU = {"constant": 0, "sutherland": 1, "power": 2}
 PRECISION = {"fp64": 0, "fp32_bf16": 1}
 

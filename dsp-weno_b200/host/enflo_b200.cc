@@ -128,6 +128,8 @@ Level make_level(const Param& P, int rl, const std::string& precision) {
   d.recon = recon_enum(P.reconstruct);
   if (P.time_scheme == "ssprk3") d.time_scheme = DSPW_SSPRK3;
   else if (P.time_scheme == "rk1") d.time_scheme = DSPW_RK1;
+  else if (P.time_scheme == "jameson_rk4") d.time_scheme = DSPW_JAMESON_RK4;
+  else if (P.time_scheme == "rk4") d.time_scheme = DSPW_RK4;
   else throw Fail("time scheme not supported by the GPU path: " + P.time_scheme);
   d.precision = precision == "fp32_bf16" ? DSPW_FP32_BF16 : DSPW_FP64;
   d.nx = P.nx[rl];

@@ -72,7 +72,7 @@ enum dspw_recon {
  * means: ghost cells hold the fixed primitive state desc.bc_state[face]. */
 enum dspw_bc { DSPW_BC_PERIODIC = 0, DSPW_BC_DIRICHLET = 1, DSPW_BC_NEUMANN = 2, DSPW_BC_WALL = 3 };
 
-enum dspw_time { DSPW_RK1 = 0, DSPW_SSPRK3 = 1 };
+enum dspw_time { DSPW_RK1 = 0, DSPW_SSPRK3 = 1, DSPW_JAMESON_RK4 = 2, DSPW_RK4 = 3 };
 enum dspw_mu { DSPW_MU_CONSTANT = 0, DSPW_MU_SUTHERLAND = 1, DSPW_MU_POWER = 2 };
 
 /* arithmetic of the stage path */
@@ -169,7 +169,9 @@ DSPW_API int dspw_compute_dt(dspw_handle* h, int p, double* dt);
 DSPW_API int dspw_residual(dspw_handle* h, int p, double* res);
 
 /* One time-integration stage rk with step dt on every problem (dt <= 0 keeps
- * the per-problem dt of the current step). */
+ * the per-problem dt of the current step); rk runs 0..0 for rk1, 0..2 for
+ * ssprk3 and 0..3 for jameson_rk4 / rk4, the stages of FV::run's loop
+ * (enflo/src/fv.cc:1268-1310), which a caller issues in order. */
 DSPW_API int dspw_stage(dspw_handle* h, int rk, double dt);
 
 /* Up to nsteps steps of the FV::run loop body on every unfinished problem:

@@ -19,6 +19,8 @@
 
 static const double ARK[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};   /* enflo/src/ext_constants.h:7 */
 static const double BRK[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};   /* enflo/src/ext_constants.h:8 */
+static const double JRK[4] = {1.0 / 4.0, 1.0 / 3.0, 1.0 / 2.0, 1.0};   /* jameson_rks, :9 */
+static const double RK4C[4] = {1.0, 1.0 / 2.0, 1.0 / 2.0, 1.0};        /* rk4_rks, :10 */
 
 struct or_state {
   dspw_desc d;
@@ -27,6 +29,7 @@ struct or_state {
   double dx, dy, dz;
   double *P, *V;                /* padded primitive / entropy variables, 5 per cell */
   double *U, *Uold, *R;         /* interior conserved, 5 per cell (scalar: 1 used) */
+  double* R2;                   /* classic RK4: weighted sum of the stage residuals */
   double time, dt, t_interval, t_save;
   int iter;
 };
@@ -620,6 +623,7 @@ or_state* or_create(const dspw_desc* d) {
   s->V = (double*)calloc(np * 5, sizeof(double));
   s->U = (double*)calloc(nc * 5, sizeof(double));
   s->Uold = (double*)calloc(nc * 5, sizeof(double));
+  s->R2 = (double*)calloc(nc * 5, sizeof(double));
   s->R = (double*)calloc(nc * 5, sizeof(double));
   s->t_interval = d->final_time / (d->t_stamps > 0 ? d->t_stamps : 1);
   s->t_save = s->t_interval;
@@ -628,7 +632,7 @@ or_state* or_create(const dspw_desc* d) {
 
 void or_destroy(or_state* s) {
   if (!s) return;
-  free(s->P); free(s->V); free(s->U); free(s->Uold); free(s->R);
+  free(s->P); free(s->V); free(s->U); free(s->Uold); free(s->R); free(s->R2);
   free(s);
 }
 
@@ -1119,8 +1123,36 @@ void or_residual(or_state* s, int rk, double* res) {
  * enflo_scalar/src_scalar/fv.cc:463-476 (scalar) */
 static void update(or_state* s, int rk) {
   double factor = s->dt / (s->dx * s->dy * s->dz);
-  double a = ARK[rk], b = BRK[rk];
   size_t nc = (size_t)s->nx * s->ny * s->nz;
+  const int ts = s->d.time_scheme;
+  if (ts == DSPW_JAMESON_RK4) {   /* fv.cc:1176-1184, scalar fv.cc:477-486 */
+    for (size_t c = 0; c < nc; c++)
+      for (int v = 0; v < (s->scalar ? 1 : 5); v++) {
+        double* u = s->U + 5 * c + v;
+        if (s->scalar) *u = (s->Uold[5 * c] - factor * JRK[rk] * s->R[5 * c]);
+        else *u = s->Uold[5 * c + v] * 1.0 + s->R[5 * c + v] * (-factor * JRK[rk]);
+      }
+    return;
+  }
+  if (ts == DSPW_RK4) {           /* fv.cc:1185-1197, scalar fv.cc:487-499 */
+    for (size_t c = 0; c < nc; c++)
+      for (int v = 0; v < (s->scalar ? 1 : 5); v++) {
+        double* u = s->U + 5 * c + v;
+        double* r2 = s->R2 + 5 * c + v;
+        const double Rv = s->R[5 * c + v], old = s->Uold[5 * c + v];
+        if (s->scalar) {
+          *r2 += (Rv / RK4C[rk]);
+          if (rk < 3) *u = (old - factor * RK4C[rk + 1] * Rv);
+          else *u = (old - factor * *r2 / 6.0);
+        } else {
+          *r2 += Rv * (1.0 / RK4C[rk]);
+          if (rk < 3) *u = old * 1.0 + Rv * (-factor * RK4C[rk + 1]);
+          else *u = old * 1.0 + *r2 * (-factor / 6.0);
+        }
+      }
+    return;
+  }
+  double a = ARK[rk], b = BRK[rk];
   if (s->scalar) {
     for (size_t c = 0; c < nc; c++) {
       double* u = s->U + 5 * c;
@@ -1149,9 +1181,11 @@ static void scalar_to_P(or_state* s) {
 int or_step(or_state* s, int nsteps, double fixed_dt) {
   int taken = 0;
   size_t nc = (size_t)s->nx * s->ny * s->nz;
-  int nrk = s->d.time_scheme == DSPW_RK1 ? 1 : 3;
+  const int ts = s->d.time_scheme;
+  int nrk = ts == DSPW_RK1 ? 1 : (ts == DSPW_SSPRK3 ? 3 : 4);
   while (taken < nsteps && s->time < s->d.final_time && s->iter < s->d.max_iter) {
     memcpy(s->Uold, s->U, sizeof(double) * 5 * nc);
+    if (ts == DSPW_RK4) memset(s->R2, 0, sizeof(double) * 5 * nc);   /* fv.cc:1268-1275 */
     if (fixed_dt > 0) s->dt = fixed_dt; else or_compute_dt(s);
     if (s->time + s->dt > s->t_save) s->dt = s->t_save - s->time;
     for (int rk = 0; rk < nrk; ++rk) {

@@ -138,6 +138,10 @@ HX int refS_step(void* hp, int nsteps, double fixed_dt) {
     f->solution_old = f->solution;
     if (fixed_dt > 0) f->dt = fixed_dt; else f->compute_dt();
     if (f->time + f->dt > h->t_soln_save) f->dt = h->t_soln_save - f->time;
+    if (f->param.time_scheme == rk4)   // enflo_scalar/src_scalar/fv.cc:560-566
+      for (int i = 0; i < f->Nx_cell; ++i)
+        for (int j = 0; j < f->Ny_cell; ++j)
+          for (int k = 0; k < f->Nz_cell; ++k) f->residual2[i][j][k] = 0.0;
     for (int rk = 0; rk < f->param.n_rks; ++rk) {
       f->compute_residual(rk);
       f->update_solution(rk);

@@ -181,7 +181,7 @@ HX double refE_compute_dt(void* hp) {
 
 // Advance up to `nsteps` steps with the loop body of FV::run
 // (enflo/src/fv.cc:1262-1313): CFL dt, clipping to the next time stamp, three
-// SSPRK3 stages.  If fixed_dt > 0 the CFL step is replaced by that value (the
+// Runge-Kutta stages (the classic RK4 accumulator zeroed first).  If fixed_dt > 0 the CFL step is replaced by that value (the
 // clipping still applies).  Returns the number of steps taken.
 HX int refE_step(void* hp, int nsteps, double fixed_dt) {
   Quiet q;
@@ -192,6 +192,10 @@ HX int refE_step(void* hp, int nsteps, double fixed_dt) {
     f->conserved_old = f->conserved;
     if (fixed_dt > 0) f->dt = fixed_dt; else f->compute_dt();
     if (f->time + f->dt > h->t_soln_save) f->dt = h->t_soln_save - f->time;
+    if (f->param.time_scheme == rk4)   // enflo/src/fv.cc:1268-1275
+      for (int i = 0; i < f->Nx_cell; ++i)
+        for (int j = 0; j < f->Ny_cell; ++j)
+          for (int k = 0; k < f->Nz_cell; ++k) f->residual2[i][j][k].zero();
     for (int rk = 0; rk < f->param.n_rks; ++rk) {
       f->prim_to_ent();
       f->compute_residual(rk);

@@ -36,6 +36,7 @@ def desc_from_cfg(cfg: dict, nx: int, ny: int, nz: int, **over):
         gamma=float(cfg.get("gamma", 1.4)), gas_const=float(cfg.get("gas_const", 1.0)),
         prandtl=float(cfg.get("prandtl", 1.0)), mu_ref=float(cfg.get("mu_ref", 0.0)),
         lin_vel=tuple(cfg.get("vel", (1.0, 0.0, 0.0))), network=net(),
+        time_scheme=cfg.get("time_scheme", "ssprk3"),
     )
     kw.update(over)
     return make_desc(**kw)

@@ -301,6 +301,14 @@ def run_cases():
     cases.append(("tgv_ns_kep_tecno", "E", euler_cfg("kepes_tecno4_roe", "sp_weno_dl", model="ns_kep", x=(0, "2*pi"),
                   y=(0, "2*pi"), z=(0, "2*pi"), Nx=8, Ny=8, Nz=8, ic=TGV_IC, dim=3, constants={"M": 0.1},
                   mu_ref=1 / 1600, prandtl=0.71, final_time=10.0), 3, 0.0))
+    for ts in ("jameson_rk4", "rk4"):
+        cases.append((f"shuosher_{ts}", "E", euler_cfg("kepes_tecno4_roe", "sp_wenoc", x=(-5, 5), Nx=100, cfl=0.4,
+                      final_time=1.8, ic=SHU_IC, bc=bc1d, time_stamps=5, time_scheme=ts), 20, 0.0))
+        cases.append((f"kh_{ts}", "E", euler_cfg("kepes_tecno4_roe", "sp_weno_dl", Nx=16, Ny=16, ic=KH_IC, dim=2,
+                      time_scheme=ts), 6, 0.0))
+        cases.append((f"burgers_{ts}", "S", dict(model="burgers", x=("-pi", "pi"), Nx=80, Ny=2, Nz=2, cfl=0.4,
+                      final_time=0.5, reconstruct="sp_weno", net_file=NET, flux="bur_tecno4", ic="0.5+sin(x)",
+                      bc="periodic", time_stamps=5, time_scheme=ts), 30, 0.0))
     cases.append(("tgv_ns_fixed", "E", euler_cfg("kepes_tecno4_roe", "sp_weno", model="ns_es", x=(0, "2*pi"),
                   y=(0, "2*pi"), z=(0, "2*pi"), Nx=6, Ny=6, Nz=6, ic=TGV_IC, dim=3, constants={"M": 0.3},
                   mu_ref=0.05, prandtl=0.71, final_time=10.0), 3, 0.01))
