@@ -851,10 +851,6 @@ __device__ inline void euler_stage_cells(const SweepArgs<T>& A, const ProbDev& P
   __syncwarp();
 }
 
-// SSPRK stage update of one Euler cell from its residual R, U^(k) (u) and U^n
-// (un): U = b U + (a U^n + R (-factor b)) (enflo/src/fv.cc:1163-1175), stored to
-// Uout, with the CFL speed / entropy / health epilogue on the stage that yields
-// U^(n+1).
 // stage coefficients of the four-stage schemes (enflo/src/ext_constants.h:9-10)
 DSPW_HD double jameson_coef(int rk) { return rk == 0 ? 1.0 / 4.0 : (rk == 1 ? 1.0 / 3.0 : (rk == 2 ? 1.0 / 2.0 : 1.0)); }
 DSPW_HD double rk4_coef(int rk) { return (rk == 1 || rk == 2) ? 1.0 / 2.0 : 1.0; }
@@ -899,6 +895,9 @@ __device__ inline void stage_combine(const SweepArgs<T>& A, const ProbDev& P, co
   }
 }
 
+// stage update of one Euler cell from its residual R, U^(k) (u) and U^n (un),
+// stored to Uout, with the CFL speed / entropy / health epilogue on the stage
+// that yields U^(n+1).
 template <typename T>
 __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
                                          const T R[5], T u[5], const T un[5], double& smax, double& ent,

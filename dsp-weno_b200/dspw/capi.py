@@ -33,6 +33,10 @@ BC = {"periodic": 0, "dirichlet": 1, "neumann": 2, "wall": 3}
 TIME = {"rk1": 0, "ssprk3": 1, "jameson_rk4": 2, "rk4": 3}
 MU = {"constant": 0, "sutherland": 1, "power": 2}
 PRECISION = {"fp64": 0, "fp32_bf16": 1}
+# columns of a per-step diagnostics row (enum dspw_diag_col)
+DIAG_NAMES = ("iter", "time", "total_entropy", "ke", "ke_diss_pr", "ke_diss_stress", "enstrophy",
+              "res_mass", "res_mom_x", "res_mom_y", "res_mom_z", "res_energy")
+DIAG_COLS = len(DIAG_NAMES)
 
 STATUS = {0: "DSPW_OK", 1: "DSPW_ERR_ARG", 2: "DSPW_ERR_CUDA", 3: "DSPW_ERR_NONFINITE",
           4: "DSPW_ERR_NONPOSITIVE", 5: "DSPW_ERR_TIMEOUT", 6: "DSPW_ERR_UNSUPPORTED",

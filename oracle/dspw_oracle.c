@@ -30,6 +30,8 @@ struct or_state {
   double *P, *V;                /* padded primitive / entropy variables, 5 per cell */
   double *U, *Uold, *R;         /* interior conserved, 5 per cell (scalar: 1 used) */
   double* R2;                   /* classic RK4: weighted sum of the stage residuals */
+  double ke_diss_pr;            /* -sum(|u|^2/2 R_mass + u.R_mom) of the last inviscid residual */
+  double ke_diss_stress;        /* viscous-stress KE dissipation of the last viscous residual */
   double time, dt, t_interval, t_save;
   int iter;
 };
@@ -921,6 +923,16 @@ static void inviscid_residual(or_state* s) {
     /* the reference visits faces direction by direction with the other two
      * indices outermost in (i,j,k) order; per cell the sum order is the same */
   }
+  /* KE dissipation of the inviscid residual, enflo/src/fv.cc:756-764 */
+  s->ke_diss_pr = 0.0;
+  if (s->scalar) return;
+  for (int i = 0; i < s->nx; ++i)
+    for (int j = 0; j < s->ny; ++j)
+      for (int k = 0; k < s->nz; ++k) {
+        const double* P = s->P + 5 * pidx(s, i + NG, j + NG, k + NG);
+        const double* R = s->R + 5 * cidx(s, i, j, k);
+        s->ke_diss_pr -= 0.5 * sq3(P + 1) * R[0] + dot3(P + 1, R + 1);
+      }
 }
 
 /* nodal_vlux_ES, enflo/src/vflux_ES.cc:15-151, node (i,j,k) at (i+1/2, j+1/2,
@@ -993,15 +1005,11 @@ static void nodal_flux_es(or_state* s, int i, int j, int k, double* xf, double* 
  * 1/4/dx of the temperature derivatives) and Temperature (enflo/src/fv.cc:1329-1332). */
 static double temp_of(const or_state* s, const double* P) { return P[4] / (s->d.gas_const * P[0]); }
 
-static void nodal_flux_ke(or_state* s, int i, int j, int k, double* xf, double* yf, double* zf) {
-  const dspw_desc* d = &s->d;
+/* velocity derivatives at node (i,j,k) (i in -1..Nx-1) from the 8 cells around
+ * it, nodal_avg_and_vel_derivatives, enflo/src/nodal_avg_and_der.cc:37-81:
+ * Tx[c] = d(u_c)/dx, Ty, Tz likewise */
+static void node_vel_derivatives(const or_state* s, int i, int j, int k, double* Tx, double* Ty, double* Tz) {
 #define PP(a, b, c) (s->P + 5 * pidx(s, NG + i + (a), NG + j + (b), NG + k + (c)))
-  const double f1 = 1.0 / 8.0;
-  double avg[5], Tx[3], Ty[3], Tz[3];
-  for (int c = 0; c < 5; c++) {
-    avg[c] = PP(1, 1, 1)[c] * f1 + PP(0, 1, 1)[c] * f1 + PP(1, 0, 1)[c] * f1 + PP(1, 1, 0)[c] * f1;
-    avg[c] += PP(0, 0, 1)[c] * f1 + PP(0, 1, 0)[c] * f1 + PP(1, 0, 0)[c] * f1 + PP(0, 0, 0)[c] * f1;
-  }
   const double vx = 1.0 / (4.0 * s->dx), vy = 1.0 / (4.0 * s->dy), vz = 1.0 / (4.0 * s->dz);
   for (int c = 0; c < 3; c++) {
     const int v = 1 + c;
@@ -1012,6 +1020,19 @@ static void nodal_flux_ke(or_state* s, int i, int j, int k, double* xf, double* 
     Tz[c] = PP(1, 1, 1)[v] * vz + PP(1, 0, 1)[v] * vz + PP(0, 1, 1)[v] * vz + PP(0, 0, 1)[v] * vz;
     Tz[c] += PP(1, 1, 0)[v] * -vz + PP(1, 0, 0)[v] * -vz + PP(0, 1, 0)[v] * -vz + PP(0, 0, 0)[v] * -vz;
   }
+#undef PP
+}
+
+static void nodal_flux_ke(or_state* s, int i, int j, int k, double* xf, double* yf, double* zf) {
+  const dspw_desc* d = &s->d;
+#define PP(a, b, c) (s->P + 5 * pidx(s, NG + i + (a), NG + j + (b), NG + k + (c)))
+  const double f1 = 1.0 / 8.0;
+  double avg[5], Tx[3], Ty[3], Tz[3];
+  for (int c = 0; c < 5; c++) {
+    avg[c] = PP(1, 1, 1)[c] * f1 + PP(0, 1, 1)[c] * f1 + PP(1, 0, 1)[c] * f1 + PP(1, 1, 0)[c] * f1;
+    avg[c] += PP(0, 0, 1)[c] * f1 + PP(0, 1, 0)[c] * f1 + PP(1, 0, 0)[c] * f1 + PP(0, 0, 0)[c] * f1;
+  }
+  node_vel_derivatives(s, i, j, k, Tx, Ty, Tz);
   const double T_avg = avg[4] / (d->gas_const * avg[0]);
   const double mu = viscosity(d, T_avg);
   const double Cp = d->gamma * d->gas_const / (d->gamma - 1.0);
@@ -1042,13 +1063,36 @@ static void nodal_flux_ke(or_state* s, int i, int j, int k, double* xf, double* 
   for (int c = 0; c < 5; c++) { xf[c] *= ax; yf[c] *= ay; zf[c] *= az; }
 }
 
+/* node weight of find_node_weights, enflo/src/find_node_weights.cc:19-66:
+ * halved on each periodic domain face the node lies on; (a,b,c) in 0..N */
+static double node_weight(const or_state* s, int a, int b, int c) {
+  double w = 1.0;
+  const int* bc = s->d.bc;
+  if (a == 0 && bc[0] == DSPW_BC_PERIODIC) w /= 2.0;
+  if (a == s->nx && bc[1] == DSPW_BC_PERIODIC) w /= 2.0;
+  if (b == 0 && bc[2] == DSPW_BC_PERIODIC) w /= 2.0;
+  if (b == s->ny && bc[3] == DSPW_BC_PERIODIC) w /= 2.0;
+  if (c == 0 && bc[4] == DSPW_BC_PERIODIC) w /= 2.0;
+  if (c == s->nz && bc[5] == DSPW_BC_PERIODIC) w /= 2.0;
+  return w;
+}
+
 /* scatter one node's fluxes into its interior cells with weights +-1/4
- * (nodal_vlux, enflo/src/fv.cc:773-780: ES for ns_es, KE otherwise) */
-static void scatter_node(or_state* s, int i, int j, int k) {
+ * (nodal_vlux, enflo/src/fv.cc:773-780: ES for ns_es, KE otherwise), and add
+ * the node's viscous-stress KE dissipation -(Tx.F_x dx + Ty.F_y dy + Tz.F_z dz) w
+ * (enflo/src/fv.cc:810-814).  The derivatives and the weight are those of node
+ * (ti,tj,tk), which is (i,j,k) except at two corners (viscous_residual). */
+static void scatter_node_at(or_state* s, int i, int j, int k, int ti, int tj, int tk) {
   const int Nx = s->nx, Ny = s->ny, Nz = s->nz;
   double xf[5], yf[5], zf[5];
   if (s->d.model == DSPW_NS_ES) nodal_flux_es(s, i, j, k, xf, yf, zf);
   else nodal_flux_ke(s, i, j, k, xf, yf, zf);
+  {
+    double Tx[3], Ty[3], Tz[3];
+    const double wt = node_weight(s, ti + 1, tj + 1, tk + 1);
+    node_vel_derivatives(s, ti, tj, tk, Tx, Ty, Tz);
+    s->ke_diss_stress -= (dot3(Tx, xf + 1) * s->dx + dot3(Ty, yf + 1) * s->dy + dot3(Tz, zf + 1) * s->dz) * wt;
+  }
   for (int l = 0; l < 2; ++l)
     for (int m = 0; m < 2; ++m)
       for (int n = 0; n < 2; ++n) {
@@ -1060,6 +1104,8 @@ static void scatter_node(or_state* s, int i, int j, int k) {
       }
 }
 
+static void scatter_node(or_state* s, int i, int j, int k) { scatter_node_at(s, i, j, k, i, j, k); }
+
 /* compute_visc_residual, enflo/src/fv.cc:786-1157.  Nodes are visited in the
  * reference's order: interior nodes, then for each domain face (x-right,
  * x-left, y-right, y-left, z-right, z-left) its face nodes and two families of
@@ -1069,6 +1115,7 @@ static void scatter_node(or_state* s, int i, int j, int k) {
  * restatement keeps that. */
 static void viscous_residual(or_state* s) {
   const int X = s->nx - 1, Y = s->ny - 1, Z = s->nz - 1;
+  s->ke_diss_stress = 0.0;
   for (int i = 0; i < X; i++)
     for (int j = 0; j < Y; j++)
       for (int k = 0; k < Z; k++) scatter_node(s, i, j, k);
@@ -1103,8 +1150,13 @@ static void viscous_residual(or_state* s) {
   scatter_node(s, -1, -1, Z);
   scatter_node(s, X, Y, -1);
   scatter_node(s, X, -1, Z);
-  scatter_node(s, -1, Y, Z);
-  scatter_node(s, X, Y, Z);
+  /* the corners (0,N,N) and (N,N,N) take their derivatives and weight at
+   * j = Nz-1 in place of Ny-1 (:1141-1150); the same node when Ny == Nz.  With
+   * Nz > Ny that index lies outside the reference's node arrays; the corner's
+   * own node is used then. */
+  const int Yq = s->nz <= s->ny ? Z : Y;
+  scatter_node_at(s, -1, Y, Z, -1, Yq, Z);
+  scatter_node_at(s, X, Y, Z, X, Yq, Z);
 }
 
 void or_residual(or_state* s, int rk, double* res) {
@@ -1176,9 +1228,80 @@ static void scalar_to_P(or_state* s) {
   apply_bc(s);
 }
 
+/* Enstrophy of compute_global (enflo/src/compute_global.cc:33-65) from the
+ * node vorticity of find_vorticity (enflo/src/find_vort.cc:18-28), nodes
+ * (i,j,k) in 0..N, ghost cells included */
+static double enstrophy(const or_state* s) {
+  const double f1 = 1.0 / 8.0;
+  double ens = 0.0;
+  for (int i = 0; i < s->nx + 1; ++i)
+    for (int j = 0; j < s->ny + 1; ++j)
+      for (int k = 0; k < s->nz + 1; ++k) {
+#define RHO(a, b, c) s->P[5 * pidx(s, NG + i + (a), NG + j + (b), NG + k + (c))]
+        double den = f1 * (RHO(-1, -1, -1) + RHO(0, -1, -1) + RHO(-1, 0, -1) + RHO(-1, -1, 0) + RHO(0, 0, -1) +
+                           RHO(0, -1, 0) + RHO(-1, 0, 0) + RHO(0, 0, 0));
+#undef RHO
+        double Tx[3], Ty[3], Tz[3], w[3];
+        node_vel_derivatives(s, i - 1, j - 1, k - 1, Tx, Ty, Tz);
+        w[0] = Ty[2] - Tz[1];
+        w[1] = Tz[0] - Tx[2];
+        w[2] = Tx[1] - Ty[0];
+        ens += den * sq3(w) * node_weight(s, i, j, k);
+      }
+  const dspw_desc* d = &s->d;
+  double nodal_volume = (d->xmax - d->xmin) / (s->nx + 1) * (d->ymax - d->ymin) / (s->ny + 1) *
+                        (d->zmax - d->zmin) / (s->nz + 1);
+  return ens * (0.5 * nodal_volume);
+}
+
+/* compute_global's cell sums, enflo/src/compute_global.cc:18-28,58-64 and
+ * enflo_scalar/src_scalar/compute_global.cc:12-21 */
+static void cell_globals(const or_state* s, double* total_ent, double* ke) {
+  double ent = 0.0, k_e = 0.0;
+  for (int i = 0; i < s->nx; ++i)
+    for (int j = 0; j < s->ny; ++j)
+      for (int k = 0; k < s->nz; ++k) {
+        const double* P = s->P + 5 * pidx(s, i + NG, j + NG, k + NG);
+        if (s->scalar) {
+          ent += 0.5 * pow(P[0], 2);
+        } else {
+          double sv = log(P[4]) - s->d.gamma * log(P[0]);
+          ent += -P[0] * sv / (s->d.gamma - 1.0);
+          k_e += P[0] * sq3(P + 1);
+        }
+      }
+  double cell_volume = s->dx * s->dy * s->dz;
+  *total_ent = ent * cell_volume;
+  *ke = k_e * (0.5 * cell_volume);
+}
+
+/* compute_residual_norm, enflo/src/fv.cc:1204-1226 (per component, scaled by
+ * the cell volume) and enflo_scalar/src_scalar/fv.cc:505-517 */
+static void residual_norm(const or_state* s, double* out) {
+  double r[5] = {0, 0, 0, 0, 0};
+  for (int i = 0; i < s->nx; ++i)
+    for (int j = 0; j < s->ny; ++j)
+      for (int k = 0; k < s->nz; ++k) {
+        const double* R = s->R + 5 * cidx(s, i, j, k);
+        if (s->scalar) r[0] += pow(R[0], 2);
+        else
+          for (int v = 0; v < 5; v++) r[v] += pow(R[v] / s->dx / s->dy / s->dz, 2);
+      }
+  for (int v = 0; v < 5; v++) out[v] = sqrt(r[v]);
+  if (!s->scalar)
+    for (int v = 0; v < 5; v++) out[v] *= (s->dx * s->dy * s->dz);
+}
+
+int or_step(or_state* s, int nsteps, double fixed_dt) { return or_step_diag(s, nsteps, fixed_dt, NULL); }
+
 /* loop body of FV::run, enflo/src/fv.cc:1262-1313 and
- * enflo_scalar/src_scalar/fv.cc:553-597 */
-int or_step(or_state* s, int nsteps, double fixed_dt) {
+ * enflo_scalar/src_scalar/fv.cc:553-597.  or_step_diag also records, per step, the row of global diagnostics FV::run
+ * computes (OR_DIAG_COLS doubles: iter, time, total entropy, KE, KE_diss_pr,
+ * KE_diss_stress, enstrophy, residual norm per component).  Systems: the
+ * values of compute_global at stage 0 (fv.cc:1280-1281), i.e. of U^n at t^n,
+ * and the residual norm of the step's last stage.  Scalar: compute_global
+ * after the step (enflo_scalar/src_scalar/fv.cc:573-576), i.e. t^(n+1). */
+int or_step_diag(or_state* s, int nsteps, double fixed_dt, double* rows) {
   int taken = 0;
   size_t nc = (size_t)s->nx * s->ny * s->nz;
   const int ts = s->d.time_scheme;
@@ -1188,14 +1311,33 @@ int or_step(or_state* s, int nsteps, double fixed_dt) {
     if (ts == DSPW_RK4) memset(s->R2, 0, sizeof(double) * 5 * nc);   /* fv.cc:1268-1275 */
     if (fixed_dt > 0) s->dt = fixed_dt; else or_compute_dt(s);
     if (s->time + s->dt > s->t_save) s->dt = s->t_save - s->time;
+    double* row = rows ? rows + (size_t)OR_DIAG_COLS * taken : NULL;
+    if (row) memset(row, 0, sizeof(double) * OR_DIAG_COLS);
     for (int rk = 0; rk < nrk; ++rk) {
       or_residual(s, rk, NULL);
+      if (row && rk == 0 && !s->scalar) {
+        row[0] = s->iter;
+        row[1] = s->time;
+        cell_globals(s, &row[2], &row[3]);
+        row[4] = s->ke_diss_pr;
+        row[5] = (s->d.model == DSPW_NS_ES || s->d.model == DSPW_NS_KEP) ? s->ke_diss_stress : 0.0;
+        row[6] = enstrophy(s);
+      }
       update(s, rk);
       if (s->scalar) scalar_to_P(s);
       else con_to_prim(s);
     }
     s->time += s->dt;
     ++s->iter;
+    if (row) {
+      residual_norm(s, row + 7);
+      if (s->scalar) {
+        double ke;
+        row[0] = s->iter;
+        row[1] = s->time;
+        cell_globals(s, &row[2], &ke);
+      }
+    }
     if (s->time == s->t_save) s->t_save += s->t_interval;
     ++taken;
   }

@@ -30,6 +30,8 @@ double or_compute_dt(or_state* s);
 void or_residual(or_state* s, int rk, double* res);
 /* loop body of FV::run; fixed_dt > 0 replaces the CFL step.  Returns steps taken. */
 int or_step(or_state* s, int nsteps, double fixed_dt);
+#define OR_DIAG_COLS 12
+int or_step_diag(or_state* s, int nsteps, double fixed_dt, double* rows);
 void or_time(const or_state* s, double* t, int* iter, double* dt);
 /* total entropy and conserved totals (dspw_globals_out semantics) */
 void or_globals(or_state* s, double* total_entropy, double* conserved5, double* ke);

@@ -21,7 +21,7 @@ import numpy as np
 ORACLE_DIR = Path(__file__).resolve().parent
 REPO = ORACLE_DIR.parent
 sys.path.insert(0, str(REPO / "dsp-weno_b200"))
-from dspw.capi import Desc, nvar  # noqa: E402
+from dspw.capi import DIAG_COLS, Desc, nvar  # noqa: E402
 from dspw.paramfile import write_param  # noqa: E402
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -50,6 +50,7 @@ def oracle_lib():
             "or_compute_dt": (D, [P]),
             "or_residual": (None, [P, I, _dp]),
             "or_step": (I, [P, I, D]),
+            "or_step_diag": (I, [P, I, D, _dp]),
             "or_time": (None, [P, C.POINTER(D), C.POINTER(I), C.POINTER(D)]),
             "or_globals": (None, [P, C.POINTER(D), _dp, C.POINTER(D)]),
             "or_logavg": (D, [D, D]),
@@ -108,6 +109,12 @@ class Oracle:
 
     def step(self, n=1, fixed_dt=0.0):
         return self.L.or_step(self.h, int(n), float(fixed_dt))
+
+    def step_diag(self, n=1, fixed_dt=0.0):
+        """Steps with the per-step diagnostics rows (DIAG_COLS columns each)."""
+        rows = np.zeros((int(n), DIAG_COLS))
+        k = self.L.or_step_diag(self.h, int(n), float(fixed_dt), rows)
+        return rows[:k]
 
     def time(self):
         t, i, dt = C.c_double(), C.c_int(), C.c_double()
@@ -180,6 +187,7 @@ def _ref_lib(kind):
             "refE_get_prim": (None, [P, _dp]), "refE_get_cons": (None, [P, _dp]),
             "refE_set_prim": (None, [P, _dp]), "refE_residual": (None, [P, I, _dp]),
             "refE_compute_dt": (D, [P]), "refE_step": (I, [P, I, D]),
+            "refE_step_diag": (I, [P, I, D, _dp]),
             "refE_face_flux": (None, [P, _dp, I, _dp, _dp]),
             "refE_reconstruct": (None, [P, _dp, _dp, _dp]),
             "refE_nn_forward": (None, [P, _dp, C.POINTER(D), C.POINTER(D)]),
@@ -193,6 +201,7 @@ def _ref_lib(kind):
             "refS_get": (None, [P, _dp]), "refS_set": (None, [P, _dp]),
             "refS_residual": (None, [P, I, _dp]), "refS_compute_dt": (D, [P]),
             "refS_step": (I, [P, I, D]), "refS_run_errors": (None, [P, _dp]),
+            "refS_step_diag": (I, [P, I, D, _dp]),
             "refS_face_flux": (D, [P, _dp, I]),
             "refS_reconstruct": (None, [P, _dp, C.POINTER(D), C.POINTER(D)]),
             "refS_sp_weno": (None, [_dp, I, C.POINTER(D), C.POINTER(D)]),
@@ -262,6 +271,11 @@ class RefEuler(_RefBase):
     def step(self, n=1, fixed_dt=0.0):
         return self.L.refE_step(self.h, int(n), float(fixed_dt))
 
+    def step_diag(self, n=1, fixed_dt=0.0):
+        rows = np.zeros((int(n), DIAG_COLS))
+        k = self.L.refE_step_diag(self.h, int(n), float(fixed_dt), rows)
+        return rows[:k]
+
     def face_flux(self, P4, direction):
         V, F = np.zeros(20), np.zeros(5)
         self.L.refE_face_flux(self.h, np.ascontiguousarray(P4, dtype=np.float64).reshape(20), direction, V, F)
@@ -309,6 +323,11 @@ class RefScalar(_RefBase):
 
     def step(self, n=1, fixed_dt=0.0):
         return self.L.refS_step(self.h, int(n), float(fixed_dt))
+
+    def step_diag(self, n=1, fixed_dt=0.0):
+        rows = np.zeros((int(n), DIAG_COLS))
+        k = self.L.refS_step_diag(self.h, int(n), float(fixed_dt), rows)
+        return rows[:k]
 
     def run_errors(self):
         e = np.zeros(3); self.L.refS_run_errors(self.h, e); return e

@@ -129,12 +129,14 @@ HX double refS_compute_dt(void* hp) {
 }
 
 // Loop body of FV::run (enflo_scalar/src_scalar/fv.cc:553-597) without output.
-HX int refS_step(void* hp, int nsteps, double fixed_dt) {
-  Quiet q;
-  Handle* h = (Handle*)hp;
+// With `rows`, each step also records 12 doubles: iter, time and total_ent of
+// compute_global after the step (:573-576), zeros in the systems-only columns
+// 3-6, the residual norm of compute_residual_norm in column 7, zeros after it.
+static int step_impl(Handle* h, int nsteps, double fixed_dt, double* rows) {
   FV* f = h->fv;
   int taken = 0;
   while (taken < nsteps && f->time < f->param.final_time && f->iter < f->param.max_iter) {
+    double* row = rows ? rows + 12 * (size_t)taken : nullptr;
     f->solution_old = f->solution;
     if (fixed_dt > 0) f->dt = fixed_dt; else f->compute_dt();
     if (f->time + f->dt > h->t_soln_save) f->dt = h->t_soln_save - f->time;
@@ -149,10 +151,29 @@ HX int refS_step(void* hp, int nsteps, double fixed_dt) {
     }
     f->time += f->dt;
     ++f->iter;
+    if (row) {
+      f->compute_residual_norm();
+      f->compute_global();
+      for (int c = 0; c < 12; c++) row[c] = 0.0;
+      row[0] = f->iter;
+      row[1] = f->time;
+      row[2] = f->total_ent;
+      row[7] = f->res_norm;
+    }
     if (f->time == h->t_soln_save) h->t_soln_save += h->t_interval;
     ++taken;
   }
   return taken;
+}
+
+HX int refS_step(void* hp, int nsteps, double fixed_dt) {
+  Quiet q;
+  return step_impl((Handle*)hp, nsteps, fixed_dt, nullptr);
+}
+
+HX int refS_step_diag(void* hp, int nsteps, double fixed_dt, double* rows) {
+  Quiet q;
+  return step_impl((Handle*)hp, nsteps, fixed_dt, rows);
 }
 
 // Run every remaining step of the current mesh level and return the L1, L2 and

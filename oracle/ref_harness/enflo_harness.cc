@@ -180,15 +180,20 @@ HX double refE_compute_dt(void* hp) {
 }
 
 // Advance up to `nsteps` steps with the loop body of FV::run
-// (enflo/src/fv.cc:1262-1313): CFL dt, clipping to the next time stamp, three
+// (enflo/src/fv.cc:1262-1313): CFL dt, clipping to the next time stamp, the
 // Runge-Kutta stages (the classic RK4 accumulator zeroed first).  If fixed_dt > 0 the CFL step is replaced by that value (the
 // clipping still applies).  Returns the number of steps taken.
-HX int refE_step(void* hp, int nsteps, double fixed_dt) {
-  Quiet q;
-  Handle* h = (Handle*)hp;
+// With `rows`, each step also records the reference's own per-step
+// diagnostics, 12 doubles: iter, time, total_ent, KE, KE_diss_pr,
+// KE_diss_stress (0 for Euler), Enstrophy from compute_global at stage 0
+// (fv.cc:1280-1281, with find_vorticity as FV::run calls it, :1244,1307), and
+// the five components of compute_residual_norm after the step (:1286).
+static int step_impl(Handle* h, int nsteps, double fixed_dt, double* rows) {
   FV* f = h->fv;
   int taken = 0;
   while (taken < nsteps && f->time < f->param.final_time && f->iter < f->param.max_iter) {
+    double* row = rows ? rows + 12 * (size_t)taken : nullptr;
+    if (row) f->find_vorticity();
     f->conserved_old = f->conserved;
     if (fixed_dt > 0) f->dt = fixed_dt; else f->compute_dt();
     if (f->time + f->dt > h->t_soln_save) f->dt = h->t_soln_save - f->time;
@@ -199,15 +204,44 @@ HX int refE_step(void* hp, int nsteps, double fixed_dt) {
     for (int rk = 0; rk < f->param.n_rks; ++rk) {
       f->prim_to_ent();
       f->compute_residual(rk);
+      if (row && rk == 0) {
+        f->compute_global();
+        const bool ns = f->param.model == ns_es || f->param.model == ns_kep;
+        row[0] = f->iter;
+        row[1] = f->time;
+        row[2] = f->total_ent;
+        row[3] = f->KE;
+        row[4] = f->KE_diss_pr;
+        row[5] = ns ? f->KE_diss_stress : 0.0;
+        row[6] = f->Enstrophy;
+      }
       f->update_solution(rk);
       f->con_to_prim();
     }
     f->time += f->dt;
     ++f->iter;
+    if (row) {
+      f->compute_residual_norm();
+      row[7] = f->res_norm.mass_flux;
+      row[8] = f->res_norm.momentum_flux.x;
+      row[9] = f->res_norm.momentum_flux.y;
+      row[10] = f->res_norm.momentum_flux.z;
+      row[11] = f->res_norm.energy_flux;
+    }
     if (f->time == h->t_soln_save) h->t_soln_save += h->t_interval;
     ++taken;
   }
   return taken;
+}
+
+HX int refE_step(void* hp, int nsteps, double fixed_dt) {
+  Quiet q;
+  return step_impl((Handle*)hp, nsteps, fixed_dt, nullptr);
+}
+
+HX int refE_step_diag(void* hp, int nsteps, double fixed_dt, double* rows) {
+  Quiet q;
+  return step_impl((Handle*)hp, nsteps, fixed_dt, rows);
 }
 
 // One face flux num_flux(P, V, n) (enflo/src/num_flux.cc:12-72) for a 4-cell

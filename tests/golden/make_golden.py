@@ -331,6 +331,25 @@ def gen_runs():
     np.savez_compressed(OUT / "runs.npz", **out)
 
 
+DIAG_CASES = ("linadv_sp_weno", "burgers_wenoc", "burgers_wall_dl", "shuosher_sp_weno", "shuosher_jameson_rk4",
+              "kh_sp_weno", "kh_sp_weno_dl", "kh_rk4", "wall2d", "neumann2d", "vortex", "euler3d", "tgv_ns",
+              "tgv_ns_kep", "tgv_ns_kep_tecno")
+DIAG_STEPS = 6
+
+
+def gen_diag():
+    """Per-step diagnostics rows of the reference (compute_global,
+    compute_residual_norm, find_vorticity) for the first steps of some runs."""
+    out = {}
+    for name, kind, cfg, nsteps, fixed_dt in run_cases():
+        if name not in DIAG_CASES:
+            continue
+        R = O.RefEuler(cfg) if kind == "E" else O.RefScalar(cfg)
+        out[f"{name}|rows"] = R.step_diag(min(nsteps, DIAG_STEPS), fixed_dt)
+        print(f"  diag {name}: {out[name + '|rows'].shape[0]} rows")
+    np.savez_compressed(OUT / "diag.npz", **out)
+
+
 def gen_ooc():
     out = {}
     for recon in ("sp_weno", "sp_wenoc", "sp_weno_dl"):
@@ -356,6 +375,7 @@ def main():
     gen_runs()
     gen_ooc()
     gen_faces_simple(np.random.default_rng(20240612))
+    gen_diag()
 
 
 if __name__ == "__main__":

@@ -99,6 +99,34 @@ def test_run_golden(case):
     _close(o.cons(), g[f"{name}|final"])
 
 
+DIAG = [c for c in run_cases() if f"{c[0]}|rows" in load("diag.npz")]
+
+
+@pytest.mark.parametrize("case", DIAG, ids=lambda c: c[0])
+def test_step_diagnostics_golden(case):
+    """Per-step rows of total entropy, KE, KE dissipation (pressure and stress
+    parts), enstrophy and residual norms: the oracle against the reference's
+    compute_global / compute_residual_norm / find_vorticity."""
+    name, kind, cfg, nsteps, fixed_dt = case
+    g = load("runs.npz")
+    ref = load("diag.npz")[f"{name}|rows"]
+    p0 = g[f"{name}|prim0"]
+    _, nz, ny, nx = p0.shape
+    o = O.Oracle(desc_from_cfg(cfg, nx, ny, nz))
+    o.set_prim(p0)
+    got = o.step_diag(len(ref), fixed_dt)
+    assert got.shape == ref.shape
+    for c in range(ref.shape[1]):
+        _close(got[:, c], ref[:, c])
+    # the columns carry real values: time advances, the state has entropy, and
+    # systems have KE and a residual
+    assert np.all(np.diff(ref[:, 1]) > 0) and np.all(ref[:, 2] != 0) and np.all(ref[:, 7] > 0)
+    if kind == "E":
+        assert np.all(ref[:, 3] > 0)
+    if cfg.get("model") in ("ns_es", "ns_kep"):
+        assert np.all(ref[:, 5] != 0) and np.all(ref[:, 6] > 0)
+
+
 def test_ooc_known_answers():
     """Config-1 L1 errors equal the values the reference prints (l1_err.dat)
     and the survey measured: 1.75268e-05 (sp_weno), 1.74048e-05 (sp_wenoc),
