@@ -129,6 +129,16 @@ struct dspw_handle {
   void* Ub = nullptr;
   void* R = nullptr;
   void* R2 = nullptr;                  // classic RK4 only
+  // per-step diagnostics (dspw_diag_enable): accumulators, the row ring
+  // (slot-major, diag_cap slots of nprob rows) and the rows drained to the host
+  int diag_cap = 0;
+  DiagAcc* ddiag = nullptr;
+  double* drows = nullptr;
+  long long* dnode_start = nullptr;
+  long long nodes_tot = 0;
+  std::vector<unsigned long long> diag_taken;   // rows of each problem moved to the host so far
+  std::vector<long long> diag_dropped;
+  std::vector<std::vector<double>> diag_host;
   void* V = nullptr;
   void* node = nullptr;
   double* dstage = nullptr;
@@ -241,6 +251,7 @@ ProbDev make_prob(const dspw_desc& d, long long off) {
   P.dz = (d.zmax - d.zmin) / d.nz;
   P.hmin = std::min(P.dx, std::min(P.dy, P.dz));
   P.vol = P.dx * P.dy * P.dz;
+  P.node_vol = (d.xmax - d.xmin) / (d.nx + 1) * (d.ymax - d.ymin) / (d.ny + 1) * (d.zmax - d.zmin) / (d.nz + 1);
   P.area[0] = P.dy * P.dz;           // num_flux face areas (enflo/src/kepec.cc:38-44)
   P.area[1] = P.dx * P.dz;
   P.area[2] = P.dx * P.dy;
@@ -341,6 +352,65 @@ void* buf(dspw_handle* h, int which) {
   }
 }
 
+template <typename T>
+DiagArgs<T> diag_args(dspw_handle* h, const long long* start, const T* U) {
+  DiagArgs<T> d;
+  memset(&d, 0, sizeof(d));
+  d.prob = h->dprob;
+  d.st = h->dst;
+  d.acc = h->ddiag;
+  d.nprob = h->nprob;
+  d.start = start;
+  d.U = U;
+  d.R = (const T*)h->R;
+  d.node = (const T*)h->node;
+  d.ctot = h->ctot;
+  d.rows = h->drows;
+  d.cap = h->diag_cap;
+  return d;
+}
+
+// Move the rows written since the last drain from the device ring into the
+// per-problem host lists.  Rows of a problem beyond the ring's capacity since
+// the last drain were overwritten and are counted as dropped.
+int drain_diag(dspw_handle* h) {
+  if (h->diag_cap == 0) return DSPW_OK;
+  const int np = h->nprob;
+  std::vector<DiagAcc> acc(np);
+  CK(cudaMemcpyAsync(acc.data(), h->ddiag, sizeof(DiagAcc) * np, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  unsigned long long lo = ~0ull, hi = 0;
+  for (int p = 0; p < np; p++) {
+    unsigned long long from = h->diag_taken[p], to = acc[p].count;
+    if (to - from > (unsigned long long)h->diag_cap) {
+      h->diag_dropped[p] += (long long)(to - from - h->diag_cap);
+      from = to - h->diag_cap;
+      h->diag_taken[p] = from;
+    }
+    if (to > from) { lo = std::min(lo, from); hi = std::max(hi, to); }
+  }
+  if (hi == 0) return DSPW_OK;
+  // slots lo .. hi-1 (at most diag_cap of them), in one or two contiguous runs
+  const size_t row_bytes = sizeof(double) * DIAG_COLS * np;
+  const unsigned long long n = hi - lo, cap = h->diag_cap;
+  std::vector<double> buf((size_t)n * DIAG_COLS * np);
+  const unsigned long long s0 = lo % cap, first = std::min(n, cap - s0);
+  CK(cudaMemcpyAsync(buf.data(), h->drows + s0 * DIAG_COLS * np, first * row_bytes, cudaMemcpyDeviceToHost,
+                     h->stream));
+  if (n > first)
+    CK(cudaMemcpyAsync(buf.data() + first * DIAG_COLS * np, h->drows, (n - first) * row_bytes,
+                       cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int p = 0; p < np; p++) {
+    for (unsigned long long r = h->diag_taken[p]; r < acc[p].count; r++) {
+      const double* row = buf.data() + ((r - lo) * np + p) * DIAG_COLS;
+      h->diag_host[p].insert(h->diag_host[p].end(), row, row + DIAG_COLS);
+    }
+    h->diag_taken[p] = acc[p].count;
+  }
+  return DSPW_OK;
+}
+
 // sweep arguments of stage rk (residual_only: write R in every sweep)
 template <typename T>
 SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
@@ -373,6 +443,7 @@ SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
   a.b_rk = rk < 3 ? brk[rk] : 0.0;
   a.final_stage = (rk == h->nrk - 1) && !residual_only;
   a.residual_only = residual_only;
+  a.store_R = h->diag_cap > 0 && !residual_only && (rk == 0 || rk == h->nrk - 1);
   a.status = h->dstatus;
   a.net = h->dnet;
   a.collect_buf = residual_only ? h->collect_buf : nullptr;
@@ -420,12 +491,30 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
       prof_mark(h, name.c_str());
     }
   }
+  const bool diag = h->diag_cap > 0 && !residual_only;
+  if (diag && rk == 0) {
+    // U^n is intact during stage 0 (it writes Ua); R holds its inviscid residual
+    DiagArgs<T> da = diag_args<T>(h, h->dcell_start, (const T*)h->Un);
+    CK(Launch<T>::diag_cells(da, 0, h->ctot, h->stream));
+    if (h->nodes_tot > 0) {
+      da.start = h->dnode_start;
+      CK(Launch<T>::diag_nodes(da, h->nodes_tot, h->stream));
+    }
+    prof_mark(h, "diag_stage0");
+  }
   if (h->has_ns) {
     CK(Launch<T>::visc_update(a, h->dcell_start, h->ctot, (const T*)h->node, h->stream));
     prof_mark(h, "visc_update");
   }
   if (h->nrk == 1 && !residual_only)
     CK(cudaMemcpyAsync(h->Un, h->Ua, h->elem * h->ctot * 5, cudaMemcpyDeviceToDevice, h->stream));
+  if (diag && rk == h->nrk - 1) {
+    // U^(n+1) is in U^n's buffer; R holds the last stage's residual
+    DiagArgs<T> da = diag_args<T>(h, h->dcell_start, (const T*)h->Un);
+    CK(Launch<T>::diag_cells(da, 1, h->ctot, h->stream));
+    CK(Launch<T>::diag_row(da, h->stream));
+    prof_mark(h, "diag_row");
+  }
   return DSPW_OK;
 }
 
@@ -698,7 +787,8 @@ int dspw_destroy(dspw_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
   void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive,
-                  h->Un, h->Ua, h->Ub, h->R, h->R2, h->V, h->node, h->dstage, h->dscratch};
+                  h->Un, h->Ua, h->Ub, h->R, h->R2, h->V, h->node, h->dstage, h->dscratch,
+                  h->ddiag, h->drows, h->dnode_start};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (SweepClass& c : h->classes) {
@@ -799,9 +889,13 @@ int dspw_step(dspw_handle* h, int nsteps, double fixed_dt) {
   if (!h || nsteps < 0) return DSPW_ERR_ARG;
   int r = build_graph(h, fixed_dt > 0 ? fixed_dt : 0.0);
   if (r) return r;
-  for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(h->graph, h->stream));
+  for (int s = 0; s < nsteps; s++) {
+    CK(cudaGraphLaunch(h->graph, h->stream));
+    // keep the diagnostics ring from wrapping
+    if (h->diag_cap > 0 && (s + 1) % h->diag_cap == 0) { r = drain_diag(h); if (r) return r; }
+  }
   CK(cudaStreamSynchronize(h->stream));
-  return DSPW_OK;
+  return drain_diag(h);
 }
 
 int dspw_run(dspw_handle* h, int chunk, int* steps) {
@@ -814,7 +908,12 @@ int dspw_run(dspw_handle* h, int chunk, int* steps) {
   long long total = 0;
   int status = DSPW_OK;
   for (;;) {
-    for (int s = 0; s < chunk; s++) CK(cudaGraphLaunch(h->graph, h->stream));
+    for (int s = 0; s < chunk; s++) {
+      CK(cudaGraphLaunch(h->graph, h->stream));
+      if (h->diag_cap > 0 && (s + 1) % h->diag_cap == 0) { r = drain_diag(h); if (r) return r; }
+    }
+    r = drain_diag(h);
+    if (r) return r;
     total += chunk;
     int nact = 0;
     StatusDev sd;
@@ -854,6 +953,68 @@ int dspw_globals(dspw_handle* h, int p, dspw_globals_out* g) {
   g->total_entropy = acc[0] * P.vol;
   g->kinetic_energy = acc[1] * P.vol;
   for (int v = 0; v < 5; v++) g->conserved[v] = acc[2 + v] * P.vol;
+  return DSPW_OK;
+}
+
+int dspw_diag_enable(dspw_handle* h, int capacity) {
+  if (!h || capacity < 0) return DSPW_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // the step graph changes
+  if (h->ddiag) cudaFree(h->ddiag);
+  if (h->drows) cudaFree(h->drows);
+  if (h->dnode_start) cudaFree(h->dnode_start);
+  h->ddiag = nullptr; h->drows = nullptr; h->dnode_start = nullptr;
+  h->diag_cap = 0;
+  h->nodes_tot = 0;
+  h->diag_taken.assign(h->nprob, 0);
+  h->diag_dropped.assign(h->nprob, 0);
+  h->diag_host.assign(h->nprob, std::vector<double>());
+  if (capacity == 0) return DSPW_OK;
+  // node prefix: (Nx+1)(Ny+1)(Nz+1) nodes per system, none for scalar problems
+  std::vector<long long> ns(h->nprob + 1, 0);
+  for (int p = 0; p < h->nprob; p++) {
+    const ProbDev& P = h->hprob[p];
+    ns[p + 1] = ns[p] + (P.is_scalar ? 0 : (long long)(P.nx + 1) * (P.ny + 1) * (P.nz + 1));
+  }
+  const size_t ring = sizeof(double) * DIAG_COLS * (size_t)h->nprob * (size_t)capacity;
+  if (cudaMalloc(&h->ddiag, sizeof(DiagAcc) * h->nprob) != cudaSuccess ||
+      cudaMalloc(&h->drows, ring) != cudaSuccess ||
+      cudaMalloc(&h->dnode_start, sizeof(long long) * (h->nprob + 1)) != cudaSuccess) {
+    if (h->ddiag) cudaFree(h->ddiag);
+    if (h->drows) cudaFree(h->drows);
+    if (h->dnode_start) cudaFree(h->dnode_start);
+    h->ddiag = nullptr; h->drows = nullptr; h->dnode_start = nullptr;
+    h->last_error = DSPW_ERR_CUDA;
+    return DSPW_ERR_CUDA;
+  }
+  CK(cudaMemset(h->ddiag, 0, sizeof(DiagAcc) * h->nprob));
+  CK(cudaMemset(h->drows, 0, ring));
+  CK(cudaMemcpy(h->dnode_start, ns.data(), sizeof(long long) * (h->nprob + 1), cudaMemcpyHostToDevice));
+  h->nodes_tot = ns[h->nprob];
+  h->diag_cap = capacity;
+  return DSPW_OK;
+}
+
+int dspw_diag_pending(dspw_handle* h, int p, int* nrows, long long* ndropped) {
+  if (check_p(h, p) || !nrows) return DSPW_ERR_ARG;
+  int r = drain_diag(h);
+  if (r) return r;
+  *nrows = h->diag_cap ? (int)(h->diag_host[p].size() / DIAG_COLS) : 0;
+  if (ndropped) *ndropped = h->diag_cap ? h->diag_dropped[p] : 0;
+  return DSPW_OK;
+}
+
+int dspw_diag_read(dspw_handle* h, int p, double* rows, int max_rows, int* nread) {
+  if (check_p(h, p) || !nread || max_rows < 0 || (max_rows > 0 && !rows)) return DSPW_ERR_ARG;
+  int r = drain_diag(h);
+  if (r) return r;
+  *nread = 0;
+  if (h->diag_cap == 0) return DSPW_OK;
+  std::vector<double>& q = h->diag_host[p];
+  const int n = std::min<int>(max_rows, (int)(q.size() / DIAG_COLS));
+  memcpy(rows, q.data(), sizeof(double) * DIAG_COLS * n);
+  q.erase(q.begin(), q.begin() + (size_t)n * DIAG_COLS);
+  *nread = n;
   return DSPW_OK;
 }
 

@@ -49,6 +49,7 @@ struct ProbDev {
   int spw_corr;       // SP-WENO correction type, -1 for the network
   long long off;      // first cell
   double dx, dy, dz, hmin, vol;
+  double node_vol;    // (xmax-xmin)/(Nx+1) * (ymax-ymin)/(Ny+1) * (zmax-zmin)/(Nz+1) (compute_global.cc:59-61)
   double area[3], rarea[3];
   double gamma, gas_const, prandtl, mu_ref, T_ref, T_0, omega, Cp;
   double lin_vel[3], lin_speed, lin_vn[3];
@@ -109,6 +110,7 @@ struct SweepArgs {
   T* R2;                   // classic RK4: weighted sum of the stage residuals
   int final_stage;         // 1: this stage produces U^(n+1)
   int residual_only;       // 1: write R in every sweep, never update
+  int store_R;             // 1: the updating sweep also stores the stage residual (diagnostics)
   int viscous;             // 1: the NS viscous kernel performs the update
   StatusDev* status;
   const NetParams* net;
@@ -904,6 +906,7 @@ __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P
                                          unsigned& bad_fin, unsigned& bad_pos) {
   stage_combine<T>(A, P, S, cell, R, u, un);
   store_cons<T>(A.Uout, A.ctot, cell, P.nv, u);
+  if (A.store_R) store_cons<T>(A.R, A.ctot, cell, P.nv, R);
   if (A.final_stage) {
     T p[5];
     cons_to_prim<T>(u, T(P.gamma), p);
@@ -963,6 +966,7 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
       x = x + (un[0] * a - T(S.factor * A.b_rk) * R[0]);
     }
     A.Uout[cell] = x;
+    if (A.store_R) A.R[cell] = R[0];
     if (A.final_stage) {
       T pp[5] = {x, T(0), T(0), T(0), T(0)};
       double sp = wave_speed<T>(P, pp);
@@ -1778,6 +1782,7 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
     load_cons<T>(A.Un, A.ctot, g, P.nv, P.dim, un);
     stage_combine<T>(A, P, S, g, R, u, un);
     store_cons<T>(A.Uout, A.ctot, g, P.nv, u);
+    if (A.store_R && A.final_stage) store_cons<T>(A.R, A.ctot, g, P.nv, R);
     if (A.final_stage) {
       T p[5];
       cons_to_prim<T>(u, T(P.gamma), p);

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "dspw_kernels.cuh"
+#include "dspw_diag.cuh"
 
 namespace dspw {
 
@@ -32,6 +33,11 @@ struct Launch {
                                  double* r, unsigned long long* acts, cudaStream_t s);
   static cudaError_t visc_update(const SweepArgs<T>& a, const long long* cell_start, long long ncell_total,
                                  const T* node, cudaStream_t s);
+  // per-step diagnostics: cell sums (mode 0 at stage 0, mode 1 after the last
+  // stage) over `total` cells, node sums over `total` nodes, the row kernel
+  static cudaError_t diag_cells(const DiagArgs<T>& a, int mode, long long total, cudaStream_t s);
+  static cudaError_t diag_nodes(const DiagArgs<T>& a, long long total, cudaStream_t s);
+  static cudaError_t diag_row(const DiagArgs<T>& a, cudaStream_t s);
 };
 
 cudaError_t launch_begin_step(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive,

@@ -228,6 +228,9 @@ def lib():
         "dspw_globals_noalloc": (I, [C.POINTER(Desc), P, LL, I, P, P]),
         "dspw_profile_step": (I, [P, dp, C.c_char_p, I, C.POINTER(I)]),
         "dspw_tune": (I, [P, I, C.POINTER(D), C.POINTER(D)]),
+        "dspw_diag_enable": (I, [P, I]),
+        "dspw_diag_pending": (I, [P, I, C.POINTER(I), C.POINTER(LL)]),
+        "dspw_diag_read": (I, [P, I, dp, I, C.POINTER(I)]),
         "dspw_stream": (P, [P]),
         "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),
         "dspw_trainer_create": (I, [C.POINTER(TrainCfg), dp, dp, C.POINTER(P)]),
@@ -397,6 +400,20 @@ class Solver:
         s = C.c_int()
         check(lib().dspw_run(self.h, int(chunk), C.byref(s)), "dspw_run")
         return s.value
+
+    def diag_enable(self, capacity=256):
+        """Record the per-step diagnostics rows (dspw_diag_enable); 0 stops."""
+        check(lib().dspw_diag_enable(self.h, int(capacity)), "dspw_diag_enable")
+
+    def diag_rows(self, p=0):
+        """Pending per-step rows of problem p as an (n, DIAG_COLS) array (read
+        and removed), and the count of rows dropped so far."""
+        n, dropped = C.c_int(), C.c_longlong()
+        check(lib().dspw_diag_pending(self.h, p, C.byref(n), C.byref(dropped)), "dspw_diag_pending")
+        rows = np.zeros((n.value, DIAG_COLS))
+        got = C.c_int()
+        check(lib().dspw_diag_read(self.h, p, rows, n.value, C.byref(got)), "dspw_diag_read")
+        return rows[:got.value], dropped.value
 
     def globals(self, p=0):
         g = Globals()

@@ -236,6 +236,41 @@ DSPW_API int dspw_reconstruct_batch(const dspw_desc* desc, const double* u4, lon
 DSPW_API int dspw_globals_noalloc(const dspw_desc* desc, const void* d_cons, long long stride, int elem_bytes,
                                   double* d_out, void* stream);
 
+/* ---- per-step diagnostics ----------------------------------------------
+ * The global quantities FV::run computes every step, evaluated on the device
+ * inside the step graph and kept in a device ring of `capacity` rows per
+ * problem, which dspw_step / dspw_run drain to host memory as they go
+ * (replaces compute_global, compute_residual_norm and find_vorticity,
+ * enflo/src/compute_global.cc:10-89, enflo/src/fv.cc:1204-1226,
+ * enflo/src/find_vort.cc:9-29, enflo_scalar/src_scalar/compute_global.cc:10-39,
+ * enflo_scalar/src_scalar/fv.cc:505-517).  One row per problem and step:
+ *   systems: iter, time, total entropy, KE, KE_diss_pr, KE_diss_stress (NS,
+ *     else 0), enstrophy -- the values compute_global writes at stage 0, of
+ *     U^n at t^n -- then the residual norm of the step's last stage per
+ *     component (mass, x/y/z momentum, energy);
+ *   scalar: iter and time after the step, the total entropy sum u^2/2 vol of
+ *     U^(n+1), zeros, the residual norm sqrt(sum R^2), zeros.
+ * Sums are taken in a different order than the reference's loops: they agree
+ * to rounding. */
+enum dspw_diag_col {
+  DSPW_DIAG_ITER = 0, DSPW_DIAG_TIME = 1, DSPW_DIAG_ENTROPY = 2, DSPW_DIAG_KE = 3, DSPW_DIAG_KE_DISS_PR = 4,
+  DSPW_DIAG_KE_DISS_STRESS = 5, DSPW_DIAG_ENSTROPHY = 6, DSPW_DIAG_RES = 7 /* 7..11 */, DSPW_DIAG_COLS = 12
+};
+
+/* capacity > 0: record a row every step from now on (the ring holds capacity
+ * steps between drains); 0: stop recording.  Either way pending rows are
+ * discarded.  Allocates device memory; not during stream capture. */
+DSPW_API int dspw_diag_enable(dspw_handle* h, int capacity);
+
+/* Rows of problem p recorded and not yet read; *ndropped (may be NULL) counts
+ * rows lost because more than `capacity` steps ran between drains (dspw_stage
+ * does not drain). */
+DSPW_API int dspw_diag_pending(dspw_handle* h, int p, int* nrows, long long* ndropped);
+
+/* Copy up to max_rows of problem p's oldest pending rows (DSPW_DIAG_COLS
+ * doubles each) into rows and remove them; *nread is the number copied. */
+DSPW_API int dspw_diag_read(dspw_handle* h, int p, double* rows, int max_rows, int* nread);
+
 /* Synchronise the handle's stream; returns the first error recorded. */
 DSPW_API int dspw_sync(dspw_handle* h);
 
