@@ -5,10 +5,14 @@
 // condition and exact solution (expr.h), and for every mesh level (all levels
 // when OOC_study is yes, the first otherwise, as FV::run, enflo/src/fv.cc:1231-1324)
 // runs the stage path through the C ABI (include/dspw.h).  It writes the
-// reference's SOLN_FILES_<reconstruction>/ directory: globals.dat, the final
-// solution, and for OOC studies l1_err.dat / l2_err.dat / linf_err.dat with the
-// table layout of compute_OOC (enflo_scalar/src_scalar/compute_ooc.cc:10-141).
-// Errors of systems are those of the density.
+// reference's SOLN_FILES_<reconstruction>/ directory: globals.dat with one row
+// per step in compute_global's layout (enflo/src/compute_global.cc:80-88,
+// enflo_scalar/src_scalar/compute_global.cc:34-38), from the diagnostics the
+// library records on the device, the final solution, and for OOC studies
+// l1_err.dat / l2_err.dat / linf_err.dat with the table layout of compute_OOC
+// (enflo_scalar/src_scalar/compute_ooc.cc:10-141).  Errors of systems are those
+// of the density.  Runs that are not OOC studies print the reference's per-step
+// residual line (enflo/src/fv.cc:1289-1299, enflo_scalar/src_scalar/fv.cc:578-584).
 //
 //   enflo_b200 -i param.in [--precision fp64|fp32_bf16] [--chunk K]
 //   enflo_b200 -i param.in --check          parse and print the descriptor, no GPU
@@ -113,6 +117,48 @@ struct Level {
   long long n;
   double xmin, xmax, ymin, ymax, zmin, zmax, dx, dy, dz;
 };
+
+// globals.dat rows in compute_global's layout, and the per-step residual line
+// of FV::run when `log` is set.  Systems rows hold iter / time at the start of
+// their step (compute_global runs at stage 0), scalar rows after it.
+void write_globals(std::ostream& glob, std::ostream& out, const double* rows, int n, bool scalar, bool log,
+                   double t_final, double& ent0) {
+  for (int r = 0; r < n; r++) {
+    const double* w = rows + (size_t)r * DSPW_DIAG_COLS;
+    const double t = w[DSPW_DIAG_TIME], ent = w[DSPW_DIAG_ENTROPY];
+    if (scalar) {
+      glob << t << " " << std::setprecision(10) << ent << " " << (ent - ent0) / ent0 << " " << std::endl;
+    } else {
+      if (t == 0.0) {   // compute_global.cc:69-77
+        ent0 = ent;
+        if (ent0 == 0.0) {
+          out << "WARNING: Initial total entropy is zero!! Re-setting it to 1.0" << std::endl;
+          ent0 = 1.0;
+        }
+      }
+      glob << t << " " << std::setprecision(10) << ent << " " << (ent - ent0) / std::fabs(ent0) << " "
+           << w[DSPW_DIAG_KE] << " " << w[DSPW_DIAG_KE_DISS_PR] << " " << w[DSPW_DIAG_KE_DISS_STRESS] << " "
+           << w[DSPW_DIAG_ENSTROPHY] << " " << std::endl;
+    }
+    if (!log) continue;
+    std::ios saved(nullptr);
+    saved.copyfmt(out);
+    const double* res = w + DSPW_DIAG_RES;
+    if (scalar) {
+      out << std::left << "ITER = " << std::setw(8) << (long long)w[DSPW_DIAG_ITER] << " " << std::scientific
+          << std::setprecision(4) << "TIME = " << t << " " << "RES = " << res[0] << std::endl;
+    } else {
+      // iter and time after the step; the reference prints the x-momentum
+      // norm under RES_MOM_y (fv.cc:1296)
+      const double t_after = r + 1 < n ? rows[(size_t)(r + 1) * DSPW_DIAG_COLS + DSPW_DIAG_TIME] : t_final;
+      out << std::left << "ITER = " << std::setw(8) << (long long)w[DSPW_DIAG_ITER] + 1 << " " << std::scientific
+          << std::setprecision(4) << "TIME = " << t_after << " " << "RES_MASS = " << res[0] << " "
+          << "RES_MOM_X = " << res[1] << " " << "RES_MOM_y = " << res[1] << " " << "RES_MOM_z = " << res[3] << " "
+          << "RES_ENERGY = " << res[4] << std::endl;
+    }
+    out.copyfmt(saved);
+  }
+}
 
 Level make_level(const Param& P, int rl, const std::string& precision) {
   Level L;
@@ -277,12 +323,27 @@ int main(int argc, char** argv) {
       check(dspw_create(&L.d, &h), "dspw_create");
       int rc = dspw_upload_prim(h, 0, ic.data());
       if (rc) { dspw_destroy(h); check(rc, "dspw_upload_prim"); }
+      if (rc == DSPW_OK) rc = dspw_diag_enable(h, chunk);
+      if (rc) { dspw_destroy(h); check(rc, "dspw_diag_enable"); }
+      double ent0 = 0.0;
+      if (P.scalar) {   // compute_global before the time loop (enflo_scalar/src_scalar/fv.cc:544)
+        dspw_globals_out g0;
+        rc = dspw_globals(h, 0, &g0);
+        if (rc) { dspw_destroy(h); check(rc, "dspw_globals"); }
+        ent0 = g0.total_entropy != 0.0 ? g0.total_entropy : 1.0;
+        glob << 0.0 << " " << std::setprecision(10) << g0.total_entropy << " " << (g0.total_entropy - ent0) / ent0
+             << " " << std::endl;
+      }
       int steps = 0;
       rc = dspw_run(h, chunk, &steps);
       dspw_globals_out g;
       if (rc == DSPW_OK) rc = dspw_globals(h, 0, &g);
       if (rc) { dspw_destroy(h); check(rc, "dspw_run"); }
-      glob << std::setprecision(10) << g.time << " " << g.total_entropy << " " << g.iter << "\n";
+      int nrows = 0, nread = 0;
+      check(dspw_diag_pending(h, 0, &nrows, nullptr), "dspw_diag_pending");
+      std::vector<double> rows((size_t)nrows * DSPW_DIAG_COLS);
+      check(dspw_diag_read(h, 0, rows.data(), nrows, &nread), "dspw_diag_read");
+      write_globals(glob, std::cout, rows.data(), nread, P.scalar, !P.ooc, g.time, ent0);
       std::vector<double> prim(L.nvar * L.n);
       check(dspw_download_prim(h, 0, prim.data()), "dspw_download_prim");
       if (P.ooc) {

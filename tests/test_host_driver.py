@@ -232,3 +232,51 @@ def test_ooc_study_through_driver(tmp_path, recon):
         # L1 converges at third order; L-inf is limited near the extrema of sin^4
         assert (2.5 < rate < 4.5) if col == 0 else (1.5 < rate < 4.5), (fname, rate)
     assert (soln / "globals.dat").exists()
+
+
+def _numbers(path):
+    return [[float(x) for x in line.split()] for line in path.read_text().splitlines() if line.strip()]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["kh_sp_weno", "tgv_ns", "wall2d", "burgers_wenoc"])
+def test_globals_file_matches_reference_rows(tmp_path, name):
+    """globals.dat in compute_global's layout (enflo/src/compute_global.cc:80-88,
+    enflo_scalar/src_scalar/compute_global.cc:34-38), one row per step from the
+    device diagnostics, against the reference's own rows of the same steps
+    (``diag.npz``); the file carries 10 significant digits."""
+    _need_cli()
+    ref = load("diag.npz")[f"{name}|rows"]
+    name_, kind, cfg, _, _ = next(c for c in run_cases() if c[0] == name)
+    cfg = dict(cfg)
+    cfg["max_iter"] = len(ref)
+    cfg["ooc"] = False
+    p = _write(tmp_path, cfg)
+    r = _run(["-i", p], tmp_path)
+    rows = _numbers(tmp_path / f"SOLN_FILES_{cfg['reconstruct']}" / "globals.dat")
+    if kind == "S":
+        # the state before the first step, then one row after every step
+        assert len(rows) == len(ref) + 1 and len(rows[0]) == 3 and rows[0][0] == 0.0
+        # sum u^2/2 vol of the initial state (the file's first row has 10 digits)
+        g = load("runs.npz")
+        ent0 = 0.5 * float(np.sum(g[f"{name}|prim0"] ** 2)) * float(np.prod(g[f"{name}|h"]))
+        assert abs(rows[0][1] - ent0) <= 1e-9 * abs(ent0)
+        got = np.array(rows[1:])
+        want = np.stack([ref[:, 1], ref[:, 2], (ref[:, 2] - ent0) / ent0], axis=1)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("ITER =")]
+        assert len(lines) == len(ref) and "RES = " in lines[0]
+    else:
+        assert len(rows) == len(ref) and all(len(x) == 7 for x in rows)
+        got = np.array(rows)
+        ent0 = ref[0, 2]
+        want = np.stack([ref[:, 1], ref[:, 2], (ref[:, 2] - ent0) / abs(ent0), ref[:, 3], ref[:, 4], ref[:, 5],
+                         ref[:, 6]], axis=1)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("ITER =")]
+        assert len(lines) == len(ref)
+        # ITER = n after the step and the mass residual norm of its last stage
+        f = lines[-1].split()
+        assert int(f[2]) == len(ref)
+        assert abs(float(f[8]) - ref[-1, 7]) <= 1e-3 * ref[-1, 7]
+    for c in range(got.shape[1]):
+        scale = np.max(np.abs(want[:, c]))
+        assert np.max(np.abs(got[:, c] - want[:, c])) <= 2e-9 * scale + 1e-300, (name, c, got[:, c], want[:, c])
