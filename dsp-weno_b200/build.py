@@ -64,7 +64,7 @@ def build_cli(lib: Path) -> Path:
     if CLI.exists() and all(CLI.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return CLI
     cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", f"-I{REPO / 'include'}", *map(str, srcs),
-           "-o", str(CLI), f"-L{lib.parent}", f"-l:{lib.name}", "-Wl,-rpath,$ORIGIN"]
+           "-o", str(CLI), f"-L{lib.parent}", f"-l:{lib.name}", "-Wl,-rpath,$ORIGIN", "-pthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"host driver build failed:\n{r.stderr}")

@@ -4,6 +4,7 @@
 // dspw_kernels.cuh (instantiated by dspw_fp64.cu / dspw_fp32.cu).
 #include <algorithm>
 #include <cmath>
+#include <deque>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -22,6 +23,7 @@ __global__ void k_begin_step_wrap(const ProbDev* prob, ProbState* st, int nprob,
   if (p >= nprob) return;
   const ProbDev& P = prob[p];
   ProbState& S = st[p];
+  S.snap = 0;
   if (!(S.time < P.final_time && S.iter < P.max_iter)) {
     S.active = 0;
     S.dt = 0.0;
@@ -62,7 +64,9 @@ __global__ void k_end_step(const ProbDev* prob, ProbState* st, int nprob) {
   if (!S.active) return;
   S.time += S.dt;
   S.iter += 1;
-  if (S.time == S.t_save) S.t_save += prob[p].t_interval;
+  const int stamp = S.time == S.t_save;   // output time stamp (fv.cc:1309-1313)
+  if (stamp) S.t_save += prob[p].t_interval;
+  S.snap = stamp;
   S.ent_prev = S.ent;
   S.ent = S.ent_acc * prob[p].vol;
   double rise = (S.ent - S.ent_prev) / fabs(S.ent_prev);
@@ -139,6 +143,17 @@ struct dspw_handle {
   std::vector<unsigned long long> diag_taken;   // rows of each problem moved to the host so far
   std::vector<long long> diag_dropped;
   std::vector<std::vector<double>> diag_host;
+  // snapshots at the output time stamps (dspw_snap_enable): a ring of
+  // snap_slots state-shaped buffers, per-problem counts and (time, iter), and
+  // the snapshots drained to the host as primitive planes
+  int snap_slots = 0;
+  void* dsnap = nullptr;
+  unsigned long long* dsnap_count = nullptr;
+  SnapMeta* dsnap_meta = nullptr;
+  struct HostSnap { double time; int iter; std::vector<double> prim; };
+  std::vector<unsigned long long> snap_taken;
+  std::vector<long long> snap_dropped;
+  std::vector<std::deque<HostSnap>> snap_host;
   void* V = nullptr;
   void* node = nullptr;
   double* dstage = nullptr;
@@ -157,6 +172,10 @@ struct dspw_handle {
   int last_error = 0;
   size_t elem = 8;
 };
+
+extern "C" {
+static int download(dspw_handle* h, int p, double* out, int prim, void* src);
+}
 
 namespace {
 
@@ -411,6 +430,43 @@ int drain_diag(dspw_handle* h) {
   return DSPW_OK;
 }
 
+// Move the snapshots taken since the last drain from the device ring to host
+// memory as primitive planes.  A problem with more than snap_slots new
+// snapshots lost the oldest ones (counted as dropped).
+int drain_snap(dspw_handle* h) {
+  if (h->snap_slots == 0) return DSPW_OK;
+  const int np = h->nprob;
+  std::vector<unsigned long long> count(np);
+  std::vector<SnapMeta> meta((size_t)np * h->snap_slots);
+  CK(cudaMemcpyAsync(count.data(), h->dsnap_count, sizeof(unsigned long long) * np, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaMemcpyAsync(meta.data(), h->dsnap_meta, sizeof(SnapMeta) * meta.size(), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const size_t slot_bytes = (size_t)h->elem * 5 * (size_t)h->ctot;
+  for (int p = 0; p < np; p++) {
+    unsigned long long from = h->snap_taken[p];
+    if (count[p] - from > (unsigned long long)h->snap_slots) {
+      h->snap_dropped[p] += (long long)(count[p] - from - h->snap_slots);
+      from = count[p] - h->snap_slots;
+    }
+    const dspw_desc& d = h->desc[p];
+    const size_t nvals = (size_t)(d.model <= DSPW_BURGERS ? 1 : 5) * (size_t)d.nx * d.ny * d.nz;
+    for (unsigned long long c = from; c < count[p]; c++) {
+      const unsigned long long slot = c % (unsigned long long)h->snap_slots;
+      dspw_handle::HostSnap s;
+      s.time = meta[slot * np + p].time;
+      s.iter = meta[slot * np + p].iter;
+      s.prim.resize(nvals);
+      int r = download(h, p, s.prim.data(), 1, (char*)h->dsnap + slot * slot_bytes);
+      if (r) return r;
+      h->snap_host[p].push_back(std::move(s));
+    }
+    h->snap_taken[p] = count[p];
+  }
+  return DSPW_OK;
+}
+
 // sweep arguments of stage rk (residual_only: write R in every sweep)
 template <typename T>
 SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
@@ -582,6 +638,33 @@ int enqueue_stage_any(dspw_handle* h, int rk, int residual_only) {
                                    : enqueue_stage<float>(h, rk, residual_only);
 }
 
+// end of a step: time, iteration and time-stamp bookkeeping, then the
+// snapshot of the problems that reached a stamp
+template <typename T>
+int enqueue_end_step_t(dspw_handle* h) {
+  CK(launch_end_step(h->dprob, h->dst, h->nprob, h->stream));
+  if (h->snap_slots > 0) {
+    SnapArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.prob = h->dprob;
+    a.st = h->dst;
+    a.nprob = h->nprob;
+    a.cell_start = h->dcell_start;
+    a.U = (const T*)h->Un;
+    a.slots = (T*)h->dsnap;
+    a.ctot = h->ctot;
+    a.nslots = h->snap_slots;
+    a.count = h->dsnap_count;
+    a.meta = h->dsnap_meta;
+    CK(Launch<T>::snap(a, h->ctot, h->stream));
+  }
+  return DSPW_OK;
+}
+
+int enqueue_end_step(dspw_handle* h) {
+  return h->precision == DSPW_FP64 ? enqueue_end_step_t<double>(h) : enqueue_end_step_t<float>(h);
+}
+
 int enqueue_step(dspw_handle* h, double fixed_dt) {
   CK(cudaMemsetAsync(h->dnactive, 0, sizeof(int), h->stream));
   CK(launch_begin_step(h->dprob, h->dst, h->nprob, fixed_dt, h->dnactive, h->stream));
@@ -590,7 +673,8 @@ int enqueue_step(dspw_handle* h, double fixed_dt) {
     int r = enqueue_stage_any(h, rk, 0);
     if (r) return r;
   }
-  CK(launch_end_step(h->dprob, h->dst, h->nprob, h->stream));
+  int re = enqueue_end_step(h);
+  if (re) return re;
   prof_mark(h, "end_step");
   return DSPW_OK;
 }
@@ -788,7 +872,7 @@ int dspw_destroy(dspw_handle* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive,
                   h->Un, h->Ua, h->Ub, h->R, h->R2, h->V, h->node, h->dstage, h->dscratch,
-                  h->ddiag, h->drows, h->dnode_start};
+                  h->ddiag, h->drows, h->dnode_start, h->dsnap, h->dsnap_count, h->dsnap_meta};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (SweepClass& c : h->classes) {
@@ -880,7 +964,10 @@ int dspw_stage(dspw_handle* h, int rk, double dt) {
   }
   int r = enqueue_stage_any(h, rk, 0);
   if (r) return r;
-  if (rk == h->nrk - 1) CK(launch_end_step(h->dprob, h->dst, h->nprob, h->stream));
+  if (rk == h->nrk - 1) {
+    r = enqueue_end_step(h);
+    if (r) return r;
+  }
   CK(cudaStreamSynchronize(h->stream));
   return DSPW_OK;
 }
@@ -891,11 +978,14 @@ int dspw_step(dspw_handle* h, int nsteps, double fixed_dt) {
   if (r) return r;
   for (int s = 0; s < nsteps; s++) {
     CK(cudaGraphLaunch(h->graph, h->stream));
-    // keep the diagnostics ring from wrapping
+    // keep the diagnostics and snapshot rings from wrapping
     if (h->diag_cap > 0 && (s + 1) % h->diag_cap == 0) { r = drain_diag(h); if (r) return r; }
+    if (h->snap_slots > 0 && (s + 1) % h->snap_slots == 0) { r = drain_snap(h); if (r) return r; }
   }
   CK(cudaStreamSynchronize(h->stream));
-  return drain_diag(h);
+  r = drain_diag(h);
+  if (r) return r;
+  return drain_snap(h);
 }
 
 int dspw_run(dspw_handle* h, int chunk, int* steps) {
@@ -911,8 +1001,11 @@ int dspw_run(dspw_handle* h, int chunk, int* steps) {
     for (int s = 0; s < chunk; s++) {
       CK(cudaGraphLaunch(h->graph, h->stream));
       if (h->diag_cap > 0 && (s + 1) % h->diag_cap == 0) { r = drain_diag(h); if (r) return r; }
+      if (h->snap_slots > 0 && (s + 1) % h->snap_slots == 0) { r = drain_snap(h); if (r) return r; }
     }
     r = drain_diag(h);
+    if (r) return r;
+    r = drain_snap(h);
     if (r) return r;
     total += chunk;
     int nact = 0;
@@ -1015,6 +1108,58 @@ int dspw_diag_read(dspw_handle* h, int p, double* rows, int max_rows, int* nread
   memcpy(rows, q.data(), sizeof(double) * DIAG_COLS * n);
   q.erase(q.begin(), q.begin() + (size_t)n * DIAG_COLS);
   *nread = n;
+  return DSPW_OK;
+}
+
+int dspw_snap_enable(dspw_handle* h, int slots) {
+  if (!h || slots < 0) return DSPW_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // the step graph changes
+  if (h->dsnap) cudaFree(h->dsnap);
+  if (h->dsnap_count) cudaFree(h->dsnap_count);
+  if (h->dsnap_meta) cudaFree(h->dsnap_meta);
+  h->dsnap = nullptr; h->dsnap_count = nullptr; h->dsnap_meta = nullptr;
+  h->snap_slots = 0;
+  h->snap_taken.assign(h->nprob, 0);
+  h->snap_dropped.assign(h->nprob, 0);
+  h->snap_host.assign(h->nprob, std::deque<dspw_handle::HostSnap>());
+  if (slots == 0) return DSPW_OK;
+  const size_t bytes = (size_t)h->elem * 5 * (size_t)h->ctot * (size_t)slots;
+  if (cudaMalloc(&h->dsnap, bytes) != cudaSuccess ||
+      cudaMalloc(&h->dsnap_count, sizeof(unsigned long long) * h->nprob) != cudaSuccess ||
+      cudaMalloc(&h->dsnap_meta, sizeof(SnapMeta) * (size_t)h->nprob * slots) != cudaSuccess) {
+    if (h->dsnap) cudaFree(h->dsnap);
+    if (h->dsnap_count) cudaFree(h->dsnap_count);
+    if (h->dsnap_meta) cudaFree(h->dsnap_meta);
+    h->dsnap = nullptr; h->dsnap_count = nullptr; h->dsnap_meta = nullptr;
+    h->last_error = DSPW_ERR_CUDA;
+    return DSPW_ERR_CUDA;
+  }
+  CK(cudaMemset(h->dsnap_count, 0, sizeof(unsigned long long) * h->nprob));
+  CK(cudaMemset(h->dsnap_meta, 0, sizeof(SnapMeta) * (size_t)h->nprob * slots));
+  h->snap_slots = slots;
+  return DSPW_OK;
+}
+
+int dspw_snap_pending(dspw_handle* h, int p, int* n, long long* ndropped) {
+  if (check_p(h, p) || !n) return DSPW_ERR_ARG;
+  int r = drain_snap(h);
+  if (r) return r;
+  *n = h->snap_slots ? (int)h->snap_host[p].size() : 0;
+  if (ndropped) *ndropped = h->snap_slots ? h->snap_dropped[p] : 0;
+  return DSPW_OK;
+}
+
+int dspw_snap_read(dspw_handle* h, int p, double* prim, double* time, int* iter) {
+  if (check_p(h, p) || !prim) return DSPW_ERR_ARG;
+  int r = drain_snap(h);
+  if (r) return r;
+  if (h->snap_slots == 0 || h->snap_host[p].empty()) return DSPW_ERR_ARG;
+  dspw_handle::HostSnap& s = h->snap_host[p].front();
+  memcpy(prim, s.prim.data(), sizeof(double) * s.prim.size());
+  if (time) *time = s.time;
+  if (iter) *iter = s.iter;
+  h->snap_host[p].pop_front();
   return DSPW_OK;
 }
 

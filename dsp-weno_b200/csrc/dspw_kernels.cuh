@@ -83,7 +83,8 @@ struct ProbState {
   double ent, ent_prev, ent_acc, ent_max_rise;
   unsigned long long smax;   // bits of the max wave speed of the newest state
   int iter, active;
-  int pad[2];
+  int snap;                  // 1: this step ended on an output time stamp
+  int pad;
 };
 
 struct StatusDev {

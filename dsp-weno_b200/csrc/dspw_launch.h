@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include "dspw_kernels.cuh"
 #include "dspw_diag.cuh"
+#include "dspw_snap.cuh"
 
 namespace dspw {
 
@@ -38,6 +39,8 @@ struct Launch {
   static cudaError_t diag_cells(const DiagArgs<T>& a, int mode, long long total, cudaStream_t s);
   static cudaError_t diag_nodes(const DiagArgs<T>& a, long long total, cudaStream_t s);
   static cudaError_t diag_row(const DiagArgs<T>& a, cudaStream_t s);
+  // snapshot of the problems that ended the step on a time stamp
+  static cudaError_t snap(const SnapArgs<T>& a, long long ncell_total, cudaStream_t s);
 };
 
 cudaError_t launch_begin_step(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive,

@@ -231,6 +231,9 @@ def lib():
         "dspw_diag_enable": (I, [P, I]),
         "dspw_diag_pending": (I, [P, I, C.POINTER(I), C.POINTER(LL)]),
         "dspw_diag_read": (I, [P, I, dp, I, C.POINTER(I)]),
+        "dspw_snap_enable": (I, [P, I]),
+        "dspw_snap_pending": (I, [P, I, C.POINTER(I), C.POINTER(LL)]),
+        "dspw_snap_read": (I, [P, I, dp, C.POINTER(D), C.POINTER(I)]),
         "dspw_stream": (P, [P]),
         "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),
         "dspw_trainer_create": (I, [C.POINTER(TrainCfg), dp, dp, C.POINTER(P)]),
@@ -414,6 +417,24 @@ class Solver:
         got = C.c_int()
         check(lib().dspw_diag_read(self.h, p, rows, n.value, C.byref(got)), "dspw_diag_read")
         return rows[:got.value], dropped.value
+
+    def snap_enable(self, slots=4):
+        """Take a snapshot whenever a step ends on an output time stamp
+        (dspw_snap_enable); 0 stops."""
+        check(lib().dspw_snap_enable(self.h, int(slots)), "dspw_snap_enable")
+
+    def snapshots(self, p=0):
+        """Pending snapshots of problem p as a list of (time, iter, prim) (read
+        and removed), and the count of snapshots dropped so far."""
+        n, dropped = C.c_int(), C.c_longlong()
+        check(lib().dspw_snap_pending(self.h, p, C.byref(n), C.byref(dropped)), "dspw_snap_pending")
+        out = []
+        for _ in range(n.value):
+            a = np.empty(self.shape(p))
+            t, it = C.c_double(), C.c_int()
+            check(lib().dspw_snap_read(self.h, p, a, C.byref(t), C.byref(it)), "dspw_snap_read")
+            out.append((t.value, it.value, a))
+        return out, dropped.value
 
     def globals(self, p=0):
         g = Globals()

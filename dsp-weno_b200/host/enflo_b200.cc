@@ -12,11 +12,15 @@
 // l1_err.dat / l2_err.dat / linf_err.dat with the table layout of compute_OOC
 // (enflo_scalar/src_scalar/compute_ooc.cc:10-141).  Errors of systems are those
 // of the density.  Runs that are not OOC studies print the reference's per-step
-// residual line (enflo/src/fv.cc:1289-1299, enflo_scalar/src_scalar/fv.cc:578-584).
+// residual line (enflo/src/fv.cc:1289-1299, enflo_scalar/src_scalar/fv.cc:578-584)
+// and write the solution files of FV::output (output.h) at t = 0 and at every
+// time stamp, from snapshots the library takes on the device; the files are
+// written by background threads while the GPU keeps stepping.
 //
 //   enflo_b200 -i param.in [--precision fp64|fp32_bf16] [--chunk K]
 //   enflo_b200 -i param.in --check          parse and print the descriptor, no GPU
 //   enflo_b200 -i param.in --dump-ic FILE   write level 0's initial state (FP64), no GPU
+//   enflo_b200 -i param.in --output-ic      write the t = 0 solution files of FV::output, no GPU
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -29,8 +33,12 @@
 #include <string>
 #include <vector>
 
+#include <deque>
+#include <thread>
+
 #include "../../include/dspw.h"
 #include "expr.h"
+#include "output.h"
 #include "param.h"
 
 using dspw_host::Expr;
@@ -160,6 +168,43 @@ void write_globals(std::ostream& glob, std::ostream& out, const double* rows, in
   }
 }
 
+dspw_host::OutGrid out_grid(const Level& L) {
+  dspw_host::OutGrid g;
+  g.nx = L.d.nx; g.ny = L.d.ny; g.nz = L.d.nz;
+  g.dx = L.dx; g.dy = L.dy; g.dz = L.dz;
+  g.xmin = L.xmin; g.ymin = L.ymin; g.zmin = L.zmin;
+  for (int f = 0; f < 6; f++) {
+    g.bc[f] = L.d.bc[f];
+    for (int v = 0; v < 5; v++) g.bc_state[f][v] = L.d.bc_state[f][v];
+  }
+  g.gamma = L.d.gamma;
+  g.scalar = L.nvar == 1;
+  return g;
+}
+
+// FV::output files written by background threads, at most `max_inflight` at a
+// time; each thread owns its state copy
+struct Writers {
+  std::vector<std::thread> threads;
+  std::deque<std::string> logs;   // stable addresses for the running threads
+  size_t done = 0;
+  void add(const std::string& dir, int counter, double time, const dspw_host::OutGrid& g, std::vector<double> prim,
+           size_t max_inflight = 3) {
+    while (threads.size() - done >= max_inflight) join_one();
+    logs.emplace_back();
+    std::string* log = &logs.back();
+    threads.emplace_back([=, prim = std::move(prim)]() { *log = dspw_host::write_output(dir, counter, time, g, prim); });
+  }
+  void join_one() {
+    threads[done].join();
+    std::cout << logs[done];
+    ++done;
+  }
+  void join_all() {
+    while (done < threads.size()) join_one();
+  }
+};
+
 Level make_level(const Param& P, int rl, const std::string& precision) {
   Level L;
   dspw_desc& d = L.d;
@@ -267,7 +312,7 @@ void write_ooc(const std::string& path, const Param& P, const std::vector<double
 
 int main(int argc, char** argv) {
   std::string file, precision = "fp64", dump;
-  bool check_only = false;
+  bool check_only = false, output_ic = false;
   int chunk = 64;
   for (int a = 1; a < argc; a++) {
     std::string s = argv[a];
@@ -276,9 +321,10 @@ int main(int argc, char** argv) {
     else if (s == "--chunk" && a + 1 < argc) chunk = std::atoi(argv[++a]);
     else if (s == "--check") check_only = true;
     else if (s == "--dump-ic" && a + 1 < argc) dump = argv[++a];
+    else if (s == "--output-ic") output_ic = true;
     else {
       std::cerr << "usage: enflo_b200 -i param.in [--precision fp64|fp32_bf16] [--chunk K] [--check] "
-                   "[--dump-ic FILE]\n";
+                   "[--dump-ic FILE] [--output-ic]\n";
       return 2;
     }
   }
@@ -313,6 +359,11 @@ int main(int argc, char** argv) {
     std::string soln_dir = P.output_path + "/SOLN_FILES_" + P.reconstruct;   // enflo/src/fv.h:28-34
     std::filesystem::remove_all(soln_dir);
     std::filesystem::create_directories(soln_dir);
+    if (output_ic) {
+      std::vector<double> ic = evaluate(levels[0], P.ic, P.constants, 0.0);
+      std::cout << dspw_host::write_output(soln_dir, 0, 0.0, out_grid(levels[0]), ic);
+      return 0;
+    }
     std::ofstream glob(soln_dir + "/globals.dat");
     std::vector<double> l1, l2, linf;
     for (int rl = 0; rl < nlev; rl++) {
@@ -335,10 +386,39 @@ int main(int argc, char** argv) {
              << " " << std::endl;
       }
       int steps = 0;
-      rc = dspw_run(h, chunk, &steps);
       dspw_globals_out g;
-      if (rc == DSPW_OK) rc = dspw_globals(h, 0, &g);
-      if (rc) { dspw_destroy(h); check(rc, "dspw_run"); }
+      if (P.ooc) {
+        rc = dspw_run(h, chunk, &steps);
+        if (rc == DSPW_OK) rc = dspw_globals(h, 0, &g);
+        if (rc) { dspw_destroy(h); check(rc, "dspw_run"); }
+      } else {
+        // solution files at t = 0 and at every time stamp (fv.cc:1242-1243,1309-1313)
+        const dspw_host::OutGrid og = out_grid(L);
+        int counter = 0;
+        Writers writers;
+        writers.add(soln_dir, counter++, 0.0, og, ic);
+        rc = dspw_snap_enable(h, std::max(1, std::min(P.time_stamps, 8)));
+        if (rc) { dspw_destroy(h); check(rc, "dspw_snap_enable"); }
+        long long dropped = 0;
+        for (;;) {
+          rc = dspw_step(h, chunk, 0.0);
+          if (rc == DSPW_OK) rc = dspw_globals(h, 0, &g);
+          dspw_status_out st;
+          if (rc == DSPW_OK && dspw_last_status(h, &st) == DSPW_OK && st.code) rc = st.code;
+          int ns = 0;
+          if (rc == DSPW_OK) rc = dspw_snap_pending(h, 0, &ns, &dropped);
+          for (int q = 0; rc == DSPW_OK && q < ns; q++) {
+            std::vector<double> snap(L.nvar * L.n);
+            double t = 0.0;
+            rc = dspw_snap_read(h, 0, snap.data(), &t, nullptr);
+            if (rc == DSPW_OK) writers.add(soln_dir, counter++, t, og, std::move(snap));
+          }
+          if (rc || g.finished) break;
+        }
+        writers.join_all();
+        if (rc) { dspw_destroy(h); check(rc, "dspw_step"); }
+        if (dropped) std::cerr << "   " << dropped << " solution snapshots were dropped" << std::endl;
+      }
       int nrows = 0, nread = 0;
       check(dspw_diag_pending(h, 0, &nrows, nullptr), "dspw_diag_pending");
       std::vector<double> rows((size_t)nrows * DSPW_DIAG_COLS);

@@ -271,6 +271,32 @@ DSPW_API int dspw_diag_pending(dspw_handle* h, int p, int* nrows, long long* ndr
  * doubles each) into rows and remove them; *nread is the number copied. */
 DSPW_API int dspw_diag_read(dspw_handle* h, int p, double* rows, int max_rows, int* nread);
 
+/* ---- snapshots at the output time stamps -----------------------------
+ * FV::run writes the solution whenever a step ends on a time stamp
+ * (enflo/src/fv.cc:1309-1313, enflo_scalar/src_scalar/fv.cc:586-590).  With
+ * snapshots enabled the step graph copies the state of every problem that
+ * reached a stamp into a device ring of `slots` state buffers; dspw_step and
+ * dspw_run drain the ring every `slots` steps into host memory (primitive
+ * planes, FP64), from where dspw_snap_read hands them out oldest first.  The
+ * writer of the reference's files stays with the caller (the command-line
+ * driver writes sol/omg VTK and 1Dsol files, enflo/src/output.cc:10-172). */
+
+/* slots > 0: take snapshots from now on; 0: stop.  Pending snapshots are
+ * discarded.  Allocates slots x the state size on the device; not during
+ * stream capture. */
+DSPW_API int dspw_snap_enable(dspw_handle* h, int slots);
+
+/* Snapshots of problem p taken and not yet read; *ndropped (may be NULL)
+ * counts those lost because more than `slots` stamps were reached between
+ * drains (dspw_stage does not drain). */
+DSPW_API int dspw_snap_pending(dspw_handle* h, int p, int* n, long long* ndropped);
+
+/* Copy problem p's oldest pending snapshot into prim (nvar x nz x ny x nx
+ * doubles, the layout of dspw_download_prim), its time and iteration count
+ * into *time and *iter (either may be NULL), and remove it.  DSPW_ERR_ARG when
+ * none is pending. */
+DSPW_API int dspw_snap_read(dspw_handle* h, int p, double* prim, double* time, int* iter);
+
 /* Synchronise the handle's stream; returns the first error recorded. */
 DSPW_API int dspw_sync(dspw_handle* h);
 

@@ -188,6 +188,7 @@ def _ref_lib(kind):
             "refE_set_prim": (None, [P, _dp]), "refE_residual": (None, [P, I, _dp]),
             "refE_compute_dt": (D, [P]), "refE_step": (I, [P, I, D]),
             "refE_step_diag": (I, [P, I, D, _dp]),
+            "refE_output": (None, [P, I]),
             "refE_face_flux": (None, [P, _dp, I, _dp, _dp]),
             "refE_reconstruct": (None, [P, _dp, _dp, _dp]),
             "refE_nn_forward": (None, [P, _dp, C.POINTER(D), C.POINTER(D)]),
@@ -202,6 +203,7 @@ def _ref_lib(kind):
             "refS_residual": (None, [P, I, _dp]), "refS_compute_dt": (D, [P]),
             "refS_step": (I, [P, I, D]), "refS_run_errors": (None, [P, _dp]),
             "refS_step_diag": (I, [P, I, D, _dp]),
+            "refS_output": (None, [P, I]),
             "refS_face_flux": (D, [P, _dp, I]),
             "refS_reconstruct": (None, [P, _dp, C.POINTER(D), C.POINTER(D)]),
             "refS_sp_weno": (None, [_dp, I, C.POINTER(D), C.POINTER(D)]),
@@ -231,6 +233,20 @@ class _RefBase:
         self.nx, self.ny, self.nz, self.ng = n[0], n[1], n[2], n[3]
         self.dx, self.dy, self.dz = d[0], d[1], d[2]
 
+    def run_outputs(self):
+        """Run to the end with the reference's solution writer on (t = 0 and
+        every time stamp); returns {file name: text} of its SOLN_FILES folder."""
+        getattr(self.L, self._prefix + "_output")(self.h, 1)
+        getattr(self.L, self._prefix + "_step")(self.h, 1 << 30, 0.0)
+        out = {}
+        for d in os.listdir(self.tmp):
+            if d.startswith("SOLN_FILES_"):
+                for fn in sorted(os.listdir(os.path.join(self.tmp, d))):
+                    if fn.startswith(("sol", "omg", "1Dsol")):
+                        with open(os.path.join(self.tmp, d, fn)) as f:
+                            out[fn] = f.read()
+        return out
+
     def info(self):
         n = (C.c_int * 5)()
         d = (C.c_double * 5)()
@@ -241,6 +257,7 @@ class _RefBase:
 class RefEuler(_RefBase):
     def __init__(self, cfg, level=0):
         self.L = _ref_lib("E")
+        self._prefix = "refE"
         self._create, self._dims = self.L.refE_create, self.L.refE_dims
         super().__init__(cfg, level)
 
@@ -295,6 +312,7 @@ class RefEuler(_RefBase):
 class RefScalar(_RefBase):
     def __init__(self, cfg, level=0):
         self.L = _ref_lib("S")
+        self._prefix = "refS"
         self._create, self._dims = self.L.refS_create, self.L.refS_dims
         super().__init__(cfg, level)
 

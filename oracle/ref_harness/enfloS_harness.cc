@@ -47,6 +47,7 @@ struct Quiet {
 struct Handle {
   FV* fv;
   double t_interval, t_soln_save;
+  int write_output;   // call FV::output at the time stamps, as FV::run does with print_soln
 };
 
 inline size_t plane_index(const FV* f, int i, int j, int k) {
@@ -73,7 +74,7 @@ HX void* refS_create(const char* param_path, int level) {
   fv->counter = 0;
   fv->time = 0.0;
   fv->iter = 0;
-  Handle* h = new Handle;
+  Handle* h = new Handle();
   h->fv = fv;
   h->t_interval = fv->param.final_time / fv->param.t_stamps;
   h->t_soln_save = h->t_interval;
@@ -160,7 +161,12 @@ static int step_impl(Handle* h, int nsteps, double fixed_dt, double* rows) {
       row[2] = f->total_ent;
       row[7] = f->res_norm;
     }
-    if (f->time == h->t_soln_save) h->t_soln_save += h->t_interval;
+    if (f->time == h->t_soln_save) {
+      if (h->write_output) {
+        f->output();
+      }
+      h->t_soln_save += h->t_interval;
+    }
     ++taken;
   }
   return taken;
@@ -213,6 +219,18 @@ HX void refS_reconstruct(void* hp, const double* u4, double* recl, double* recr)
 // sp_weno_rec (enflo_scalar/src_scalar/limiter.h:193-252) with an explicit corr_type.
 HX void refS_sp_weno(const double* u4, int corr_type, double* recl, double* recr) {
   sp_weno_rec(u4, *recl, *recr, corr_type);
+}
+
+// Write FV::output's files now (the reference's solution writer,
+// enflo_scalar/src_scalar/output.cc:10-68) into the run's SOLN_FILES directory, as FV::run
+// does before its time loop, and (on = 1) at every time stamp reached by
+// later steps.
+HX void refS_output(void* hp, int on) {
+  Quiet q;
+  Handle* h = (Handle*)hp;
+  FV* f = h->fv;
+  f->output();
+  h->write_output = on;
 }
 
 }  // extern "C"

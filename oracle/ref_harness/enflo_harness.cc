@@ -49,6 +49,7 @@ struct Quiet {   // the reference prints progress to std::cout; silence it insid
 struct Handle {
   FV* fv;
   double t_interval, t_soln_save;
+  int write_output;   // call FV::output at the time stamps, as FV::run does with print_soln
 };
 
 inline int ncell(const FV* f) { return f->Nx_cell * f->Ny_cell * f->Nz_cell; }
@@ -77,7 +78,8 @@ HX void* refE_create(const char* param_path, int level) {
   fv->prim_to_ent();
   fv->time = 0.0;
   fv->iter = 0;
-  Handle* h = new Handle;
+  fv->counter = 0;   // output file numbering, FV::run (enflo/src/fv.cc:1245)
+  Handle* h = new Handle();
   h->fv = fv;
   h->t_interval = fv->param.final_time / fv->param.t_stamps;
   h->t_soln_save = h->t_interval;
@@ -228,7 +230,13 @@ static int step_impl(Handle* h, int nsteps, double fixed_dt, double* rows) {
       row[10] = f->res_norm.momentum_flux.z;
       row[11] = f->res_norm.energy_flux;
     }
-    if (f->time == h->t_soln_save) h->t_soln_save += h->t_interval;
+    if (f->time == h->t_soln_save) {
+      if (h->write_output) {
+        f->find_vorticity();
+        f->output();
+      }
+      h->t_soln_save += h->t_interval;
+    }
     ++taken;
   }
   return taken;
@@ -303,5 +311,18 @@ HX void refE_nn_forward(void* hp, const double* u4, double* recl, double* recr) 
 }
 
 HX double refE_logavg(double a, double b) { return logavg(a, b); }
+
+// Write FV::output's files now (the reference's solution writer,
+// enflo/src/output.cc:10-172) into the run's SOLN_FILES directory, as FV::run
+// does before its time loop, and (on = 1) at every time stamp reached by
+// later steps.
+HX void refE_output(void* hp, int on) {
+  Quiet q;
+  Handle* h = (Handle*)hp;
+  FV* f = h->fv;
+  f->find_vorticity();
+  f->output();
+  h->write_output = on;
+}
 
 }  // extern "C"

@@ -350,6 +350,40 @@ def gen_diag():
     np.savez_compressed(OUT / "diag.npz", **out)
 
 
+def output_cases():
+    """(name, kind, cfg) of short runs whose solution files (FV::output at t = 0
+    and at every time stamp) are kept as golden text."""
+    bc1d = ["neumann", "neumann", "periodic", "periodic", "periodic", "periodic"]
+    wall_ic = dict(density="1+0.5*exp(-40*((x-0.4)^2+(y-0.6)^2))", xvelocity="0.3", yvelocity="-0.2*x",
+                   pressure="1+0.5*exp(-40*((x-0.4)^2+(y-0.6)^2))")
+    return [
+        ("kh_out", "E", euler_cfg("kepes_tecno4_roe", "sp_weno", Nx=16, Ny=16, ic=KH_IC, dim=2, final_time=0.02,
+                                  time_stamps=2)),
+        ("wall_out", "E", euler_cfg("kepes_tecno4_roe", "sp_weno", Nx=12, Ny=10, ic=wall_ic, dim=2,
+                                    bc=["wall", "wall", "wall", "neumann", "periodic", "periodic"], final_time=0.01,
+                                    time_stamps=2)),
+        ("shu_out", "E", euler_cfg("kepes_tecno4_roe", "sp_weno_dl", x=(-5, 5), Nx=50, cfl=0.4, final_time=0.05,
+                                   ic=SHU_IC, bc=bc1d, time_stamps=2)),
+        ("tgv_out", "E", euler_cfg("kepes_tecno4_roe", "sp_weno", model="ns_es", x=(0, "2*pi"), y=(0, "2*pi"),
+                                   z=(0, "2*pi"), Nx=6, Ny=6, Nz=6, ic=TGV_IC, dim=3, constants={"M": 0.3},
+                                   mu_ref=0.05, prandtl=0.71, final_time=0.02, time_stamps=1)),
+        ("linadv_out", "S", dict(model="linadv", x=("-pi", "pi"), Nx=40, Ny=2, Nz=2, cfl=0.5, final_time=0.1,
+                                 reconstruct="sp_weno", net_file=NET, flux="lin_tecno4", ic="pow(sin(x),4)",
+                                 bc="periodic", time_stamps=2)),
+    ]
+
+
+def gen_output():
+    out = {}
+    for name, kind, cfg in output_cases():
+        R = O.RefEuler(cfg) if kind == "E" else O.RefScalar(cfg)
+        files = R.run_outputs()
+        for fn, text in files.items():
+            out[f"{name}|{fn}"] = np.array(text)
+        print(f"  output {name}: {sorted(files)}")
+    np.savez_compressed(OUT / "output.npz", **out)
+
+
 def gen_ooc():
     out = {}
     for recon in ("sp_weno", "sp_wenoc", "sp_weno_dl"):
@@ -376,6 +410,7 @@ def main():
     gen_ooc()
     gen_faces_simple(np.random.default_rng(20240612))
     gen_diag()
+    gen_output()
 
 
 if __name__ == "__main__":

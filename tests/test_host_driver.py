@@ -280,3 +280,66 @@ def test_globals_file_matches_reference_rows(tmp_path, name):
     for c in range(got.shape[1]):
         scale = np.max(np.abs(want[:, c]))
         assert np.max(np.abs(got[:, c] - want[:, c])) <= 2e-9 * scale + 1e-300, (name, c, got[:, c], want[:, c])
+
+
+def _output_cases():
+    from make_golden import output_cases
+    return output_cases()
+
+
+def _compare_text(got, want, what, rtol):
+    """Line-by-line comparison of a solution file: identical structure and
+    words, numbers equal to `rtol` (the files print 6 significant digits)."""
+    gl, wl = got.splitlines(), want.splitlines()
+    assert len(gl) == len(wl), (what, len(gl), len(wl))
+    for n, (a, b) in enumerate(zip(gl, wl)):
+        if a == b:
+            continue
+        ta, tb = a.split(), b.split()
+        assert len(ta) == len(tb), (what, n, a, b)
+        for x, y in zip(ta, tb):
+            if x == y:
+                continue
+            fx, fy = float(x), float(y)   # words must be identical; numbers may differ in the last digit
+            assert abs(fx - fy) <= rtol * max(abs(fy), 1e-300) or abs(fx - fy) <= 1e-12, (what, n, a, b)
+
+
+@pytest.mark.parametrize("case", _output_cases(), ids=lambda c: c[0])
+def test_initial_solution_files_match_reference(tmp_path, case):
+    """The t = 0 files of FV::output (sol0000.vtk, omg0000.vtk with the node
+    vorticity, 1Dsol0000.dat) written by the driver's own writer, against the
+    files the reference's writer produced for the same param.in."""
+    _need_cli()
+    name, kind, cfg = case
+    gold = load("output.npz")
+    cfg = dict(cfg)
+    cfg["ooc"] = False
+    p = _write(tmp_path, cfg)
+    r = _run(["-i", p, "--output-ic"], tmp_path)
+    soln = tmp_path / f"SOLN_FILES_{cfg['reconstruct']}"
+    names = [k.split("|")[1] for k in gold.files if k.startswith(name + "|") and "0000" in k]
+    assert names and "Saving solutions in" in r.stdout
+    for fn in names:
+        # the initial state is the same expression evaluation: only last-digit
+        # differences of the 6-digit print are allowed
+        _compare_text((soln / fn).read_text(), str(gold[f"{name}|{fn}"]), f"{name}/{fn}", rtol=2e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", _output_cases(), ids=lambda c: c[0])
+def test_solution_files_at_time_stamps_match_reference(tmp_path, case):
+    """A full run through the driver: the solution files at t = 0 and at every
+    time stamp (from the device snapshots) against the reference's files."""
+    _need_cli()
+    name, kind, cfg = case
+    gold = load("output.npz")
+    cfg = dict(cfg)
+    cfg["ooc"] = False
+    p = _write(tmp_path, cfg)
+    _run(["-i", p], tmp_path)
+    soln = tmp_path / f"SOLN_FILES_{cfg['reconstruct']}"
+    names = sorted(k.split("|")[1] for k in gold.files if k.startswith(name + "|"))
+    got_names = sorted(f.name for f in soln.iterdir() if f.name.startswith(("sol", "omg", "1Dsol")))
+    assert got_names == names
+    for fn in names:
+        _compare_text((soln / fn).read_text(), str(gold[f"{name}|{fn}"]), f"{name}/{fn}", rtol=2e-5)
