@@ -216,6 +216,36 @@ __global__ void k_feature_max(const float* data, long long cap, long long n, uns
   for (int k = 0; k < 5; k++) atomicMax(&out[k], __float_as_uint(fabsf(data[k * cap + i])));
 }
 
+// One row of the reference trainer's data file per sample, in the column
+// order its reader slices (DSP-WENO_trainer/DSP-WENO_network_trainer.py:305-333
+// with tanh_theta: cell values 0-3, theta-, theta+ 4-5, the network inputs
+// tanh theta-, tanh theta+, del1..del3 6-10, vertex x 11-15, vertex y 16-20,
+// target interface values left, right 21-22), recomputed in FP64 from the
+// sample's cell values with the kernels' own feature code.  valid[i] = 0 for
+// samples the trainer ignores.
+constexpr int EXPORT_COLS = 23;
+__global__ void k_export_rows(const float* data, long long cap, long long n, double* out, int* valid) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (data[21 * cap + i] == 0.f) { valid[i] = 0; return; }
+  double u[4];
+  for (int k = 0; k < 4; k++) u[k] = (double)data[(15 + k) * cap + i];
+  double f[5], vx[5], vy[5];
+  nn_features<double>(u[0], u[1], u[2], u[3], f, vx, vy);
+  // theta of the scaled stencil, as nn_features forms it (neural_network.cc:27-28)
+  double mx = 1.0;
+  for (int k = 0; k < 4; k++) mx = fmax(mx, fabs(u[k]));
+  const double c0 = u[0] / mx, c1 = u[1] / mx, c2 = u[2] / mx, c3 = u[3] / mx;
+  double* r = out + (size_t)EXPORT_COLS * i;
+  for (int k = 0; k < 4; k++) r[k] = u[k];
+  r[4] = (c3 - c2) / (c2 - c1);
+  r[5] = (c1 - c0) / (c2 - c1);
+  for (int k = 0; k < 5; k++) { r[6 + k] = f[k]; r[11 + k] = vx[k]; r[16 + k] = vy[k]; }
+  r[21] = (double)data[19 * cap + i];
+  r[22] = (double)data[20 * cap + i];
+  valid[i] = 1;
+}
+
 }  // namespace
 
 struct dspw_trainer {
@@ -454,6 +484,39 @@ int dspw_trainer_get_params(dspw_trainer* t, double* w, double* b) {
   if (cudaMemcpy(h, t->prm, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return DSPW_ERR_CUDA;
   for (int k = 0; k < 100; k++) w[k] = h[k];
   for (int k = 0; k < 20; k++) b[k] = h[100 + k];
+  return DSPW_OK;
+}
+
+int dspw_trainer_export(dspw_trainer* t, double* rows, long long max_rows, long long* nrows) {
+  if (!t || !nrows || max_rows < 0 || (max_rows > 0 && !rows)) return DSPW_ERR_ARG;
+  *nrows = 0;
+  if (t->n == 0) return DSPW_OK;
+  double* dout = nullptr;
+  int* dvalid = nullptr;
+  if (cudaMalloc(&dout, sizeof(double) * EXPORT_COLS * t->n) != cudaSuccess ||
+      cudaMalloc(&dvalid, sizeof(int) * t->n) != cudaSuccess) {
+    if (dout) cudaFree(dout);
+    return DSPW_ERR_CUDA;
+  }
+  std::vector<double> h((size_t)EXPORT_COLS * t->n);
+  std::vector<int> valid(t->n);
+  k_export_rows<<<(int)((t->n + TPB - 1) / TPB), TPB, 0, t->stream>>>(t->data, t->cap, t->n, dout, dvalid);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h.data(), dout, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, t->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(valid.data(), dvalid, sizeof(int) * t->n, cudaMemcpyDeviceToHost, t->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+  cudaFree(dout);
+  cudaFree(dvalid);
+  if (e != cudaSuccess) return DSPW_ERR_CUDA;
+  long long k = 0;
+  for (long long i = 0; i < t->n; i++) {
+    if (!valid[i]) continue;
+    if (rows && k < max_rows) memcpy(rows + EXPORT_COLS * k, &h[(size_t)EXPORT_COLS * i], sizeof(double) * EXPORT_COLS);
+    k++;
+  }
+  *nrows = rows ? std::min(k, max_rows) : k;
   return DSPW_OK;
 }
 

@@ -245,6 +245,7 @@ def lib():
         "dspw_trainer_get_params": (I, [P, dp, dp]),
         "dspw_trainer_info": (I, [P, C.POINTER(LL), dp]),
         "dspw_trainer_eval": (I, [P, C.POINTER(D)]),
+        "dspw_trainer_export": (I, [P, C.c_void_p, LL, C.POINTER(LL)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -320,6 +321,17 @@ class Trainer:
         v = C.c_double()
         check(lib().dspw_trainer_eval(self.h, C.byref(v)), "dspw_trainer_eval")
         return v.value
+
+    def export_rows(self):
+        """The valid samples as rows of the reference trainer's data file
+        (dspw_trainer_export; 23 columns, see dspw.traindata)."""
+        n = C.c_longlong()
+        check(lib().dspw_trainer_export(self.h, None, 0, C.byref(n)), "dspw_trainer_export")
+        rows = np.zeros((n.value, 23))
+        got = C.c_longlong()
+        check(lib().dspw_trainer_export(self.h, rows.ctypes.data_as(C.c_void_p), n.value, C.byref(got)),
+              "dspw_trainer_export")
+        return rows[:got.value]
 
     def params(self):
         w, b = np.zeros(100), np.zeros(20)

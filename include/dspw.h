@@ -344,6 +344,13 @@ DSPW_API int dspw_trainer_eval(dspw_trainer* t, double* mean_loss);
 /* Number of samples and the largest |feature| of each of the 5 network inputs
  * over the valid samples: the training box used for the SP-WENO fallback. */
 DSPW_API int dspw_trainer_info(dspw_trainer* t, long long* nsamples, double* feature_max /* 5 */);
+/* The trainer's valid samples as rows of the reference trainer's data file
+ * (23 doubles each, the column order its reader slices with tanh_theta,
+ * DSP-WENO_trainer/DSP-WENO_network_trainer.py:305-333: cell values u0..u3,
+ * theta-, theta+, tanh theta-, tanh theta+, del1..del3, vertex x 0..4,
+ * vertex y 0..4, target left, target right).  rows == NULL: *nrows is the
+ * number of valid samples; else at most max_rows are copied. */
+DSPW_API int dspw_trainer_export(dspw_trainer* t, double* rows, long long max_rows, long long* nrows);
 
 #ifdef __cplusplus
 }
