@@ -46,7 +46,6 @@ __global__ void k_begin_step_wrap(const ProbDev* prob, ProbState* st, int nprob,
   S.dt = dt;
   S.factor = dt / (P.dx * P.dy * P.dz);
   S.smax = 0ull;
-  S.ent_acc = 0.0;
 }
 
 cudaError_t launch_begin_step(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive,
@@ -67,28 +66,11 @@ __global__ void k_end_step(const ProbDev* prob, ProbState* st, int nprob) {
   const int stamp = S.time == S.t_save;   // output time stamp (fv.cc:1309-1313)
   if (stamp) S.t_save += prob[p].t_interval;
   S.snap = stamp;
-  S.ent_prev = S.ent;
-  S.ent = S.ent_acc * prob[p].vol;
-  double rise = (S.ent - S.ent_prev) / fabs(S.ent_prev);
-  if (rise > S.ent_max_rise) S.ent_max_rise = rise;
 }
 
 
 cudaError_t launch_end_step(const ProbDev* prob, ProbState* st, int nprob, cudaStream_t s) {
   k_end_step<<<(nprob + 127) / 128, 128, 0, s>>>(prob, st, nprob);
-  return cudaGetLastError();
-}
-
-__global__ void k_init_state(const ProbDev* prob, ProbState* st, int p) {
-  ProbState& S = st[p];
-  S.ent = S.ent_acc * prob[p].vol;
-  S.ent_prev = S.ent;
-  S.ent_acc = 0.0;
-  S.ent_max_rise = -1e300;
-}
-
-cudaError_t launch_init_state(const ProbDev* prob, ProbState* st, int p, cudaStream_t s) {
-  k_init_state<<<1, 1, 0, s>>>(prob, st, p);
   return cudaGetLastError();
 }
 
@@ -908,7 +890,6 @@ int dspw_upload_prim(dspw_handle* h, int p, const double* prim) {
     CK(Launch<double>::upload(h->dprob, h->dst, p, h->dstage, (double*)h->Un, h->ctot, n, h->stream));
   else
     CK(Launch<float>::upload(h->dprob, h->dst, p, h->dstage, (float*)h->Un, h->ctot, n, h->stream));
-  CK(launch_init_state(h->dprob, h->dst, p, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return DSPW_OK;
 }

@@ -80,7 +80,6 @@ constexpr int spec_code(int dim, int rec) { return 10 * dim + rec; }
 
 struct ProbState {
   double time, dt, t_save, factor;
-  double ent, ent_prev, ent_acc, ent_max_rise;
   unsigned long long smax;   // bits of the max wave speed of the newest state
   int iter, active;
   int snap;                  // 1: this step ended on an output time stamp
@@ -229,6 +228,14 @@ template <typename T>
 DSPW_HD double wave_speed(const ProbDev& P, const T p[5]) {
   if (P.model == DSPW_LINADV) return P.lin_speed;
   if (P.model == DSPW_BURGERS) return (double)Mth<T>::abs(p[0]);
+  if constexpr (sizeof(T) == 4) {
+    // FP32 state: its speed in FP32 (the FP64 square roots cost 4 % of the
+    // FP32 step); the viscous term stays in FP64
+    if (P.model == DSPW_EULER) {
+      const float s = sqrtf(p[1] * p[1] + p[2] * p[2] + p[3] * p[3]) + sqrtf((float)P.gamma * p[4] / p[0]);
+      return (double)s;
+    }
+  }
   double rho = (double)p[0], pr = (double)p[4];
   double u = p[1], v = p[2], w = p[3];
   double s = ::sqrt(u * u + v * v + w * w) + ::sqrt(P.gamma * pr / rho);
@@ -777,11 +784,10 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
     Lam[0] = Lam[1] = Lam[2] = Lam[3] = Lam[4] = lr;
   }
   T Diff[5] = {T(0), T(0), T(0), T(0), T(0)};
-#pragma unroll
-  for (int j = 0; j < 5; j++) {
+  auto component = [&](int j) {
     // components that are identically zero in lower dimensions (exact skip)
-    if (DIM == 1 && (j == 2 || j == 3)) continue;
-    if (DIM == 2 && j == 3) continue;
+    if (DIM == 1 && (j == 2 || j == 3)) return;
+    if (DIM == 2 && j == 3) return;
     // column j of R (kepes_tecno4_roe.cc:66-72), scaled by S[j]
     T col[5];
     if (j == 0) { col[0] = T(1); col[1] = vel[0] - a * n0; col[2] = vel[1] - a * n1; col[3] = vel[2] - a * n2; col[4] = H - a * fa.vn; }
@@ -789,8 +795,10 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
     else if (j == 2) { col[0] = T(0); col[1] = n1; col[2] = -n0; col[3] = T(0); col[4] = v1; }
     else if (j == 3) { col[0] = T(0); col[1] = -n2; col[2] = T(0); col[3] = n0; col[4] = v2; }
     else { col[0] = T(1); col[1] = vel[0] + a * n0; col[2] = vel[1] + a * n1; col[3] = vel[2] + a * n2; col[4] = H + a * fa.vn; }
+    // S[j] and Lam[j] by selects: j may be a run-time value (no local memory)
+    const T Sj = j == 0 ? S[0] : (j == 1 ? S[1] : (j == 2 ? S[2] : (j == 3 ? S[3] : S[4])));
 #pragma unroll
-    for (int r = 0; r < 5; r++) col[r] *= S[j];
+    for (int r = 0; r < 5; r++) col[r] *= Sj;
     T z[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -808,9 +816,20 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
                       z[0], z[1], z[2], z[3], zl, zr);
     T dZ = zr - zl;
     if (valid && sign_violation<T>(z[0], z[1], z[2], z[3], zl, zr)) signv++;
-    T ld = Lam[j];
+    T ld = j == 0 ? Lam[0] : (j == 1 ? Lam[1] : (j == 2 ? Lam[2] : (j == 3 ? Lam[3] : Lam[4])));
 #pragma unroll
     for (int i = 0; i < 5; i++) Diff[i] += col[i] * ld * dZ;
+  };
+  // The FP32 DSP-WENO kernels keep this loop rolled: one copy of the
+  // reconstruction (features, network, limiter) instead of four or five
+  // relieves the instruction cache (KH 2048^2: 3.31 -> 3.23 ms per step).
+  // Unrolled is faster for the SP-WENO family and for FP64 (1-3 %).
+  if constexpr (sizeof(T) == 4 && Sp::rec == 2) {
+#pragma unroll 1
+    for (int j = 0; j < 5; j++) component(j);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 5; j++) component(j);
   }
   flux[0] -= T(0.5) * Diff[0];
   flux[1] -= T(0.5) * Diff[1];
@@ -899,11 +918,11 @@ __device__ inline void stage_combine(const SweepArgs<T>& A, const ProbDev& P, co
 }
 
 // stage update of one Euler cell from its residual R, U^(k) (u) and U^n (un),
-// stored to Uout, with the CFL speed / entropy / health epilogue on the stage
+// stored to Uout, with the CFL speed / health epilogue on the stage
 // that yields U^(n+1).
 template <typename T>
 __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
-                                         const T R[5], T u[5], const T un[5], double& smax, double& ent,
+                                         const T R[5], T u[5], const T un[5], double& smax,
                                          unsigned& bad_fin, unsigned& bad_pos) {
   stage_combine<T>(A, P, S, cell, R, u, un);
   store_cons<T>(A.Uout, A.ctot, cell, P.nv, u);
@@ -916,19 +935,17 @@ __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P
     double rho = p[0], pr = p[4];
     if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
     if (!isfinite(rho) || !isfinite(pr) || !isfinite((double)u[1]) || !isfinite((double)u[4])) bad_fin++;
-    double s = ::log(pr) - P.gamma * ::log(rho);
-    ent += -rho * s / (P.gamma - 1.0);
   }
 }
 
 // final combination for one cell: residual (reference order
 // ((R_prev - F_left) + F_right)) then either store R or apply the SSPRK stage
 // update U = b U + (a U^n + R (-factor b)) (enflo/src/fv.cc:1163-1175), with
-// the CFL speed / entropy / health epilogue on the stage that yields U^(n+1).
+// the CFL speed / health epilogue on the stage that yields U^(n+1).
 template <typename T>
 __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
                                    bool first, bool final_sweep, const T Fl[5], const T Fr[5], int nv_eff,
-                                   double& smax, double& ent, unsigned& bad_fin, unsigned& bad_pos) {
+                                   double& smax, unsigned& bad_fin, unsigned& bad_pos) {
   T R[5];
   if (first) {
 #pragma unroll
@@ -972,29 +989,24 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
       T pp[5] = {x, T(0), T(0), T(0), T(0)};
       double sp = wave_speed<T>(P, pp);
       if (sp > smax) smax = sp;   // NaN speeds are skipped, as std::min skips them in compute_dt
-      ent += 0.5 * (double)x * (double)x;
       if (!isfinite((double)x)) bad_fin++;
     }
     return;
   }
   load_cons<T>(A.Uin, A.ctot, cell, P.nv, P.dim, u);
   load_cons<T>(A.Un, A.ctot, cell, P.nv, P.dim, un);
-  update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
+  update_euler_cell<T>(A, P, S, cell, R, u, un, smax, bad_fin, bad_pos);
   (void)a; (void)c2; (void)nv_eff;
 }
 
 template <typename T>
-__device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax, double ent,
+__device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax,
                                      unsigned bad_fin, unsigned bad_pos, unsigned long long signv, int viol,
                                      unsigned checked) {
   if (A.final_stage && !A.residual_only) {
     unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
     warp_max_u64_lane0(sb);
-    double es = warp_sum(ent);
-    if (lane == 0) {
-      atomicMax(&S.smax, sb);
-      atomicAdd(&S.ent_acc, es);
-    }
+    if (lane == 0) atomicMax(&S.smax, sb);
   }
   unsigned bf = __reduce_add_sync(0xffffffffu, bad_fin);
   unsigned bp = __reduce_add_sync(0xffffffffu, bad_pos);
@@ -1088,19 +1100,19 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
   // phase D: cells
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
-  double smax = 0.0, ent = 0.0;
+  double smax = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
   if (lane < ncell) {
     T Fl[5], Fr[5];
 #pragma unroll
     for (int v = 0; v < 5; v++) { Fl[v] = sm->F[v][lane]; Fr[v] = sm->F[v][lane + 1]; }
     long long cell = cell_index<DIR>(P, i0, j0, k0, c0 + lane);
-    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, P.nv, smax, ent, bad_fin, bad_pos);
+    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, P.nv, smax, bad_fin, bad_pos);
   }
-  if (!final_sweep) { smax = 0.0; ent = 0.0; }
+  if (!final_sweep) smax = 0.0;
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
+  warp_epilogue<T>(A2, S, lane, smax, bad_fin, bad_pos, signv, viol, checked);
   __syncwarp();
 }
 
@@ -1250,7 +1262,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
     euler_faces<T, DIR, DIM, Sp>(A, P, sm0 + warp, lane, ncell, viol, signv, checked, (unsigned)(lt0 + warp));
   if (aligned) cp_async_wait<0>();
   __syncthreads();
-  double smax = 0.0, ent = 0.0;
+  double smax = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
   for (int row = tid / COOP_COLS; row < ncell && col < ncols; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
     WarpSmem<T>* sc = sm0 + col;
@@ -1265,13 +1277,13 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
       T u[5], un[5];
       tile_cons<T>(tl.U, nv, row + 2, col, u);
       tile_cons<T>(tl.Un, nv, row, col, un);
-      update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
+      update_euler_cell<T>(A, P, S, cell, R, u, un, smax, bad_fin, bad_pos);
     }
   }
-  if (!final_sweep) { smax = 0.0; ent = 0.0; }
+  if (!final_sweep) smax = 0.0;
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
+  warp_epilogue<T>(A2, S, lane, smax, bad_fin, bad_pos, signv, viol, checked);
   __syncthreads();
 }
 
@@ -1335,17 +1347,17 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   __syncwarp();
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && (DIR == P.dim - 1);
-  double smax = 0.0, ent = 0.0;
+  double smax = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
   if (lane < ncell) {
     T Fl[5] = {sm->F[0][lane], T(0), T(0), T(0), T(0)};
     T Fr[5] = {sm->F[0][lane + 1], T(0), T(0), T(0), T(0)};
     long long cell = cell_index<DIR>(P, i0, j0, k0, c0 + lane);
-    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, 1, smax, ent, bad_fin, bad_pos);
+    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, 1, smax, bad_fin, bad_pos);
   }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, (P.tecno && valid) ? 1u : 0u);
+  warp_epilogue<T>(A2, S, lane, smax, bad_fin, bad_pos, signv, viol, (P.tecno && valid) ? 1u : 0u);
   __syncwarp();
 }
 
@@ -1424,21 +1436,20 @@ k_sweep(SweepArgs<T> A) {
 
 // ----------------------------------------------------------- step control --
 
-// upload: primitive (FP64, staging) -> conserved state, plus the wave speed and
-// entropy of that primitive state (prim_to_con, enflo/src/fv.cc:405-416)
+// upload: primitive (FP64, staging) -> conserved state, plus the wave speed of
+// that primitive state (prim_to_con, enflo/src/fv.cc:405-416)
 template <typename T>
 __global__ void k_upload(const ProbDev* prob, ProbState* st, int p, const double* prim, T* U, long long ctot) {
   const ProbDev& P = prob[p];
   ProbState& S = st[p];
   long long n = (long long)P.nx * P.ny * P.nz;
-  double smax = 0.0, ent = 0.0;
+  double smax = 0.0;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     if (P.is_scalar) {
       double u = prim[c];
       U[P.off + c] = T(u);
       double sp = (P.model == DSPW_LINADV) ? P.lin_speed : fabs(u);
       if (sp > smax) smax = sp;
-      ent += 0.5 * u * u;
     } else {
       double pd[5];
       for (int v = 0; v < 5; v++) pd[v] = prim[v * n + c];
@@ -1448,17 +1459,11 @@ __global__ void k_upload(const ProbDev* prob, ProbState* st, int p, const double
       store_cons<T>(U, ctot, P.off + c, P.nv, u);
       double sp = wave_speed<double>(P, pd);
       if (sp > smax) smax = sp;
-      double s = ::log(pd[4]) - P.gamma * ::log(pd[0]);
-      ent += -pd[0] * s / (P.gamma - 1.0);
     }
   }
   unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
   warp_max_u64_lane0(sb);
-  double es = warp_sum(ent);
-  if ((threadIdx.x & 31) == 0) {
-    atomicMax(&S.smax, sb);
-    atomicAdd(&S.ent_acc, es);
-  }
+  if ((threadIdx.x & 31) == 0) atomicMax(&S.smax, sb);
 }
 
 // wave-speed max of the current state (dspw_compute_dt)
@@ -1743,7 +1748,7 @@ __global__ void k_visc_nodes(const ProbDev* prob, int nprob, const long long* ce
 template <typename T>
 __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const T* node) {
   long long total = cell_start[A.nprob];
-  double smax = 0.0, ent = 0.0;
+  double smax = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
   int pcur = -1;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
@@ -1792,26 +1797,19 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
       double rho = p[0], pr = p[4];
       if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
       if (!isfinite(rho) || !isfinite(pr)) bad_fin++;
-      double s = ::log(pr) - P.gamma * ::log(rho);
-      ent += -rho * s / (P.gamma - 1.0);
     }
   }
-  // one speed-max / entropy flush per thread, warp-aggregated when the warp
-  // worked on a single problem
+  // one speed-max flush per thread, warp-aggregated when the warp worked on a
+  // single problem
   int p0 = __shfl_sync(0xffffffffu, pcur, 0);
   bool uniform = __all_sync(0xffffffffu, pcur == p0 || pcur < 0);
   if (A.final_stage && !A.residual_only) {
     if (uniform) {
       unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
       warp_max_u64_lane0(sb);
-      double es = warp_sum(ent);
-      if ((threadIdx.x & 31) == 0 && p0 >= 0) {
-        atomicMax(&A.st[p0].smax, sb);
-        atomicAdd(&A.st[p0].ent_acc, es);
-      }
+      if ((threadIdx.x & 31) == 0 && p0 >= 0) atomicMax(&A.st[p0].smax, sb);
     } else if (pcur >= 0) {
       atomicMax(&A.st[pcur].smax, (unsigned long long)__double_as_longlong(smax));
-      atomicAdd(&A.st[pcur].ent_acc, ent);
     }
   }
   if (bad_fin) { atomicAdd(&A.status->nonfinite, (unsigned long long)bad_fin); atomicCAS(&A.status->code, 0, DSPW_ERR_NONFINITE); }

@@ -57,6 +57,5 @@ namespace dspw {
 // enabled (used by the trainer); returns a dspw status
 int handle_collect(dspw_handle* h, float* buf, unsigned long long* count, unsigned long long cap, unsigned stride);
 int handle_precision(const dspw_handle* h);
-cudaError_t launch_init_state(const ProbDev* prob, ProbState* st, int p, cudaStream_t s);
 
 }  // namespace dspw
