@@ -28,7 +28,10 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 
 UNITS = {
     "dspw_fp64.cu": ["--fmad=false"],
-    "dspw_fp32.cu": ["--fmad=true"],
+    # FP32 form: approximate division and square root, denormals flushed
+    # (KH 2048^2: DSP-WENO 3.15 -> 3.02 ms, SP-WENO 2.29 -> 1.91 ms per step);
+    # the FP64 units keep IEEE arithmetic without contraction, for parity
+    "dspw_fp32.cu": ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "dspw_capi.cu": ["--fmad=false"],
     "dspw_train.cu": ["--fmad=true"],
     "dspw_noalloc.cu": ["--fmad=false"],
@@ -40,14 +43,19 @@ def compile_unit(name: str, flags: list[str], verbose: bool) -> Path:
     obj = BUILD / (name + ".o")
     deps = [src] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc")) + [
         REPO / "include" / "dspw.h"]
-    if obj.exists() and all(obj.stat().st_mtime >= d.stat().st_mtime for d in deps) and not verbose:
-        return obj
     cmd = [NVCC, *ARCH, *COMMON, *EXTRA, *flags, "-c", str(src), "-o", str(obj)]
+    # the object is current when it is newer than its sources and was built
+    # with the same command line
+    stamp = obj.with_suffix(".cmd")
+    same = stamp.exists() and stamp.read_text() == " ".join(cmd)
+    if same and obj.exists() and all(obj.stat().st_mtime >= d.stat().st_mtime for d in deps) and not verbose:
+        return obj
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {name}:\n{r.stderr}")
+    stamp.write_text(" ".join(cmd))
     if verbose and r.stderr:
         print(r.stderr)
     return obj
