@@ -45,9 +45,13 @@ sys.path.insert(0, str(REPO / "oracle"))
 
 METRIC = "cell-updates/s"
 NET_FILE = REPO / "tests" / "golden" / "dsp_weno.txt"
-# per-launch DRAM traffic of the dominant kernel from the committed ncu capture
-# (profiles/sweep_kernels_kh.md); None until measured
-NCU_TRAFFIC_BYTES_PER_CELL = None
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant
+# launch per cell, from one ncu capture of that launch
+# (profiles/sweep_kernels_kh2048.md): KH 2048^2 FP32 DSP-WENO, last-stage y sweep,
+# 203.04 MB + 47.42 MB for 4194304 cells
+NCU_TRAFFIC_BYTES_PER_CELL = {
+    ("kh2048_fp32_bf16_sp_weno_dl_kepes_tecno4_roe", "sweep_y"): (203.043072e6 + 47.419392e6) / 4194304,
+}
 
 
 # ------------------------------------------------------------------ CPU legs
@@ -525,9 +529,9 @@ def main():
     e2e_v = r["ncell_all"] * r["e2e_steps"] / r["e2e_s"]
     dom = r["dom"]
     traffic = None
-    if NCU_TRAFFIC_BYTES_PER_CELL is not None:
-        traffic = NCU_TRAFFIC_BYTES_PER_CELL.get(dom[0], None)
-        traffic = traffic * r["ncell"] if traffic else None
+    per_cell = NCU_TRAFFIC_BYTES_PER_CELL.get((config.get("workload"), dom[0]))
+    if per_cell:
+        traffic = per_cell * r["ncell"]
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": r["ms"] / steps, "higher_is_better": True, "scaling": r["scaling"],
