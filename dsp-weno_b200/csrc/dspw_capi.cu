@@ -69,6 +69,30 @@ __global__ void k_end_step(const ProbDev* prob, ProbState* st, int nprob) {
 }
 
 
+// checks of an uploaded primitive state (nvar planes of n values, FP64):
+// bad[0] counts cells with density or pressure <= 0 or NaN (systems), bad[1]
+// non-finite values; the initial state must be positive (enflo/src/fv.cc:88-89)
+__global__ void k_check_prim(const double* prim, long long n, int nv, unsigned long long* bad) {
+  unsigned long long pos = 0, fin = 0;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    if (nv == 5 && (!(prim[c] > 0.0) || !(prim[4 * n + c] > 0.0))) pos++;
+    for (int v = 0; v < nv; v++) fin += !isfinite(prim[v * n + c]);
+  }
+  pos = __reduce_add_sync(0xffffffffu, (unsigned)pos);
+  fin = __reduce_add_sync(0xffffffffu, (unsigned)fin);
+  if ((threadIdx.x & 31) == 0 && (pos | fin)) {
+    atomicAdd(bad, pos);
+    atomicAdd(bad + 1, fin);
+  }
+}
+
+cudaError_t launch_check_prim(const double* prim, long long n, int nv, unsigned long long* bad, cudaStream_t s) {
+  long long g = (n + 255) / 256;
+  if (g > 148LL * 8) g = 148LL * 8;
+  k_check_prim<<<(int)(g < 1 ? 1 : g), 256, 0, s>>>(prim, n, nv, bad);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_end_step(const ProbDev* prob, ProbState* st, int nprob, cudaStream_t s) {
   k_end_step<<<(nprob + 127) / 128, 128, 0, s>>>(prob, st, nprob);
   return cudaGetLastError();
@@ -872,13 +896,17 @@ int dspw_upload_prim(dspw_handle* h, int p, const double* prim) {
   const dspw_desc& d = h->desc[p];
   long long n = ncells(d);
   int nv = d.model <= DSPW_BURGERS ? 1 : 5;
-  // positivity of the initial state (enflo/src/fv.cc:88-89 asserts it)
-  if (nv == 5)
-    for (long long c = 0; c < n; c++)
-      if (!(prim[c] > 0.0) || !(prim[4 * n + c] > 0.0)) return DSPW_ERR_NONPOSITIVE;
-  for (long long c = 0; c < n * nv; c++)
-    if (!std::isfinite(prim[c])) return DSPW_ERR_NONFINITE;
   CK(cudaMemcpyAsync(h->dstage, prim, sizeof(double) * nv * n, cudaMemcpyHostToDevice, h->stream));
+  // positivity (enflo/src/fv.cc:88-89 asserts it) and finiteness, checked on
+  // the staged copy before the state is touched
+  unsigned long long* bad = (unsigned long long*)h->dscratch;
+  unsigned long long hb[2] = {0, 0};
+  CK(cudaMemsetAsync(bad, 0, sizeof(hb), h->stream));
+  CK(launch_check_prim(h->dstage, n, nv, bad, h->stream));
+  CK(cudaMemcpyAsync(hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (hb[0]) return DSPW_ERR_NONPOSITIVE;
+  if (hb[1]) return DSPW_ERR_NONFINITE;
   ProbState s;
   memset(&s, 0, sizeof(s));
   s.time = 0.0;

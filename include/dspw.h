@@ -157,7 +157,10 @@ DSPW_API int dspw_create(const dspw_desc* desc, dspw_handle** out);
 DSPW_API int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out);
 DSPW_API int dspw_destroy(dspw_handle* h);
 
-/* Interior primitive state of problem p in, conserved/primitive state out. */
+/* Interior primitive state of problem p in, conserved/primitive state out.
+ * dspw_upload_prim checks the state on the device after the copy: density or
+ * pressure <= 0 (or NaN) gives DSPW_ERR_NONPOSITIVE, another non-finite value
+ * DSPW_ERR_NONFINITE, and the problem keeps its previous state. */
 DSPW_API int dspw_upload_prim(dspw_handle* h, int p, const double* prim);
 DSPW_API int dspw_download_prim(dspw_handle* h, int p, double* prim);
 DSPW_API int dspw_download_cons(dspw_handle* h, int p, double* cons);

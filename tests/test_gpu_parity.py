@@ -279,3 +279,25 @@ def test_tune_keeps_results_and_state():
         assert np.array_equal(a.cons(p), b.cons(p)), p
     # the timing runs leave the status counters (read-and-clear) untouched
     assert a.status().faces_checked == b.status().faces_checked
+
+
+def test_upload_rejects_bad_states():
+    """dspw_upload_prim checks positivity (enflo/src/fv.cc:88-89) and
+    finiteness on the device before it touches the state: the error codes of
+    a host check, in the same order, and the previous state is kept."""
+    from dspw.capi import DspwError
+    name, kind, cfg, _, _ = next(c for c in run_cases() if c[0] == "kh_sp_weno")
+    p0 = load("runs.npz")[f"{name}|prim0"]
+    _, nz, ny, nx = p0.shape
+    s = Solver(desc_from_cfg(cfg, nx, ny, nz))
+    s.upload_prim(p0)
+    c0 = s.cons()
+    for comp, val, code in ((0, -1.0, 4), (4, 0.0, 4), (0, np.nan, 4), (1, np.nan, 3), (2, np.inf, 3)):
+        bad = p0.copy()
+        bad[comp, 0, 3, 5] = val
+        with pytest.raises(DspwError) as e:
+            s.upload_prim(bad)
+        assert e.value.code == code, (comp, val, e.value.code)
+        np.testing.assert_array_equal(s.cons(), c0)
+    s.upload_prim(p0)
+    np.testing.assert_array_equal(s.cons(), c0)
