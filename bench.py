@@ -210,9 +210,14 @@ def build_workload(args, precision, recon, rank, world):
 def kernel_class(d, dim):
     """Sweep kernel class of a problem (the library's spec_of): Euler / NS with a
     kepes_tecno4 flux run the kernels specialised for their dimension and
-    reconstruction family (10 * dim + 1 SP-WENO, + 2 DSP-WENO), others class 0."""
+    reconstruction family (10 * dim + 1 SP-WENO, + 2 DSP-WENO), 1-D scalar
+    problems the scalar kernel (100 + 1 or 2), others class 0."""
     from dspw import FLUX, RECON
-    if d.model in (0, 1) or d.flux not in (FLUX["kepes_tecno4_roe"], FLUX["kepes_tecno4_rusanov"]):
+    if d.model in (0, 1):
+        if dim == 1 and d.recon < RECON["first"]:
+            return 100 + (2 if d.recon == RECON["sp_weno_dl"] else 1)
+        return 0
+    if d.flux not in (FLUX["kepes_tecno4_roe"], FLUX["kepes_tecno4_rusanov"]):
         return 0
     return 10 * dim + (2 if d.recon == RECON["sp_weno_dl"] else 1)
 

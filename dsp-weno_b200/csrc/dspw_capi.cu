@@ -353,7 +353,9 @@ NetParams make_net(const dspw_desc& dn) {
 // dimension and reconstruction family; every other problem the generic ones.
 int spec_of(const ProbDev& P, const dspw_desc& d) {
   if (d.reserved_i[1] == 1) return 0;   // generic kernels requested
-  if (P.is_scalar || P.central != 0 || !P.fourth || !P.tecno || P.recon >= DSPW_REC_FIRST) return 0;
+  if (P.is_scalar)   // 1-D linear advection / Burgers with an SP-WENO-family or network reconstruction
+    return (P.dim == 1 && P.recon < DSPW_REC_FIRST) ? scalar_spec_code(P.spw_corr < 0 ? 2 : 1) : 0;
+  if (P.central != 0 || !P.fourth || !P.tecno || P.recon >= DSPW_REC_FIRST) return 0;
   return spec_code(P.dim, P.spw_corr < 0 ? 2 : 1);
 }
 

@@ -77,6 +77,12 @@ struct SpecHot {
 };
 // host-side code of a specialisation: 0 generic, else 10 * dim + rec
 constexpr int spec_code(int dim, int rec) { return 10 * dim + rec; }
+// 1-D scalar problems (linear advection, Burgers) with the reconstruction
+// family rec fixed: k_sweep_scalar
+constexpr int scalar_spec_code(int rec) { return 100 + rec; }
+// resident blocks per SM of k_sweep_scalar: 64 registers per thread for FP32,
+// 128 for FP64 (the FP64 network forward spills at 64)
+template <typename T> struct ScalarMinBlocks { static constexpr int value = sizeof(T) == 8 ? 2 : 4; };
 
 struct ProbState {
   double time, dt, t_save, factor;
@@ -1289,7 +1295,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
 
 // scalar laws: lin_/bur_ fluxes (enflo_scalar/src_scalar/num_flux.cc:12-57,
 // lin_tecno4.cc:10-31, lin_ec4.cc:10-34, bur_tecno4.cc:10-35, bur_ec4.cc:10-34)
-template <typename T, int DIR>
+template <typename T, int DIR, typename Sp = SpecGeneric>
 __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S,
                             WarpSmem<T>* sm, int lane, int lt) {
   typedef Mth<T> m;
@@ -1337,7 +1343,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   if (P.tecno) {
     T D = (P.model == DSPW_LINADV) ? m::abs(vn) : T(0.5) * (m::abs(s1) + m::abs(s2));
     T l = T(0), r = T(0);
-    reconstruct_lane<T, SpecGeneric>(P, *A.net, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
+    reconstruct_lane<T, Sp>(P, *A.net, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
     if (valid && sign_violation<T>(s0, s1, s2, s3, l, r)) signv++;
     if (A.collect_buf && valid) collect_pair<T>(A, (unsigned)lt * 32u + (unsigned)lane, s0, s1, s2, s3, l, r);
     flux -= T(0.5) * D * (r - l);
@@ -1431,6 +1437,29 @@ k_sweep(SweepArgs<T> A) {
         }
       }
     }
+  }
+}
+
+// The x sweep of 1-D scalar problems alone: the reconstruction family fixed at
+// compile time (REC 1: SP-WENO, the correction a run-time flag; 2: DSP-WENO),
+// none of the Euler code of the generic kernel, and its own register budget.
+template <typename T, int REC>
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, ScalarMinBlocks<T>::value)
+k_sweep_scalar(SweepArgs<T> A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem<T>* sm = reinterpret_cast<WarpSmem<T>*>(smem_raw) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (REC == 2) net_frag_stage<T>(*A.net, lane, sm->ns);
+  const int stride = gridDim.x * WARPS_PER_BLOCK;
+  for (int base = blockIdx.x * WARPS_PER_BLOCK; base < A.ntask; base += stride) {
+    const int task = base + (threadIdx.x >> 5);
+    if (task >= A.ntask) continue;
+    const int p = find_problem(A.task_start, A.nprob, task);
+    const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+    const ProbDev& P = A.prob[pp];
+    ProbState& S = A.st[pp];
+    if (!A.residual_only && !*((volatile int*)&S.active)) continue;
+    scalar_task<T, 0, SpecHot<1, REC>>(A, P, S, sm, lane, task - __ldg(A.task_start + p));
   }
 }
 

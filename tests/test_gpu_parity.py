@@ -301,3 +301,33 @@ def test_upload_rejects_bad_states():
         np.testing.assert_array_equal(s.cons(), c0)
     s.upload_prim(p0)
     np.testing.assert_array_equal(s.cons(), c0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_bf16"])
+@pytest.mark.parametrize("model,flux", [("burgers", "bur_tecno4"), ("linadv", "lin_tecno4"), ("burgers", "bur_ec")])
+@pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_dl"])
+def test_scalar_kernel_equals_generic(precision, model, flux, recon):
+    """1-D scalar problems run k_sweep_scalar (reconstruction family fixed at
+    compile time); with reserved_i[1] = 1 they run the generic kernel.  Two
+    problems of different sizes and boundary conditions in one batch: FP64
+    gives the same bits, FP32 agrees to rounding."""
+    rng = np.random.default_rng(5)
+    kw = dict(model=model, flux=flux, recon=recon, network=net(), precision=precision, x=(-1, 1))
+    shapes = [(97, "periodic"), (150, ["wall", "neumann", "periodic", "periodic", "periodic", "periodic"])]
+    states = [rng.uniform(-1, 1, size=(1, 1, 1, nx)) + 0.2 for nx, _ in shapes]
+    out = []
+    for generic in (False, True):
+        ds = [make_desc(nx=nx, ny=1, nz=1, bc=bc, **kw) for nx, bc in shapes]
+        for d in ds:
+            d.reserved_i[1] = int(generic)
+        s = Solver(ds)
+        for p, st in enumerate(states):
+            s.upload_prim(st, p)
+        s.step(12)
+        assert s.status().code == 0 and s.status().sign_violations == 0
+        out.append([s.cons(p) for p in range(2)])
+    for a, b in zip(*out):
+        if precision == "fp64":
+            assert np.array_equal(a, b)
+        else:
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-4 * np.max(np.abs(b)))
