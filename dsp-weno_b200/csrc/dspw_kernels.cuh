@@ -681,18 +681,20 @@ __device__ inline void warp_mlp_bf16(NetScratch<float>& ns, const float in[5], f
 // to act (FP32 form).
 template <typename T>
 __device__ inline int dsp_weno_warp(const NetParams& NP, WarpSmem<T>* sm, int lane, bool valid,
-                                    T u0, T u1, T u2, T u3, T& l, T& r);
+                                    T u0, T u1, T u2, T u3, T& l, T& r, unsigned long long& signv);
 
 template <>
 __device__ inline int dsp_weno_warp<double>(const NetParams& NP, WarpSmem<double>*, int, bool valid,
-                                            double u0, double u1, double u2, double u3, double& l, double& r) {
+                                            double u0, double u1, double u2, double u3, double& l, double& r,
+                                            unsigned long long&) {
   if (valid) dsp_weno_fp64(NP, u0, u1, u2, u3, l, r);
   return 0;
 }
 
 template <>
 __device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>* sm, int lane,
-                                           bool valid, float u0, float u1, float u2, float u3, float& l, float& r) {
+                                           bool valid, float u0, float u1, float u2, float u3, float& l, float& r,
+                                           unsigned long long& signv) {
   // The reference skips the network when |u2 - u1| < 1e-15 (reconstruct.cc:152);
   // in FP32 the equivalent "no jump" test is a jump of a few ulps of the values,
   // below which the scaled differences of the features are rounding noise.
@@ -720,6 +722,7 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>*
   if (guard) { l = 0.f; r = 0.f; return 0; }
   if (!finite || !inbox) {   // degenerate features or outside the training range: plain SP-WENO
     sp_weno<float>(u0, u1, u2, u3, 0, l, r);
+    if (sign_violation<float>(u0, u1, u2, u3, l, r)) signv++;   // not limited: checked here
     return 0;
   }
   nn_finish<float>(lg, vx, vy, u0, u1, u2, u3, l, r);
@@ -734,15 +737,31 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>*
   return 0;
 }
 
+// The FP32 network path ends in a sign-preserving limiter that tests the same
+// two jumps (dsp_weno_warp<float>), so there the property holds by
+// construction and the caller does not re-check it; the path's SP-WENO
+// fallback faces, which are not limited, are checked inside it.  SP-WENO, the
+// lower-order reconstructions and the FP64 (unlimited) network are checked by
+// the caller.
+template <typename T, typename Sp>
+__device__ __forceinline__ bool sign_checked(const ProbDev& P) {
+  if constexpr (sizeof(T) == 4) {
+    if constexpr (Sp::fixed) return Sp::rec != 2;
+    else return !(P.recon < DSPW_REC_FIRST && P.spw_corr < 0);
+  }
+  return true;
+}
+
 template <typename T, typename Sp>
 __device__ inline void reconstruct_lane(const ProbDev& P, const NetParams& NP, WarpSmem<T>* sm,
-                                        int lane, bool valid, T s0, T s1, T s2, T s3, T& l, T& r, int& viol) {
+                                        int lane, bool valid, T s0, T s1, T s2, T s3, T& l, T& r, int& viol,
+                                        unsigned long long& signv) {
   if (!Sp::fixed && P.recon >= DSPW_REC_FIRST) {
     if (valid) simple_recon<T>(P.recon, s0, s1, s2, s3, l, r);
   } else if (Sp::fixed ? Sp::rec == 1 : P.spw_corr >= 0) {
     if (valid) sp_weno<T>(s0, s1, s2, s3, P.spw_corr, l, r);
   } else {
-    viol += dsp_weno_warp<T>(NP, sm, lane, valid, s0, s1, s2, s3, l, r);
+    viol += dsp_weno_warp<T>(NP, sm, lane, valid, s0, s1, s2, s3, l, r, signv);
   }
 }
 
@@ -816,12 +835,12 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
       z[k] = T(0.0) + acc;
     }
     T zl = T(0), zr = T(0);
-    reconstruct_lane<T, Sp>(P, NP, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol);
+    reconstruct_lane<T, Sp>(P, NP, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol, signv);
     if (A.collect_buf && valid)
       collect_pair<T>(A, (unsigned)(blockIdx.x * 1024 + threadIdx.x) * 8u + (unsigned)j + 977u * collect_salt,
                       z[0], z[1], z[2], z[3], zl, zr);
     T dZ = zr - zl;
-    if (valid && sign_violation<T>(z[0], z[1], z[2], z[3], zl, zr)) signv++;
+    if (valid && sign_checked<T, Sp>(P) && sign_violation<T>(z[0], z[1], z[2], z[3], zl, zr)) signv++;
     T ld = j == 0 ? Lam[0] : (j == 1 ? Lam[1] : (j == 2 ? Lam[2] : (j == 3 ? Lam[3] : Lam[4])));
 #pragma unroll
     for (int i = 0; i < 5; i++) Diff[i] += col[i] * ld * dZ;
@@ -1343,8 +1362,8 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   if (P.tecno) {
     T D = (P.model == DSPW_LINADV) ? m::abs(vn) : T(0.5) * (m::abs(s1) + m::abs(s2));
     T l = T(0), r = T(0);
-    reconstruct_lane<T, Sp>(P, *A.net, sm, lane, valid, s0, s1, s2, s3, l, r, viol);
-    if (valid && sign_violation<T>(s0, s1, s2, s3, l, r)) signv++;
+    reconstruct_lane<T, Sp>(P, *A.net, sm, lane, valid, s0, s1, s2, s3, l, r, viol, signv);
+    if (valid && sign_checked<T, Sp>(P) && sign_violation<T>(s0, s1, s2, s3, l, r)) signv++;
     if (A.collect_buf && valid) collect_pair<T>(A, (unsigned)lt * 32u + (unsigned)lane, s0, s1, s2, s3, l, r);
     flux -= T(0.5) * D * (r - l);
   }
@@ -1865,7 +1884,8 @@ k_recon_batch(const ProbDev* prob, const NetParams* net, const double* u4, long 
     T s2 = valid ? T(u4[4 * i + 2]) : T(2), s3 = valid ? T(u4[4 * i + 3]) : T(3);
     T lo = T(0), ro = T(0);
     int viol = 0;
-    reconstruct_lane<T, SpecGeneric>(*prob, *net, sm, lane, valid, s0, s1, s2, s3, lo, ro, viol);
+    unsigned long long signv = 0;   // not reported by this entry point
+    reconstruct_lane<T, SpecGeneric>(*prob, *net, sm, lane, valid, s0, s1, s2, s3, lo, ro, viol, signv);
     if (valid) { l[i] = (double)lo; r[i] = (double)ro; }
     unsigned v = __reduce_add_sync(0xffffffffu, (unsigned)viol);
     if (lane == 0 && v) atomicAdd(acts, (unsigned long long)v);
