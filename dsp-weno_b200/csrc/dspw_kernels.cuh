@@ -1710,6 +1710,19 @@ __device__ inline void visc_node_ke(const ProbDev& P, const T* V, long long ctot
   }
 }
 
+// (i, j, k) of cell l of a problem (x fastest): 32-bit divisions when the
+// problem has fewer than 2^32 cells (every problem that fits in memory)
+DSPW_HD void cell_ijk(const ProbDev& P, long long l, int& i, int& j, int& k) {
+  const long long nxy = (long long)P.nx * P.ny;
+  if (nxy * P.nz <= 0xffffffffLL) {
+    const unsigned u = (unsigned)l, nx = (unsigned)P.nx, n2 = (unsigned)nxy;
+    const unsigned kk = u / n2, r = u - kk * n2, jj = r / nx;
+    i = (int)(r - jj * nx); j = (int)jj; k = (int)kk;
+  } else {
+    i = (int)(l % P.nx); j = (int)((l / P.nx) % P.ny); k = (int)(l / nxy);
+  }
+}
+
 template <typename T>
 __global__ void k_visc_nodes(const ProbDev* prob, int nprob, const long long* cell_start, const T* V, long long ctot,
                              T* node) {
@@ -1720,9 +1733,9 @@ __global__ void k_visc_nodes(const ProbDev* prob, int nprob, const long long* ce
     while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_start[mid] <= g) lo = mid; else hi = mid - 1; }
     const ProbDev& P = prob[lo];
     if (P.model != DSPW_NS_ES && P.model != DSPW_NS_KEP) continue;
-    long long l = g - P.off;
-    int i = (int)(l % P.nx), j = (int)((l / P.nx) % P.ny), k = (int)(l / ((long long)P.nx * P.ny));
-    int i1 = (i + 1) % P.nx, j1 = (j + 1) % P.ny, k1 = (k + 1) % P.nz;
+    int i, j, k;
+    cell_ijk(P, g - P.off, i, j, k);
+    const int i1 = i + 1 == P.nx ? 0 : i + 1, j1 = j + 1 == P.ny ? 0 : j + 1, k1 = k + 1 == P.nz ? 0 : k + 1;
     if (P.model == DSPW_NS_KEP) {
       visc_node_ke<T>(P, V, ctot, node, g, i, j, k, i1, j1, k1);
       continue;
@@ -1807,8 +1820,8 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
     ProbState& S = A.st[lo];
     if (!A.residual_only && !S.active) continue;
     pcur = lo;
-    long long l = g - P.off;
-    int I = (int)(l % P.nx), J = (int)((l / P.nx) % P.ny), K = (int)(l / ((long long)P.nx * P.ny));
+    int I, J, K;
+    cell_ijk(P, g - P.off, I, J, K);
     T R[5];
     load_cons<T>(A.R, A.ctot, g, P.nv, P.dim, R);
 #pragma unroll
@@ -1821,7 +1834,8 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
           int ni = I - 1 + a, nj = J - 1 + b, nk = K - 1 + c;
           int onb = (ni == -1 || ni == P.nx - 1) + (nj == -1 || nj == P.ny - 1) + (nk == -1 || nk == P.nz - 1);
           int mult = (onb == 2) ? 2 : 1;
-          int pi = (ni + P.nx) % P.nx, pj = (nj + P.ny) % P.ny, pk = (nk + P.nz) % P.nz;
+          // periodic node index (ni in -1 .. nx-1)
+          const int pi = ni < 0 ? ni + P.nx : ni, pj = nj < 0 ? nj + P.ny : nj, pk = nk < 0 ? nk + P.nz : nk;
           long long ng = P.off + ((long long)pk * P.ny + pj) * P.nx + pi;
           const T cx = a ? T(0.25) : T(-0.25), cy = b ? T(0.25) : T(-0.25), cz = c ? T(0.25) : T(-0.25);
           for (int rep = 0; rep < mult; rep++) {
