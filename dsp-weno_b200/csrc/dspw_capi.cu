@@ -36,7 +36,9 @@ __global__ void k_begin_step_wrap(const ProbDev* prob, ProbState* st, int nprob,
   if (fixed_dt > 0) {
     dt = fixed_dt;
   } else {
-    double smax = __longlong_as_double((long long)S.smax);
+    unsigned long long sb = 0ull;   // max over the slots (ordered bits of non-negative speeds)
+    for (int k = 0; k < EPI_SLOTS; k++) sb = S.smax[k] > sb ? S.smax[k] : sb;
+    double smax = __longlong_as_double((long long)sb);
     dt = 1.0e20;
     double c = P.hmin / smax;
     if (c < dt) dt = c;
@@ -45,7 +47,17 @@ __global__ void k_begin_step_wrap(const ProbDev* prob, ProbState* st, int nprob,
   if (S.time + dt > S.t_save) dt = S.t_save - S.time;
   S.dt = dt;
   S.factor = dt / (P.dx * P.dy * P.dz);
-  S.smax = 0ull;
+  for (int k = 0; k < EPI_SLOTS; k++) {
+    S.smax[k] = 0ull;
+    S.ent_acc[k] = 0.0;
+  }
+}
+
+// sum of the entropy slots of a problem
+__device__ inline double ent_sum(const ProbState& S) {
+  double e = 0.0;
+  for (int k = 0; k < EPI_SLOTS; k++) e += S.ent_acc[k];
+  return e;
 }
 
 cudaError_t launch_begin_step(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive,
@@ -66,6 +78,21 @@ __global__ void k_end_step(const ProbDev* prob, ProbState* st, int nprob) {
   const int stamp = S.time == S.t_save;   // output time stamp (fv.cc:1309-1313)
   if (stamp) S.t_save += prob[p].t_interval;
   S.snap = stamp;
+  // discrete entropy inequality: relative change of the total entropy
+  const double e = ent_sum(S) * prob[p].vol;
+  const double rise = (e - S.ent) / fabs(S.ent);
+  if (rise > S.ent_max_rise) S.ent_max_rise = rise;
+  S.ent = e;
+  S.ent_steps += 1;
+}
+
+// total entropy of an uploaded state; the inequality's record starts anew
+__global__ void k_init_entropy(const ProbDev* prob, ProbState* st, int p) {
+  ProbState& S = st[p];
+  S.ent = ent_sum(S) * prob[p].vol;
+  for (int k = 0; k < EPI_SLOTS; k++) S.ent_acc[k] = 0.0;
+  S.ent_max_rise = -1.0e300;
+  S.ent_steps = 0;
 }
 
 
@@ -920,7 +947,19 @@ int dspw_upload_prim(dspw_handle* h, int p, const double* prim) {
     CK(Launch<double>::upload(h->dprob, h->dst, p, h->dstage, (double*)h->Un, h->ctot, n, h->stream));
   else
     CK(Launch<float>::upload(h->dprob, h->dst, p, h->dstage, (float*)h->Un, h->ctot, n, h->stream));
+  k_init_entropy<<<1, 1, 0, h->stream>>>(h->dprob, h->dst, p);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));
+  return DSPW_OK;
+}
+
+int dspw_entropy_check(dspw_handle* h, int p, double* max_rise, long long* steps) {
+  if (check_p(h, p) || !max_rise) return DSPW_ERR_ARG;
+  ProbState s;
+  CK(cudaMemcpyAsync(&s, h->dst + p, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *max_rise = s.ent_max_rise;
+  if (steps) *steps = s.ent_steps;
   return DSPW_OK;
 }
 

@@ -84,9 +84,19 @@ constexpr int scalar_spec_code(int rec) { return 100 + rec; }
 // 128 for FP64 (the FP64 network forward spills at 64)
 template <typename T> struct ScalarMinBlocks { static constexpr int value = sizeof(T) == 8 ? 2 : 4; };
 
+// The per-step reductions of a problem (wave-speed max, entropy sum) go to
+// EPI_SLOTS slots picked by block index, so that the one atomic per warp of
+// the sweeps does not queue on a single address; the step kernels combine them.
+constexpr int EPI_SLOTS = 16;
+
 struct ProbState {
   double time, dt, t_save, factor;
-  unsigned long long smax;   // bits of the max wave speed of the newest state
+  unsigned long long smax[EPI_SLOTS];   // bits of the max wave speed of the newest state
+  // discrete entropy inequality: total entropy of the newest state, the sum
+  // of the step being built, the largest relative one-step rise, steps checked
+  double ent, ent_max_rise;
+  double ent_acc[EPI_SLOTS];
+  long long ent_steps;
   int iter, active;
   int snap;                  // 1: this step ended on an output time stamp
   int pad;
@@ -947,7 +957,7 @@ __device__ inline void stage_combine(const SweepArgs<T>& A, const ProbDev& P, co
 // that yields U^(n+1).
 template <typename T>
 __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
-                                         const T R[5], T u[5], const T un[5], double& smax,
+                                         const T R[5], T u[5], const T un[5], double& smax, T& ent,
                                          unsigned& bad_fin, unsigned& bad_pos) {
   stage_combine<T>(A, P, S, cell, R, u, un);
   store_cons<T>(A.Uout, A.ctot, cell, P.nv, u);
@@ -960,6 +970,9 @@ __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P
     double rho = p[0], pr = p[4];
     if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
     if (!isfinite(rho) || !isfinite(pr) || !isfinite((double)u[1]) || !isfinite((double)u[4])) bad_fin++;
+    // entropy -rho s / (gamma - 1), s = ln p - gamma ln rho, in the state's type
+    const T sT = Mth<T>::log(p[4]) - T(P.gamma) * Mth<T>::log(p[0]);
+    ent += -p[0] * sT / T(P.gamma - 1.0);
   }
 }
 
@@ -970,7 +983,7 @@ __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P
 template <typename T>
 __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
                                    bool first, bool final_sweep, const T Fl[5], const T Fr[5], int nv_eff,
-                                   double& smax, unsigned& bad_fin, unsigned& bad_pos) {
+                                   double& smax, T& ent, unsigned& bad_fin, unsigned& bad_pos) {
   T R[5];
   if (first) {
 #pragma unroll
@@ -1014,24 +1027,30 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
       T pp[5] = {x, T(0), T(0), T(0), T(0)};
       double sp = wave_speed<T>(P, pp);
       if (sp > smax) smax = sp;   // NaN speeds are skipped, as std::min skips them in compute_dt
+      ent += T(0.5) * x * x;   // entropy u^2 / 2
       if (!isfinite((double)x)) bad_fin++;
     }
     return;
   }
   load_cons<T>(A.Uin, A.ctot, cell, P.nv, P.dim, u);
   load_cons<T>(A.Un, A.ctot, cell, P.nv, P.dim, un);
-  update_euler_cell<T>(A, P, S, cell, R, u, un, smax, bad_fin, bad_pos);
+  update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
   (void)a; (void)c2; (void)nv_eff;
 }
 
 template <typename T>
-__device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax,
+__device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax, T ent,
                                      unsigned bad_fin, unsigned bad_pos, unsigned long long signv, int viol,
                                      unsigned checked) {
   if (A.final_stage && !A.residual_only) {
     unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
     warp_max_u64_lane0(sb);
-    if (lane == 0) atomicMax(&S.smax, sb);
+    const double es = warp_sum((double)ent);
+    if (lane == 0) {
+      const int sl = blockIdx.x & (EPI_SLOTS - 1);
+      atomicMax(&S.smax[sl], sb);
+      atomicAdd(&S.ent_acc[sl], es);
+    }
   }
   unsigned bf = __reduce_add_sync(0xffffffffu, bad_fin);
   unsigned bp = __reduce_add_sync(0xffffffffu, bad_pos);
@@ -1126,18 +1145,19 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
   double smax = 0.0;
+  T ent = T(0);
   unsigned bad_fin = 0, bad_pos = 0;
   if (lane < ncell) {
     T Fl[5], Fr[5];
 #pragma unroll
     for (int v = 0; v < 5; v++) { Fl[v] = sm->F[v][lane]; Fr[v] = sm->F[v][lane + 1]; }
     long long cell = cell_index<DIR>(P, i0, j0, k0, c0 + lane);
-    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, P.nv, smax, bad_fin, bad_pos);
+    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, P.nv, smax, ent, bad_fin, bad_pos);
   }
-  if (!final_sweep) smax = 0.0;
+  if (!final_sweep) { smax = 0.0; ent = T(0); }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, bad_fin, bad_pos, signv, viol, checked);
+  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
   __syncwarp();
 }
 
@@ -1288,6 +1308,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   if (aligned) cp_async_wait<0>();
   __syncthreads();
   double smax = 0.0;
+  T ent = T(0);
   unsigned bad_fin = 0, bad_pos = 0;
   for (int row = tid / COOP_COLS; row < ncell && col < ncols; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
     WarpSmem<T>* sc = sm0 + col;
@@ -1302,13 +1323,13 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
       T u[5], un[5];
       tile_cons<T>(tl.U, nv, row + 2, col, u);
       tile_cons<T>(tl.Un, nv, row, col, un);
-      update_euler_cell<T>(A, P, S, cell, R, u, un, smax, bad_fin, bad_pos);
+      update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
     }
   }
-  if (!final_sweep) smax = 0.0;
+  if (!final_sweep) { smax = 0.0; ent = T(0); }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, bad_fin, bad_pos, signv, viol, checked);
+  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
   __syncthreads();
 }
 
@@ -1373,16 +1394,17 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && (DIR == P.dim - 1);
   double smax = 0.0;
+  T ent = T(0);
   unsigned bad_fin = 0, bad_pos = 0;
   if (lane < ncell) {
     T Fl[5] = {sm->F[0][lane], T(0), T(0), T(0), T(0)};
     T Fr[5] = {sm->F[0][lane + 1], T(0), T(0), T(0), T(0)};
     long long cell = cell_index<DIR>(P, i0, j0, k0, c0 + lane);
-    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, 1, smax, bad_fin, bad_pos);
+    finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, 1, smax, ent, bad_fin, bad_pos);
   }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, bad_fin, bad_pos, signv, viol, (P.tecno && valid) ? 1u : 0u);
+  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, (P.tecno && valid) ? 1u : 0u);
   __syncwarp();
 }
 
@@ -1485,19 +1507,23 @@ k_sweep_scalar(SweepArgs<T> A) {
 // ----------------------------------------------------------- step control --
 
 // upload: primitive (FP64, staging) -> conserved state, plus the wave speed of
-// that primitive state (prim_to_con, enflo/src/fv.cc:405-416)
+// that primitive state (prim_to_con, enflo/src/fv.cc:405-416) and the sum of
+// its entropy (in the state's type, as the steps take it)
 template <typename T>
 __global__ void k_upload(const ProbDev* prob, ProbState* st, int p, const double* prim, T* U, long long ctot) {
   const ProbDev& P = prob[p];
   ProbState& S = st[p];
   long long n = (long long)P.nx * P.ny * P.nz;
   double smax = 0.0;
+  double ent = 0.0;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     if (P.is_scalar) {
       double u = prim[c];
       U[P.off + c] = T(u);
       double sp = (P.model == DSPW_LINADV) ? P.lin_speed : fabs(u);
       if (sp > smax) smax = sp;
+      const double ut = (double)T(u);
+      ent += 0.5 * ut * ut;
     } else {
       double pd[5];
       for (int v = 0; v < 5; v++) pd[v] = prim[v * n + c];
@@ -1507,11 +1533,18 @@ __global__ void k_upload(const ProbDev* prob, ProbState* st, int p, const double
       store_cons<T>(U, ctot, P.off + c, P.nv, u);
       double sp = wave_speed<double>(P, pd);
       if (sp > smax) smax = sp;
+      const T sT = Mth<T>::log(pp[4]) - T(P.gamma) * Mth<T>::log(pp[0]);
+      ent += (double)(-pp[0] * sT / T(P.gamma - 1.0));
     }
   }
   unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
   warp_max_u64_lane0(sb);
-  if ((threadIdx.x & 31) == 0) atomicMax(&S.smax, sb);
+  const double es = warp_sum(ent);
+  if ((threadIdx.x & 31) == 0) {
+    const int sl = blockIdx.x & (EPI_SLOTS - 1);
+    atomicMax(&S.smax[sl], sb);
+    atomicAdd(&S.ent_acc[sl], es);
+  }
 }
 
 // wave-speed max of the current state (dspw_compute_dt)
@@ -1810,6 +1843,7 @@ template <typename T>
 __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const T* node) {
   long long total = cell_start[A.nprob];
   double smax = 0.0;
+  T ent = T(0);
   unsigned bad_fin = 0, bad_pos = 0;
   int pcur = -1;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
@@ -1859,19 +1893,28 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
       double rho = p[0], pr = p[4];
       if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
       if (!isfinite(rho) || !isfinite(pr)) bad_fin++;
+      const T sT = Mth<T>::log(p[4]) - T(P.gamma) * Mth<T>::log(p[0]);
+      ent += -p[0] * sT / T(P.gamma - 1.0);
     }
   }
-  // one speed-max flush per thread, warp-aggregated when the warp worked on a
-  // single problem
+  // one speed-max and entropy flush per thread, warp-aggregated when the warp
+  // worked on a single problem
   int p0 = __shfl_sync(0xffffffffu, pcur, 0);
   bool uniform = __all_sync(0xffffffffu, pcur == p0 || pcur < 0);
   if (A.final_stage && !A.residual_only) {
     if (uniform) {
       unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
       warp_max_u64_lane0(sb);
-      if ((threadIdx.x & 31) == 0 && p0 >= 0) atomicMax(&A.st[p0].smax, sb);
+      const double es = warp_sum((double)ent);
+      if ((threadIdx.x & 31) == 0 && p0 >= 0) {
+        const int sl = blockIdx.x & (EPI_SLOTS - 1);
+        atomicMax(&A.st[p0].smax[sl], sb);
+        atomicAdd(&A.st[p0].ent_acc[sl], es);
+      }
     } else if (pcur >= 0) {
-      atomicMax(&A.st[pcur].smax, (unsigned long long)__double_as_longlong(smax));
+      const int sl = blockIdx.x & (EPI_SLOTS - 1);
+      atomicMax(&A.st[pcur].smax[sl], (unsigned long long)__double_as_longlong(smax));
+      atomicAdd(&A.st[pcur].ent_acc[sl], (double)ent);
     }
   }
   if (bad_fin) { atomicAdd(&A.status->nonfinite, (unsigned long long)bad_fin); atomicCAS(&A.status->code, 0, DSPW_ERR_NONFINITE); }

@@ -228,6 +228,7 @@ def lib():
         "dspw_globals_noalloc": (I, [C.POINTER(Desc), P, LL, I, P, P]),
         "dspw_profile_step": (I, [P, dp, C.c_char_p, I, C.POINTER(I)]),
         "dspw_tune": (I, [P, I, C.POINTER(D), C.POINTER(D)]),
+        "dspw_entropy_check": (I, [P, I, C.POINTER(D), C.POINTER(LL)]),
         "dspw_diag_enable": (I, [P, I]),
         "dspw_diag_pending": (I, [P, I, C.POINTER(I), C.POINTER(LL)]),
         "dspw_diag_read": (I, [P, I, dp, I, C.POINTER(I)]),
@@ -415,6 +416,13 @@ class Solver:
         s = C.c_int()
         check(lib().dspw_run(self.h, int(chunk), C.byref(s)), "dspw_run")
         return s.value
+
+    def entropy_check(self, p=0):
+        """(largest relative one-step rise of the total entropy since the
+        upload, steps checked) (dspw_entropy_check)."""
+        r, n = C.c_double(), C.c_longlong()
+        check(lib().dspw_entropy_check(self.h, p, C.byref(r), C.byref(n)), "dspw_entropy_check")
+        return r.value, n.value
 
     def diag_enable(self, capacity=256):
         """Record the per-step diagnostics rows (dspw_diag_enable); 0 stops."""

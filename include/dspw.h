@@ -239,6 +239,17 @@ DSPW_API int dspw_reconstruct_batch(const dspw_desc* desc, const double* u4, lon
 DSPW_API int dspw_globals_noalloc(const dspw_desc* desc, const void* d_cons, long long stride, int elem_bytes,
                                   double* d_out, void* stream);
 
+/* Discrete entropy inequality, checked every step on the device: the total
+ * entropy E = sum U(u) vol of each new state (U = -rho s / (gamma - 1) with
+ * s = ln p - gamma ln rho for systems, u^2 / 2 for scalar laws; the
+ * reference's compute_global, enflo/src/compute_global.cc:18-28,
+ * enflo_scalar/src_scalar/compute_global.cc:12-21), taken in the state's own
+ * arithmetic type, against the state before the step.  *max_rise is the
+ * largest relative one-step increase (E_{n+1} - E_n) / |E_n| since the last
+ * upload (negative when E only fell), *steps (may be NULL) the steps checked.
+ * An entropy-stable TeCNO run keeps *max_rise at rounding level. */
+DSPW_API int dspw_entropy_check(dspw_handle* h, int p, double* max_rise, long long* steps);
+
 /* ---- per-step diagnostics ----------------------------------------------
  * The global quantities FV::run computes every step, evaluated on the device
  * inside the step graph and kept in a device ring of `capacity` rows per

@@ -331,3 +331,41 @@ def test_scalar_kernel_equals_generic(precision, model, flux, recon):
             assert np.array_equal(a, b)
         else:
             np.testing.assert_allclose(a, b, rtol=0, atol=1e-4 * np.max(np.abs(b)))
+
+
+def test_entropy_inequality_checked_every_step():
+    """dspw_entropy_check: the device records, every step, the relative change
+    of the total entropy; its largest rise equals the one computed from the
+    total entropy of each step's state (dspw_globals, FP64), and entropy-stable
+    TeCNO runs keep it at rounding level (the entropy falls)."""
+    name, kind, cfg, _, _ = next(c for c in run_cases() if c[0] == "kh_sp_weno")
+    p0 = load("runs.npz")[f"{name}|prim0"]
+    _, nz, ny, nx = p0.shape
+    s = Solver(desc_from_cfg(cfg, nx, ny, nz))
+    s.upload_prim(p0)
+    e = [s.globals().total_entropy]
+    for _ in range(10):
+        s.step(1)
+        e.append(s.globals().total_entropy)
+    rises = [(e[i + 1] - e[i]) / abs(e[i]) for i in range(10)]
+    got, steps = s.entropy_check()
+    assert steps == 10
+    assert abs(got - max(rises)) <= 1e-12, (got, max(rises))
+    assert got < 1e-12
+    # FP32 + BF16 DSP-WENO: the same bookkeeping in the FP32 state's arithmetic
+    d = make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno_dl", nx=64, ny=64, nz=1, network=net(),
+                  precision="fp32_bf16")
+    rng = np.random.default_rng(3)
+    st = random_state(rng, 64, 64, 1)
+    s32 = Solver(d)
+    s32.upload_prim(st)
+    s32.step(20)
+    got32, steps32 = s32.entropy_check()
+    assert steps32 == 20 and got32 < 1e-5, got32
+    # scalar entropy u^2/2 of an entropy-stable Burgers flux
+    db = make_desc(model="burgers", flux="bur_tecno4", recon="sp_weno", nx=200, ny=1, nz=1, x=(-np.pi, np.pi))
+    sb = Solver(db)
+    sb.upload_prim((0.5 + np.sin(np.linspace(-np.pi, np.pi, 200, endpoint=False))).reshape(1, 1, 1, 200))
+    sb.step(30)
+    gotb, stepsb = sb.entropy_check()
+    assert stepsb == 30 and gotb < 1e-12, gotb
