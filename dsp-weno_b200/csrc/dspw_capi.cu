@@ -1223,8 +1223,12 @@ int dspw_last_status(dspw_handle* h, dspw_status_out* s) {
   s->nonfinite_cells = (long long)d.nonfinite;
   s->nonpositive_cells = (long long)d.nonpositive;
   s->sign_violations = (long long)d.sign_viol;
-  s->faces_checked = (long long)d.faces_checked;
-  s->limiter_acts = (long long)d.limiter_acts;
+  s->faces_checked = 0;
+  s->limiter_acts = 0;
+  for (int k = 0; k < EPI_SLOTS; k++) {
+    s->faces_checked += (long long)d.faces_checked[k];
+    s->limiter_acts += (long long)d.limiter_acts[k];
+  }
   h->last_error = 0;
   return DSPW_OK;
 }

@@ -105,7 +105,9 @@ struct ProbState {
 struct StatusDev {
   int code;
   int pad;
-  unsigned long long nonfinite, nonpositive, sign_viol, faces_checked, limiter_acts;
+  unsigned long long nonfinite, nonpositive, sign_viol;
+  // incremented by nearly every warp of every sweep: slots by block index
+  unsigned long long faces_checked[EPI_SLOTS], limiter_acts[EPI_SLOTS];
 };
 
 template <typename T>
@@ -1058,11 +1060,12 @@ __device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int la
   unsigned vv = __reduce_add_sync(0xffffffffu, (unsigned)viol);
   unsigned ck = __reduce_add_sync(0xffffffffu, checked);
   if (lane == 0) {
-    if (ck) atomicAdd(&A.status->faces_checked, (unsigned long long)ck);
+    const int sl = blockIdx.x & (EPI_SLOTS - 1);
+    if (ck) atomicAdd(&A.status->faces_checked[sl], (unsigned long long)ck);
     if (bf) { atomicAdd(&A.status->nonfinite, (unsigned long long)bf); atomicCAS(&A.status->code, 0, DSPW_ERR_NONFINITE); }
     if (bp) { atomicAdd(&A.status->nonpositive, (unsigned long long)bp); atomicCAS(&A.status->code, 0, DSPW_ERR_NONPOSITIVE); }
     if (sv) atomicAdd(&A.status->sign_viol, (unsigned long long)sv);
-    if (vv) atomicAdd(&A.status->limiter_acts, (unsigned long long)vv);
+    if (vv) atomicAdd(&A.status->limiter_acts[sl], (unsigned long long)vv);
   }
 }
 
