@@ -857,11 +857,13 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
 #pragma unroll
     for (int i = 0; i < 5; i++) Diff[i] += col[i] * ld * dZ;
   };
-  // The FP32 DSP-WENO kernels keep this loop rolled: one copy of the
-  // reconstruction (features, network, limiter) instead of four or five
+  // The 2-D / 3-D FP32 DSP-WENO kernels keep this loop rolled: one copy of
+  // the reconstruction (features, network, limiter) instead of four or five
   // relieves the instruction cache (KH 2048^2: 3.31 -> 3.23 ms per step).
-  // Unrolled is faster for the SP-WENO family and for FP64 (1-3 %).
-  if constexpr (sizeof(T) == 4 && Sp::rec == 2) {
+  // Unrolled is faster for the SP-WENO family and for FP64 (1-3 %), and for
+  // the 1-D kernels (3 components; the small 1-D grids of the matched-error
+  // runs are bound by the latency of one warp task: 5 % faster).
+  if constexpr (sizeof(T) == 4 && Sp::rec == 2 && DIM > 1) {
 #pragma unroll 1
     for (int j = 0; j < 5; j++) component(j);
   } else {
