@@ -244,10 +244,15 @@ int validate(const dspw_desc& d) {
   int N[3] = {d.nx, d.ny, d.nz};
   for (int k = 0; k < dim; k++)
     if (N[k] < 2) return DSPW_ERR_UNSUPPORTED;   // a swept direction needs >= 2 cells
+  // eno 3 has three ghost cells: on a line of two cells the wall mirror of the
+  // third would lie outside the line (periodic ghosts wrap, neumann ones copy)
+  if (d.recon == DSPW_REC_ENO3)
+    for (int k = 0; k < dim; k++)
+      if (N[k] < 3 && (d.bc[2 * k] == DSPW_BC_WALL || d.bc[2 * k + 1] == DSPW_BC_WALL)) return DSPW_ERR_UNSUPPORTED;
   if (!(d.xmax > d.xmin) || !(d.ymax > d.ymin) || !(d.zmax > d.zmin)) return DSPW_ERR_ARG;
   if (d.precision != DSPW_FP64 && d.precision != DSPW_FP32_BF16) return DSPW_ERR_ARG;
   if (d.time_scheme < DSPW_RK1 || d.time_scheme > DSPW_RK4) return DSPW_ERR_UNSUPPORTED;
-  if (d.recon < DSPW_REC_SP_WENO || d.recon > DSPW_REC_ENO2) return DSPW_ERR_UNSUPPORTED;
+  if (d.recon < DSPW_REC_SP_WENO || d.recon > DSPW_REC_ENO3) return DSPW_ERR_UNSUPPORTED;
   bool scalar = d.model <= DSPW_BURGERS;
   if (scalar) {
     if (d.model == DSPW_LINADV && !(d.flux >= DSPW_LIN_EC && d.flux <= DSPW_LIN_TECNO4)) return DSPW_ERR_ARG;

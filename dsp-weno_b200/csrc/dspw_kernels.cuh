@@ -369,10 +369,13 @@ DSPW_HD bool sign_violation(T z0, T z1, T z2, T z3, T zl, T zr) {
 template <typename T> struct NetScratch { float feat[32][8]; float logit[32][8]; uint32_t frag[32][12]; };
 template <> struct NetScratch<double> { float feat[1][8]; float logit[1][8]; uint32_t frag[1][12]; };
 
+// P and V hold the staged cells of a warp task: SEG_LOAD of them (two ghost
+// cells per side), two more for the three-cell halo of point-wise ENO of
+// level 3, which the generic kernel stages one slot further right (eno_shift).
 template <typename T>
 struct WarpSmem {
-  T P[5][SEG_LOAD];
-  T V[5][SEG_LOAD];
+  T P[5][SEG_LOAD + 2];
+  T V[5][SEG_LOAD + 2];
   T W[5][32];      // wide two-point fluxes, centre g = c0 - 1 + idx
   T F[5][32];      // face fluxes, face f = c0 + idx
   NetScratch<T> ns;
@@ -764,6 +767,13 @@ __device__ __forceinline__ bool sign_checked(const ProbDev& P) {
   return true;
 }
 
+// Staging shift of the six-cell stencils of point-wise ENO of level 3 (generic
+// kernel only; the specialised kernels never see it, and fold it to 0).
+template <typename Sp>
+__device__ inline int eno_shift(const ProbDev& P) {
+  return (!Sp::fixed && P.recon == DSPW_REC_ENO3) ? 1 : 0;
+}
+
 template <typename T, typename Sp>
 __device__ inline void reconstruct_lane(const ProbDev& P, const NetParams& NP, WarpSmem<T>* sm,
                                         int lane, bool valid, T s0, T s1, T s2, T s3, T& l, T& r, int& viol,
@@ -792,6 +802,8 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
   const T G = T(P.gamma);
   const T n0 = T(DIR == 0), n1 = T(DIR == 1), n2 = T(DIR == 2);
   const T* vel = fa.vel;
+  const int qb = eno_shift<Sp>(P);
+  const int cq = q0 + qb;   // first of the four cells around the face
   T a = m::sqrt(m::div(T(0.5) * G, fa.beta));
   T vsq = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
   T H = m::div(a * a, G - T(1.0)) + T(0.5) * vsq;
@@ -808,7 +820,7 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
     T L0 = m::abs(fa.vn - a), L4 = m::abs(fa.vn + a);
     if (P.ec1) {
       // LambdaL[0]-LambdaR[0] and LambdaL[3]-LambdaR[3] (kepes_tecno4_roe.cc:92-113)
-      T vnl = sm->P[1 + DIR][q0 + 1], vnr = sm->P[1 + DIR][q0 + 2];
+      T vnl = sm->P[1 + DIR][cq + 1], vnr = sm->P[1 + DIR][cq + 2];
       T al = m::sqrt(m::div(T(0.5) * G, fa.betal));
       T ar = m::sqrt(m::div(T(0.5) * G, fa.betar));
       ma = T(1.0 / 6.0);
@@ -836,18 +848,24 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
     const T Sj = j == 0 ? S[0] : (j == 1 ? S[1] : (j == 2 ? S[2] : (j == 3 ? S[3] : S[4])));
 #pragma unroll
     for (int r = 0; r < 5; r++) col[r] *= Sj;
-    T z[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      int q = q0 + k;
+    // Z_k = (R S^(1/2))^T V_k of staged cell q
+    auto zdot = [&](int q) {
       T acc = col[0] * sm->V[0][q] + col[1] * sm->V[1][q];
       if (DIM >= 2) acc = acc + col[2] * sm->V[2][q];
       if (DIM >= 3) acc = acc + col[3] * sm->V[3][q];
       acc = acc + col[4] * sm->V[4][q];
-      z[k] = T(0.0) + acc;
-    }
+      return T(0.0) + acc;
+    };
+    T z[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) z[k] = zdot(cq + k);
     T zl = T(0), zr = T(0);
-    reconstruct_lane<T, Sp>(P, NP, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol, signv);
+    if (qb) {
+      const T zo0 = zdot(q0), zo5 = zdot(q0 + 5);
+      if (valid) eno3_recon<T>(zo0, z[0], z[1], z[2], z[3], zo5, zl, zr);
+    } else {
+      reconstruct_lane<T, Sp>(P, NP, sm, lane, valid, z[0], z[1], z[2], z[3], zl, zr, viol, signv);
+    }
     if (A.collect_buf && valid)
       collect_pair<T>(A, (unsigned)(blockIdx.x * 1024 + threadIdx.x) * 8u + (unsigned)j + 977u * collect_salt,
                       z[0], z[1], z[2], z[3], zl, zr);
@@ -883,13 +901,16 @@ __device__ inline void tecno_dissipation(const SweepArgs<T>& A, const ProbDev& P
 // primitive and entropy variables; ghost cells follow apply_bc
 // (enflo/src/fv.cc:121-361): periodic wrap, wall mirror with the normal
 // velocity negated, neumann copy of the boundary cell, dirichlet fixed state.
+// qb = eno_shift(): staged cell q is c0 - 2 - qb + q, so that point-wise ENO
+// of level 3 finds its third ghost cell at q = 0 and every other reader the
+// four-cell stencil of face c0 + lane at q = lane + qb .. lane + qb + 3.
 template <typename T, int DIR>
 __device__ inline void euler_stage_cells(const SweepArgs<T>& A, const ProbDev& P, WarpSmem<T>* sm, int lane, int i0,
-                                         int j0, int k0, int c0, int ncell) {
+                                         int j0, int k0, int c0, int ncell, int qb) {
   const int N = dir_len<DIR>(P);
   const T G = T(P.gamma);
-  for (int q = lane; q < ncell + 4; q += 32) {
-    int c = c0 - 2 + q;
+  for (int q = lane; q < ncell + 4 + 2 * qb; q += 32) {
+    int c = c0 - 2 - qb + q;
     int side = c < 0 ? 0 : 1;
     int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
     T p[5];
@@ -1078,25 +1099,27 @@ __device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, Warp
                                    int lane, int ncell, int& viol, unsigned long long& signv, unsigned& checked,
                                    unsigned collect_salt = 0) {
   const T G = T(P.gamma), Rg = T(P.gas_const), area = T(P.area[DIR]);
+  const int qb = eno_shift<Sp>(P);
   // phase B: wide two-point flux centred at g = c0 - 1 + lane (cells g-1, g+1)
   const bool fourth = Sp::fixed || P.fourth;
   if (fourth && lane <= ncell + 1) {
     T Fw[5], Pl[5], Pr[5];
 #pragma unroll
-    for (int v = 0; v < 5; v++) { Pl[v] = sm->P[v][lane]; Pr[v] = sm->P[v][lane + 2]; }
+    for (int v = 0; v < 5; v++) { Pl[v] = sm->P[v][lane + qb]; Pr[v] = sm->P[v][lane + 2 + qb]; }
     if (Sp::fixed) kepec_pair<T, DIR>(Pl, Pr, G, Rg, area, Fw);
     else central_pair<T, DIR>(P.central, Pl, Pr, G, Rg, area, Fw);
 #pragma unroll
     for (int v = 0; v < 5; v++) sm->W[v][lane] = Fw[v];
   }
   __syncwarp();
-  // phase C: face f = c0 + lane between staged cells q = lane+1 and lane+2
+  // phase C: face f = c0 + lane between staged cells q = lane+1+qb and lane+2+qb
   const bool valid = lane <= ncell;
+  const int lq = valid ? lane : 0;
   T flux[5] = {T(0), T(0), T(0), T(0), T(0)};
   FaceAvg<T> fa;
   {
     T Pl[5], Pr[5];
-    const int ql = valid ? lane + 1 : 1;
+    const int ql = lq + 1 + qb;
 #pragma unroll
     for (int v = 0; v < 5; v++) { Pl[v] = sm->P[v][ql]; Pr[v] = sm->P[v][ql + 1]; }
     face_avg<T, DIR>(Pl, Pr, Rg, fa);
@@ -1110,8 +1133,8 @@ __device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, Warp
       for (int v = 0; v < 5; v++) {
         T f = T(0.0);
         f += Fn[v] * T(4.0 / 3.0);
-        f += sm->W[v][ql - 1] * fact;
-        f += sm->W[v][ql] * fact;
+        f += sm->W[v][lq] * fact;
+        f += sm->W[v][lq + 1] * fact;
         flux[v] = f;
       }
     } else {
@@ -1123,8 +1146,7 @@ __device__ inline void euler_faces(const SweepArgs<T>& A, const ProbDev& P, Warp
     const T ra = T(P.rarea[DIR]);
 #pragma unroll
     for (int v = 0; v < 5; v++) flux[v] *= ra;
-    tecno_dissipation<T, DIR, DIM, Sp>(A, P, *A.net, sm, lane, valid, valid ? lane : 0, fa, flux, viol, signv,
-                                   collect_salt);
+    tecno_dissipation<T, DIR, DIM, Sp>(A, P, *A.net, sm, lane, valid, lq, fa, flux, viol, signv, collect_salt);
 #pragma unroll
     for (int v = 0; v < 5; v++) flux[v] *= area;
     checked = valid ? (DIM == 1 ? 3u : (DIM == 2 ? 4u : 5u)) : 0u;
@@ -1141,7 +1163,7 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
                            WarpSmem<T>* sm, int lane, int lt) {
   int i0, j0, k0, c0, ncell;
   decode_task<DIR>(P, lt, i0, j0, k0, c0, ncell);
-  euler_stage_cells<T, DIR>(A, P, sm, lane, i0, j0, k0, c0, ncell);
+  euler_stage_cells<T, DIR>(A, P, sm, lane, i0, j0, k0, c0, ncell, eno_shift<Sp>(P));
   int viol = 0;
   unsigned long long signv = 0;
   unsigned checked = 0;
@@ -1347,8 +1369,9 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   int i0, j0, k0, c0, ncell;
   decode_task<DIR>(P, lt, i0, j0, k0, c0, ncell);
   const int N = dir_len<DIR>(P);
-  for (int q = lane; q < ncell + 4; q += 32) {
-    int c = c0 - 2 + q;
+  const int qb = eno_shift<Sp>(P);
+  for (int q = lane; q < ncell + 4 + 2 * qb; q += 32) {
+    int c = c0 - 2 - qb + q;
     int side = c < 0 ? 0 : 1;
     int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
     T u;
@@ -1363,7 +1386,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   }
   __syncwarp();
   const bool valid = lane <= ncell;
-  const int q = valid ? lane : 0;
+  const int q = (valid ? lane : 0) + qb;
   T s0 = sm->P[0][q], s1 = sm->P[0][q + 1], s2 = sm->P[0][q + 2], s3 = sm->P[0][q + 3];
   const T vn = T(P.lin_vn[DIR]);
   T flux = T(0);
@@ -1388,7 +1411,11 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   if (P.tecno) {
     T D = (P.model == DSPW_LINADV) ? m::abs(vn) : T(0.5) * (m::abs(s1) + m::abs(s2));
     T l = T(0), r = T(0);
-    reconstruct_lane<T, Sp>(P, *A.net, sm, lane, valid, s0, s1, s2, s3, l, r, viol, signv);
+    if (qb) {
+      if (valid) eno3_recon<T>(sm->P[0][q - 1], s0, s1, s2, s3, sm->P[0][q + 4], l, r);
+    } else {
+      reconstruct_lane<T, Sp>(P, *A.net, sm, lane, valid, s0, s1, s2, s3, l, r, viol, signv);
+    }
     if (valid && sign_checked<T, Sp>(P) && sign_violation<T>(s0, s1, s2, s3, l, r)) signv++;
     if (A.collect_buf && valid) collect_pair<T>(A, (unsigned)lt * 32u + (unsigned)lane, s0, s1, s2, s3, l, r);
     flux -= T(0.5) * D * (r - l);
@@ -1443,7 +1470,8 @@ k_sweep(SweepArgs<T> A) {
         const int pp = A.pmap ? __ldg(A.pmap + p) : p;
         const int lt0 = base - __ldg(A.task_start + p);
         const ProbDev& P = A.prob[pp];
-        if ((Sp::fixed || !P.is_scalar) && base + WARPS_PER_BLOCK <= __ldg(A.task_start + p + 1) &&
+        if ((Sp::fixed || (!P.is_scalar && P.recon != DSPW_REC_ENO3)) &&
+            base + WARPS_PER_BLOCK <= __ldg(A.task_start + p + 1) &&
             (lt0 % P.nx) % COOP_COLS == 0 && (lt0 % P.nx) + COOP_COLS <= P.nx) {
           ProbState& S = A.st[pp];
           if (!A.residual_only && !*((volatile int*)&S.active)) continue;

@@ -122,6 +122,40 @@ DSPW_HD T eno2_side(T q0, T q1, T q2) {
   return res;
 }
 
+// eno_pw with eno_level 3 (enflo/src/limiter.h:63-96, ENO3_COEF :10-12) of
+// five values: the stencil shifts left once for the first-order and once for
+// the second-order divided difference whose right member is the larger in
+// magnitude, then the three-point interpolation of the chosen stencil, summed
+// in the reference's order.  Selects, not indexing: no local memory.
+template <typename T>
+DSPW_HD T eno3_side(T q0, T q1, T q2, T q3, T q4) {
+  typedef Mth<T> m;
+  const T d10 = q1 - q0, d11 = q2 - q1, d12 = q3 - q2, d13 = q4 - q3;
+  const T d20 = d11 - d10, d21 = d12 - d11, d22 = d13 - d12;
+  const bool s1 = m::abs(d12) > m::abs(d11);
+  // second order: r = 0 compares d22 with d21, r = 1 compares d21 with d20
+  const bool s2 = s1 ? (m::abs(d21) > m::abs(d20)) : (m::abs(d22) > m::abs(d21));
+  const int r = (int)s1 + (int)s2;
+  T a, b, c, x, y, z;
+  if (r == 0) { a = T(0.375); b = T(0.75); c = T(-0.125); x = q2; y = q3; z = q4; }
+  else if (r == 1) { a = T(-0.125); b = T(0.75); c = T(0.375); x = q1; y = q2; z = q3; }
+  else { a = T(0.375); b = T(-1.25); c = T(1.875); x = q0; y = q1; z = q2; }
+  T res = T(0);
+  res += a * x;
+  res += b * y;
+  res += c * z;
+  return res;
+}
+
+// point-wise ENO of level 3 at the middle face of a six-cell stencil
+// (reconstruct_eno_pw, enflo/src/reconstruct.cc:84-110): left state from
+// s0..s4, right state from s5..s1
+template <typename T>
+DSPW_HD void eno3_recon(T s0, T s1, T s2, T s3, T s4, T s5, T& recl, T& recr) {
+  recl = eno3_side<T>(s0, s1, s2, s3, s4);
+  recr = eno3_side<T>(s5, s4, s3, s2, s1);
+}
+
 template <typename T>
 DSPW_HD void simple_recon(int kind, T s0, T s1, T s2, T s3, T& recl, T& recr) {
   typedef Mth<T> m;

@@ -28,7 +28,8 @@ FLUX = {
     "roe_tecno4_roe": 25,
 }
 RECON = {"sp_weno": 0, "sp_wenoc": 1, "sp_weno_corr2": 2, "sp_weno_dl": 3,
-         "first": 4, "second": 5, "minmod": 6, "minabs": 7, "eno2": 8}
+         "first": 4, "second": 5, "minmod": 6, "minabs": 7, "eno2": 8,
+         "eno3": 9}
 BC = {"periodic": 0, "dirichlet": 1, "neumann": 2, "wall": 3}
 TIME = {"rk1": 0, "ssprk3": 1, "jameson_rk4": 2, "rk4": 3}
 MU = {"constant": 0, "sutherland": 1, "power": 2}

@@ -71,7 +71,8 @@ int recon_enum(const std::string& r) {
                                                {"sp_weno_corr2", DSPW_REC_SP_WENO_CORR2},
                                                {"sp_weno_dl", DSPW_REC_SP_WENO_DL}, {"first", DSPW_REC_FIRST},
                                                {"second", DSPW_REC_SECOND}, {"minmod", DSPW_REC_MINMOD},
-                                               {"minabs", DSPW_REC_MINABS}, {"eno2", DSPW_REC_ENO2}};
+                                               {"minabs", DSPW_REC_MINABS}, {"eno2", DSPW_REC_ENO2},
+                                               {"eno3", DSPW_REC_ENO3}};
   auto it = m.find(r);
   if (it == m.end()) throw Fail("reconstruction not supported by the GPU path: " + r);
   return it->second;

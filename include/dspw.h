@@ -64,7 +64,11 @@ enum dspw_flux {
 enum dspw_recon {
   DSPW_REC_SP_WENO = 0, DSPW_REC_SP_WENOC = 1, DSPW_REC_SP_WENO_CORR2 = 2, DSPW_REC_SP_WENO_DL = 3,
   DSPW_REC_FIRST = 4, DSPW_REC_SECOND = 5, DSPW_REC_MINMOD = 6, DSPW_REC_MINABS = 7,
-  DSPW_REC_ENO2 = 8          /* point-wise ENO, eno_level 2 (param.in "reconstruct eno 2") */
+  DSPW_REC_ENO2 = 8,         /* point-wise ENO, eno_level 2 (param.in "reconstruct eno 2") */
+  DSPW_REC_ENO3 = 9          /* point-wise ENO, eno_level 3 ("reconstruct eno 3"): three ghost
+                                cells and six-cell face stencils, as the reference's
+                                ng_cell = 3 (enflo/src/parameter.cc:178-184, fv.cc:26).  A
+                                wall axis needs at least 3 cells. */
 };
 
 /* boundary conditions (enflo/src/ext_constants.h:25).  DIRICHLET is parsed but
@@ -218,7 +222,8 @@ DSPW_API int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, i
  * face with desc->recon in desc->precision, on the GPU, with the same device
  * code as the stage kernels (reconstruct(), enflo/src/reconstruct.cc:192-239).
  * limiter_acts receives how often the FP32 form's sign-preserving limiter
- * acted.  Allocates its own temporary device buffers. */
+ * acted.  Allocates its own temporary device buffers.  DSPW_REC_ENO3 reads
+ * six-cell stencils and returns DSPW_ERR_UNSUPPORTED here. */
 DSPW_API int dspw_reconstruct_batch(const dspw_desc* desc, const double* u4, long long n, double* recl,
                                     double* recr, long long* limiter_acts);
 

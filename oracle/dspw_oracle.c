@@ -13,7 +13,9 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define NG 2                  /* ghost width: max(flux_ng, rec_ng) = 2 (enflo/src/parameter.cc:179-206,315-318) */
+/* ghost width of the state `s` in scope: max(flux_ng, rec_ng), 3 for eno 3 and
+ * 2 otherwise (enflo/src/parameter.cc:156-206,315-318, enflo/src/fv.cc:26) */
+#define NG (s->ng)
 #define SPW_EPS 1.0e-13       /* enflo/src/limiter.h:14 */
 #define NN_THRESHOLD 1e-8     /* enflo/src/neural_network.cc:137 */
 
@@ -25,6 +27,7 @@ static const double RK4C[4] = {1.0, 1.0 / 2.0, 1.0 / 2.0, 1.0};        /* rk4_rk
 struct or_state {
   dspw_desc d;
   int scalar, nvar;
+  int ng;                       /* ghost width; face stencils hold 2 ng cells */
   int nx, ny, nz, px, py, pz;   /* interior and padded sizes */
   double dx, dy, dz;
   double *P, *V;                /* padded primitive / entropy variables, 5 per cell */
@@ -228,8 +231,33 @@ void or_nn_forward(const dspw_desc* d, const double u[4], double* recl, double* 
   *recr = w[3] * 0.5 * (u[1] + u[2]) + w[2] * (-0.5 * u[3] + 1.5 * u[2]);
 }
 
-/* reconstruct dispatch for one component, enflo/src/reconstruct.cc:115-157,192-239 */
-static void reconstruct1(const dspw_desc* d, const double s[4], double* l, double* r) {
+/* eno_pw with eno_level 3 on five values q[0..4] (enflo/src/limiter.h:63-96,
+ * ENO3_COEF :10-12): divided differences of order 1 and 2, the stencil shifted
+ * left once per order whose right difference is the larger in magnitude, then
+ * the three-point interpolation of the chosen stencil. */
+static double eno3_pw(const double q[5]) {
+  static const double coef[3][3] = {{0.375, -1.25, 1.875}, {-0.125, 0.75, 0.375}, {0.375, 0.75, -0.125}};
+  double dd1[4], dd2[3];
+  for (int j = 0; j < 4; j++) dd1[j] = q[j + 1] - q[j];
+  for (int j = 0; j < 3; j++) dd2[j] = dd1[j + 1] - dd1[j];
+  int r = 0;
+  if (fabs(dd1[2 - r]) > fabs(dd1[1 - r])) r++;
+  if (fabs(dd2[2 - r]) > fabs(dd2[1 - r])) r++;
+  double res = 0;
+  for (int i = 0; i < 3; i++) res += coef[2 - r][i] * q[2 - r + i];
+  return res;
+}
+
+/* reconstruct dispatch for one component, enflo/src/reconstruct.cc:115-157,192-239.
+ * s holds the face stencil: 4 values, 6 for eno 3 (reconstruct_eno_pw,
+ * reconstruct.cc:84-110: left from s[0..4], right from s[5..1]). */
+static void reconstruct1(const dspw_desc* d, const double* s, double* l, double* r) {
+  if (d->recon == DSPW_REC_ENO3) {
+    const double L[5] = {s[0], s[1], s[2], s[3], s[4]}, Rr[5] = {s[5], s[4], s[3], s[2], s[1]};
+    *l = eno3_pw(L);
+    *r = eno3_pw(Rr);
+    return;
+  }
   switch (d->recon) {
     case DSPW_REC_SP_WENO: or_sp_weno(s, 0, l, r); break;
     case DSPW_REC_SP_WENOC: or_sp_weno(s, 1, l, r); break;
@@ -442,10 +470,11 @@ static void prim_to_ent1(const dspw_desc* d, const double* P, double* V) {
  * (enflo/src/kepes_tecno4_roe.cc:10-176) is the template; the variants differ in
  * the central flux (kepes_tecno_roe.cc:51-54, kep_tecno_roe.cc:53, roe_tecno*_roe.cc)
  * and in Lambda (kepes_tecno4_rusanov.cc:83-85). */
-static void tecno_flux(const dspw_desc* d, const double* P, const double* V, const double* n, double area,
-                       double h, double* flux) {
+static void tecno_flux(const dspw_desc* d, const double* Pst, const double* V, int ns, const double* n,
+                       double area, double h, double* flux) {
   (void)h;
   double G = d->gamma, Rg = d->gas_const;
+  const double* P = Pst + 5 * (ns / 2 - 2);   /* the four cells around the face */
   const double* Pl = P + 5;
   const double* Pr = P + 10;
   double rhol = Pl[0], rhor = Pr[0];
@@ -507,8 +536,8 @@ static void tecno_flux(const dspw_desc* d, const double* P, const double* V, con
     for (int i = 0; i < 5; i++) Lam[i] = lr;
   }
 
-  double Z[4][5];
-  for (int k = 0; k < 4; k++)
+  double Z[6][5];
+  for (int k = 0; k < ns; k++)
     for (int i = 0; i < 5; i++) {
       const double* Vk = V + 5 * k;
       Z[k][i] = 0.0;
@@ -516,8 +545,9 @@ static void tecno_flux(const dspw_desc* d, const double* P, const double* V, con
     }
   double Zij[5], Zji[5];
   for (int i = 0; i < 5; i++) {
-    double s4[4] = {Z[0][i], Z[1][i], Z[2][i], Z[3][i]};
-    reconstruct1(d, s4, &Zij[i], &Zji[i]);
+    double sk[6];
+    for (int k = 0; k < ns; k++) sk[k] = Z[k][i];
+    reconstruct1(d, sk, &Zij[i], &Zji[i]);
   }
   double dZ[5], Diff[5];
   for (int i = 0; i < 5; i++) { dZ[i] = Zji[i] - Zij[i]; Diff[i] = 0; }
@@ -532,8 +562,9 @@ static void tecno_flux(const dspw_desc* d, const double* P, const double* V, con
 }
 
 /* num_flux dispatch, enflo/src/num_flux.cc:12-72 */
-static void euler_num_flux(const dspw_desc* d, const double* P, const double* V, int dir, double dx,
+static void euler_num_flux(const dspw_desc* d, const double* Pst, const double* V, int ns, int dir, double dx,
                            double dy, double dz, double* F) {
+  const double* P = Pst + 5 * (ns / 2 - 2);   /* central fluxes read the four middle cells */
   double n[3] = {0, 0, 0};
   n[dir] = 1;
   double area = dir == 0 ? dy * dz : (dir == 1 ? dx * dz : dx * dy);
@@ -548,14 +579,18 @@ static void euler_num_flux(const dspw_desc* d, const double* P, const double* V,
     case DSPW_KEPS: keps_flux(d, P + 5, P + 10, n, area, F); break;
     case DSPW_KEPS4: four_point(d, keps_flux, P, n, area, F); break;
     case DSPW_ROE: roe_flux(d, P + 5, P + 10, n, area, F); break;
-    default: tecno_flux(d, P, V, n, area, h, F);
+    default: tecno_flux(d, Pst, V, ns, n, area, h, F);
   }
 }
 
-void or_euler_face_flux(const dspw_desc* d, const double P[20], int dir, double dx, double dy, double dz,
-                        double V[20], double flux[5]) {
-  for (int k = 0; k < 4; k++) prim_to_ent1(d, P + 5 * k, V + 5 * k);
-  euler_num_flux(d, P, V, dir, dx, dy, dz, flux);
+/* cells of a face stencil: 2 ng */
+static int stencil_cells(const dspw_desc* d) { return d->recon == DSPW_REC_ENO3 ? 6 : 4; }
+
+void or_euler_face_flux(const dspw_desc* d, const double* P, int dir, double dx, double dy, double dz,
+                        double* V, double flux[5]) {
+  const int ns = stencil_cells(d);
+  for (int k = 0; k < ns; k++) prim_to_ent1(d, P + 5 * k, V + 5 * k);
+  euler_num_flux(d, P, V, ns, dir, dx, dy, dz, flux);
 }
 
 /* ----------------------------------------------------------- scalar pieces -- */
@@ -569,7 +604,8 @@ static double bur_ec(double ul, double ur) { return (ul * ul + ur * ur + ul * ur
 
 /* num_flux and the lin_ and bur_ fluxes, enflo_scalar/src_scalar/num_flux.cc:12-57,
  * lin_tecno4.cc:10-31, lin_ec4.cc:10-34, bur_tecno4.cc:10-35, bur_ec4.cc:10-34 */
-double or_scalar_face_flux(const dspw_desc* d, const double* u, int dir, double dx, double dy, double dz) {
+double or_scalar_face_flux(const dspw_desc* d, const double* ust, int dir, double dx, double dy, double dz) {
+  const double* u = ust + (stencil_cells(d) / 2 - 2);   /* central fluxes read the four middle cells */
   double n[3] = {0, 0, 0};
   n[dir] = 1;
   double area = dir == 0 ? dy * dz : (dir == 1 ? dx * dz : dx * dy);
@@ -597,11 +633,11 @@ double or_scalar_face_flux(const dspw_desc* d, const double* u, int dir, double 
   }
   if (d->flux == DSPW_LIN_TECNO || d->flux == DSPW_LIN_TECNO4) {
     double D = fabs(n[0] * vel[0] + n[1] * vel[1] + n[2] * vel[2]);
-    reconstruct1(d, u, &l, &r);
+    reconstruct1(d, ust, &l, &r);
     flux -= 0.5 * D * (r - l);
   } else if (d->flux == DSPW_BUR_TECNO || d->flux == DSPW_BUR_TECNO4) {
     double D = 0.5 * (fabs(u[1]) + fabs(u[2]));
-    reconstruct1(d, u, &l, &r);
+    reconstruct1(d, ust, &l, &r);
     flux -= 0.5 * D * (r - l);
   }
   flux *= area;
@@ -616,6 +652,7 @@ or_state* or_create(const dspw_desc* d) {
   s->scalar = (d->model == DSPW_LINADV || d->model == DSPW_BURGERS);
   s->nvar = s->scalar ? 1 : 5;
   s->nx = d->nx; s->ny = d->ny; s->nz = d->nz;
+  s->ng = d->recon == DSPW_REC_ENO3 ? 3 : 2;
   s->px = d->nx + 2 * NG; s->py = d->ny + 2 * NG; s->pz = d->nz + 2 * NG;
   s->dx = (d->xmax - d->xmin) / d->nx;   /* enflo/src/fv.cc:29-31 */
   s->dy = (d->ymax - d->ymin) / d->ny;
@@ -859,8 +896,8 @@ double or_compute_dt(or_state* s) {
 
 /* ------------------------------------------------------- residual assembly -- */
 
-/* gather the 4-cell stencil of face `f` along direction dir of line (a, b) in
- * padded coordinates: cells f .. f+3 along dir */
+/* cell of the face stencil along direction dir of line (a, b), in padded
+ * coordinates: face f reads cells f .. f + 2 ng - 1 along dir */
 static void line_cell(const or_state* s, int dir, int f, int a, int b, int* i, int* j, int* k) {
   if (dir == 0) { *i = f; *j = a; *k = b; }
   else if (dir == 1) { *i = a; *j = f; *k = b; }
@@ -885,12 +922,13 @@ static void inviscid_residual(or_state* s) {
     int o1 = dir == 0 ? 1 : 0, o2 = dir == 2 ? 1 : 2;   /* the two other directions */
     for (int a = 0; a < N[o1]; a++)
       for (int b = 0; b < N[o2]; b++) {
+        const int ns = 2 * NG;
         for (int f = 0; f <= N[dir]; f++) {   /* face f between cells f-1 and f */
-          double Pst[20], Vst[20], F[5];
-          for (int l = 0; l < 4; l++) {
+          double Pst[30], Vst[30], F[5];
+          for (int l = 0; l < ns; l++) {
             int i, j, k;
             int coord[3];
-            coord[dir] = f + l;          /* padded: cells f-2..f+1 */
+            coord[dir] = f + l;          /* padded: cells f-ng..f+ng-1 */
             coord[o1] = a + NG;
             coord[o2] = b + NG;
             line_cell(s, 0, coord[0], coord[1], coord[2], &i, &j, &k);
@@ -899,10 +937,11 @@ static void inviscid_residual(or_state* s) {
             memcpy(Vst + 5 * l, s->V + 5 * c, 5 * sizeof(double));
           }
           if (s->scalar) {
-            double u4[4] = {Pst[0], Pst[5], Pst[10], Pst[15]};
-            F[0] = or_scalar_face_flux(&s->d, u4, dir, s->dx, s->dy, s->dz);
+            double us[6];
+            for (int l = 0; l < ns; l++) us[l] = Pst[5 * l];
+            F[0] = or_scalar_face_flux(&s->d, us, dir, s->dx, s->dy, s->dz);
           } else {
-            euler_num_flux(&s->d, Pst, Vst, dir, s->dx, s->dy, s->dz, F);
+            euler_num_flux(&s->d, Pst, Vst, ns, dir, s->dx, s->dy, s->dz, F);
           }
           int cl[3], cr[3];
           cl[dir] = f - 1; cl[o1] = a; cl[o2] = b;

@@ -42,10 +42,12 @@ void or_sp_weno(const double u[4], int corr_type, double* recl, double* recr);
 void or_nn_forward(const dspw_desc* d, const double u[4], double* recl, double* recr);
 /* DSP-WENO pieces exposed for the training checks: features (5), vertices (2x5). */
 void or_nn_features(const double u[4], double feat[5], double vx[5], double vy[5]);
-/* Euler face flux for a 4-cell primitive stencil P[4][5] with unit normal dir,
- * cell sizes dx,dy,dz; V[4][5] receives the entropy variables used. */
-void or_euler_face_flux(const dspw_desc* d, const double P[20], int dir, double dx, double dy,
-                        double dz, double V[20], double flux[5]);
+/* Euler face flux for a primitive face stencil P[ns][5] with unit normal dir,
+ * cell sizes dx,dy,dz; V[ns][5] receives the entropy variables used.  ns = 4,
+ * 6 for eno 3 (the reference's 2 ng_cell). */
+void or_euler_face_flux(const dspw_desc* d, const double* P, int dir, double dx, double dy,
+                        double dz, double* V, double flux[5]);
+/* scalar face flux of a stencil u[ns] (ns as above) */
 double or_scalar_face_flux(const dspw_desc* d, const double* u, int dir, double dx, double dy,
                            double dz);
 

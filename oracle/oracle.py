@@ -21,7 +21,7 @@ import numpy as np
 ORACLE_DIR = Path(__file__).resolve().parent
 REPO = ORACLE_DIR.parent
 sys.path.insert(0, str(REPO / "dsp-weno_b200"))
-from dspw.capi import DIAG_COLS, Desc, nvar  # noqa: E402
+from dspw.capi import DIAG_COLS, RECON, Desc, nvar  # noqa: E402
 from dspw.paramfile import write_param  # noqa: E402
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -146,11 +146,17 @@ def nn_features(u4):
     return f, vx, vy
 
 
+def stencil_cells(desc) -> int:
+    """Cells of a face stencil: 2 ghost widths, 6 for eno 3 and 4 otherwise."""
+    return 6 if desc.recon == RECON["eno3"] else 4
+
+
 def euler_face_flux(desc, P4, direction, dx, dy, dz):
-    V, F = np.zeros(20), np.zeros(5)
-    oracle_lib().or_euler_face_flux(C.byref(desc), np.ascontiguousarray(P4, dtype=np.float64).reshape(20),
+    ns = stencil_cells(desc)
+    V, F = np.zeros(5 * ns), np.zeros(5)
+    oracle_lib().or_euler_face_flux(C.byref(desc), np.ascontiguousarray(P4, dtype=np.float64).reshape(5 * ns),
                                     direction, dx, dy, dz, V, F)
-    return F, V.reshape(4, 5)
+    return F, V.reshape(ns, 5)
 
 
 def scalar_face_flux(desc, u4, direction, dx, dy, dz):
@@ -294,9 +300,11 @@ class RefEuler(_RefBase):
         return rows[:k]
 
     def face_flux(self, P4, direction):
-        V, F = np.zeros(20), np.zeros(5)
-        self.L.refE_face_flux(self.h, np.ascontiguousarray(P4, dtype=np.float64).reshape(20), direction, V, F)
-        return F, V.reshape(4, 5)
+        P4 = np.ascontiguousarray(P4, dtype=np.float64)
+        ns = P4.size // 5
+        V, F = np.zeros(5 * ns), np.zeros(5)
+        self.L.refE_face_flux(self.h, P4.reshape(5 * ns), direction, V, F)
+        return F, V.reshape(ns, 5)
 
     def reconstruct(self, Z45):
         l, r = np.zeros(5), np.zeros(5)

@@ -197,10 +197,14 @@ HX void refS_run_errors(void* hp, double* err3) {
   std::swap(l1, f->L1_err); std::swap(l2, f->L2_err); std::swap(li, f->Linf_err);
 }
 
-// One face flux num_flux(Soln, n) (enflo_scalar/src_scalar/num_flux.cc:12-57).
+// cells of a face stencil passed in: 4, or 2 ng_cell when that is more (eno 3)
+static int stencil_len(const FV* f) { return std::max(4, 2 * f->ng_cell); }
+
+// One face flux num_flux(Soln, n) (enflo_scalar/src_scalar/num_flux.cc:12-57)
+// of a stencil of stencil_len values.
 HX double refS_face_flux(void* hp, const double* u4, int dir) {
   FV* f = ((Handle*)hp)->fv;
-  std::vector<double> s(u4, u4 + 4);
+  std::vector<double> s(u4, u4 + stencil_len(f));
   Vector n;
   n = 0;
   if (dir == 0) n.x = 1; else if (dir == 1) n.y = 1; else n.z = 1;
@@ -209,10 +213,11 @@ HX double refS_face_flux(void* hp, const double* u4, int dir) {
   return fl;
 }
 
-// Configured reconstruction of one stencil (enflo_scalar/src_scalar/reconstruct.cc:181-228).
+// Configured reconstruction of one stencil of stencil_len values
+// (enflo_scalar/src_scalar/reconstruct.cc:181-228).
 HX void refS_reconstruct(void* hp, const double* u4, double* recl, double* recr) {
   FV* f = ((Handle*)hp)->fv;
-  std::vector<double> s(u4, u4 + 4);
+  std::vector<double> s(u4, u4 + stencil_len(f));
   f->reconstruct(f->param.reconstruct_scheme, f->dx, s, *recl, *recr);
 }
 

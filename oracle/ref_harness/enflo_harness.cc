@@ -252,11 +252,12 @@ HX int refE_step_diag(void* hp, int nsteps, double fixed_dt, double* rows) {
   return step_impl((Handle*)hp, nsteps, fixed_dt, rows);
 }
 
-// One face flux num_flux(P, V, n) (enflo/src/num_flux.cc:12-72) for a 4-cell
-// stencil.  The stencil is written into an x-line of the mesh and V is taken
-// from the reference's own prim_to_ent (enflo/src/fv.cc:421-552); the mesh must
-// have Nx >= 2 and ng == 2.  pin: (4, 5) primitive rows; vout: (4, 5) entropy
-// variables used; flux: 5 values.  dir 0/1/2 selects the unit normal.
+// One face flux num_flux(P, V, n) (enflo/src/num_flux.cc:12-72) for a stencil
+// of 2 ng cells (4; 6 for eno 3).  The stencil is written into an x-line of the
+// mesh and V is taken from the reference's own prim_to_ent
+// (enflo/src/fv.cc:421-552); the mesh must have Nx >= 2.  pin: (2 ng, 5)
+// primitive rows; vout: (2 ng, 5) entropy variables used; flux: 5 values.
+// dir 0/1/2 selects the unit normal.
 HX void refE_face_flux(void* hp, const double* pin, int dir, double* vout, double* flux) {
   FV* f = ((Handle*)hp)->fv;
   int g = f->ng_cell;

@@ -25,7 +25,7 @@ def _num(v):
 def desc_from_cfg(cfg: dict, nx: int, ny: int, nz: int, **over):
     """dspw_desc equivalent to a param.in dict written by dspw.paramfile.write_param."""
     kw = dict(
-        model=cfg["model"], flux=cfg["flux"], recon=cfg.get("reconstruct", "sp_weno"),
+        model=cfg["model"], flux=cfg["flux"], recon=cfg.get("reconstruct", "sp_weno").replace(" ", ""),
         nx=nx, ny=ny, nz=nz,
         x=tuple(_num(v) for v in cfg.get("x", (0, 1))),
         y=tuple(_num(v) for v in cfg.get("y", (0, 1))),

@@ -54,6 +54,13 @@ VORTEX_IC = dict(  # isentropic vortex, strength 5, gamma 1.4 (enflo/examples/2D
     pressure="pow(1-(0.4)*25/(8*1.4*pi*pi)*exp(1-x*x-y*y),1.4/0.4)")
 TGV_IC = dict(density="1", xvelocity="sin(x)*cos(y)*cos(z)", yvelocity="-cos(x)*sin(y)*cos(z)",
               zvelocity="0", pressure="1/(1.4*M*M)+(cos(2*x)+cos(2*y))*(cos(2*z)+2)/16")
+# a periodic flow without the symmetries of TGV_IC: ENO compares two jumps to
+# pick its stencil, and the exact ties of a symmetric state are then decided by
+# rounding, where the device's viscous sums (another order) differ from the
+# reference's by ulps
+SKEW_IC = dict(density="1+0.2*sin(x+0.37)*cos(2*y+0.91)+0.1*sin(z+1.3)",
+               xvelocity="sin(x+0.2)*cos(y+0.7)*cos(z+0.5)", yvelocity="-cos(x+0.9)*sin(y+0.3)*cos(z+1.1)",
+               zvelocity="0.3*sin(x+y+0.45)", pressure="1/(1.4*M*M)+0.3*sin(x+2*z+0.61)")
 
 
 def euler_cfg(flux="kepes_tecno4_roe", recon="sp_weno", **kw):
@@ -63,16 +70,16 @@ def euler_cfg(flux="kepes_tecno4_roe", recon="sp_weno", **kw):
     return c
 
 
-def random_prim_stencils(rng, n):
-    P = np.zeros((n, 4, 5))
-    P[:, :, 0] = rng.uniform(0.1, 4.0, (n, 4))
-    P[:, :, 1:4] = rng.normal(0.0, 1.5, (n, 4, 3))
-    P[:, :, 4] = rng.uniform(0.1, 6.0, (n, 4))
+def random_prim_stencils(rng, n, ncell=4):
+    P = np.zeros((n, ncell, 5))
+    P[:, :, 0] = rng.uniform(0.1, 4.0, (n, ncell))
+    P[:, :, 1:4] = rng.normal(0.0, 1.5, (n, ncell, 3))
+    P[:, :, 4] = rng.uniform(0.1, 6.0, (n, ncell))
     # a third of the stencils are smooth (small jumps) so the log-mean series
     # branch and the smooth SP-WENO regions are exercised
     m = n // 3
     base = P[:m, 1:2, :]
-    P[:m] = base * (1.0 + rng.normal(0.0, 1e-3, (m, 4, 5)))
+    P[:m] = base * (1.0 + rng.normal(0.0, 1e-3, (m, ncell, 5)))
     # a sixth are 1-D / 2-D states (zero transverse velocity)
     P[m:m + n // 6, :, 2:4] = 0.0
     return P
@@ -208,6 +215,36 @@ def gen_faces_simple(rng):
         out[key + "|dir"] = dirs
         out[key + "|F"] = F
         out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
+    # point-wise ENO of level 3: the reference's stencils have 2 ng = 6 cells
+    for flux in ("kepes_tecno4_roe", "kepes_tecno_roe", "kepes_tecno4_rusanov"):
+        R = O.RefEuler(euler_cfg(flux, "eno 3", EC1_fix="yes" if "roe" in flux else "no", y=(0, 0.5),
+                                 z=(0, 0.25)))
+        n = 150
+        P = random_prim_stencils(rng, n, ncell=6)
+        dirs = np.arange(n) % 3
+        F = np.zeros((n, 5)); V = np.zeros((n, 6, 5))
+        for t in range(n):
+            F[t], V[t] = R.face_flux(P[t], int(dirs[t]))
+        key = f"E|{flux}|eno3|{int('roe' in flux)}"
+        out[key + "|P"] = P
+        out[key + "|dir"] = dirs
+        out[key + "|F"] = F
+        out[key + "|V"] = V
+        out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
+    for model, flux in (("linadv", "lin_tecno4"), ("linadv", "lin_tecno"), ("burgers", "bur_tecno4")):
+        cfg = dict(model=model, x=("-pi", "pi"), y=(0, 0.5), z=(0, 0.25), Nx=16, Ny=2, Nz=2, cfl=0.5,
+                   final_time=0.5, reconstruct="eno 3", net_file=NET, flux=flux, ic="sin(x)",
+                   vel=(1.0, -0.5, 0.25), bc="periodic")
+        R = O.RefScalar(cfg)
+        n = 200
+        U = rng.normal(0, 1, (n, 6))
+        dirs = np.arange(n) % 3
+        F = np.array([R.face_flux(U[t], int(dirs[t])) for t in range(n)])
+        key = f"S|{flux}|eno3"
+        out[key + "|U"] = U
+        out[key + "|dir"] = dirs
+        out[key + "|F"] = F
+        out[key + "|h"] = np.array([R.dx, R.dy, R.dz])
     np.savez_compressed(OUT / "faces_simple.npz", **out)
 
 
@@ -312,6 +349,25 @@ def run_cases():
     cases.append(("tgv_ns_fixed", "E", euler_cfg("kepes_tecno4_roe", "sp_weno", model="ns_es", x=(0, "2*pi"),
                   y=(0, "2*pi"), z=(0, "2*pi"), Nx=6, Ny=6, Nz=6, ic=TGV_IC, dim=3, constants={"M": 0.3},
                   mu_ref=0.05, prandtl=0.71, final_time=10.0), 3, 0.01))
+    # point-wise ENO of level 3: the reference runs with three ghost cells and
+    # six-cell face stencils (ng_cell = 3, parameter.cc:178-184, fv.cc:26)
+    cases.append(("shuosher_eno3", "E", euler_cfg("kepes_tecno4_roe", "eno 3", x=(-5, 5), Nx=100, cfl=0.4,
+                  final_time=1.8, ic=SHU_IC, bc=bc1d, time_stamps=5, EC1_fix="yes"), 25, 0.0))
+    cases.append(("kh_eno3", "E", euler_cfg("kepes_tecno_roe", "eno 3", Nx=16, Ny=16, ic=KH_IC, dim=2,
+                  EC1_fix="yes"), 6, 0.0))
+    cases.append(("wall2d_eno3", "E", euler_cfg("kepes_tecno4_roe", "eno 3", Nx=14, Ny=11, ic=wall_ic, dim=2,
+                  bc=["wall", "neumann", "wall", "wall", "periodic", "periodic"]), 8, 0.0))
+    cases.append(("euler3d_eno3", "E", euler_cfg("roe_tecno4_roe", "eno 3", x=(0, "2*pi"), y=(0, "2*pi"),
+                  z=(0, "2*pi"), Nx=7, Ny=5, Nz=4, ic=TGV_IC, dim=3, constants={"M": 0.3}), 3, 0.0))
+    cases.append(("ns_eno3", "E", euler_cfg("kepes_tecno4_rusanov", "eno 3", model="ns_es", x=(0, "2*pi"),
+                  y=(0, "2*pi"), z=(0, "2*pi"), Nx=6, Ny=7, Nz=5, ic=SKEW_IC, dim=3, constants={"M": 0.3},
+                  mu_ref=0.05, prandtl=0.71, final_time=10.0), 3, 0.0))
+    cases.append(("burgers_eno3", "S", dict(model="burgers", x=("-pi", "pi"), Nx=64, Ny=2, Nz=2, cfl=0.4,
+                  final_time=0.5, reconstruct="eno 3", net_file=NET, flux="bur_tecno4", ic="0.5+sin(x)",
+                  bc="periodic", time_stamps=5), 30, 0.0))
+    cases.append(("linadv_wall_eno3", "S", dict(model="linadv", x=(-1, 1), Nx=50, Ny=2, Nz=2, cfl=0.5,
+                  final_time=0.4, reconstruct="eno 3", net_file=NET, flux="lin_tecno", ic="exp(-20*x*x)",
+                  bc=["wall", "neumann", "periodic", "periodic", "periodic", "periodic"], time_stamps=2), 30, 0.0))
     return cases
 
 

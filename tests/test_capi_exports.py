@@ -4,6 +4,7 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 from dspw import capi
@@ -57,6 +58,13 @@ def test_bad_descriptor_rejected_without_gpu():
     d = capi.make_desc()
     d.abi_version = 99
     assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    # eno 3 on a wall axis of two cells: the third ghost's mirror leaves the line
+    d = capi.make_desc(recon="eno3", nx=16, ny=2, bc=["periodic", "periodic", "wall", "wall", "periodic", "periodic"])
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 6
+    # the four-cell reconstruction entry point has no six-cell stencils
+    l, r, acts = np.zeros(1), np.zeros(1), ctypes.c_longlong()
+    u = np.arange(4, dtype=np.float64)
+    assert lib.dspw_reconstruct_batch(ctypes.byref(capi.make_desc(recon="eno3")), u, 1, l, r, ctypes.byref(acts)) == 6
 
 
 def test_network_file_roundtrip(tmp_path):

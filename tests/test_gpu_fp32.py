@@ -26,7 +26,7 @@ def state(nx, ny, nz):
 
 
 @pytest.mark.parametrize("dims", [(64, 1, 1), (48, 40, 1), (16, 12, 10)])
-@pytest.mark.parametrize("recon", ["sp_weno", "sp_weno_dl"])
+@pytest.mark.parametrize("recon", ["sp_weno", "sp_weno_dl", "eno3"])
 def test_fp32_vs_fp64(dims, recon):
     p = state(*dims)
     out = {}
@@ -38,7 +38,7 @@ def test_fp32_vs_fp64(dims, recon):
         s.step(5)
         st = s.status()
         assert st.code == 0 and st.nonfinite_cells == 0, (prec, st.code, st.nonfinite_cells)
-        if prec == "fp32_bf16":
+        if prec == "fp32_bf16" and recon != "eno3":   # eno 3 lacks the sign property
             assert st.sign_violations <= 0.001 * dims[0] * dims[1] * dims[2] * 5 * 3
         out[prec] = s.cons()
     a, b = out["fp32_bf16"], out["fp64"]
@@ -46,7 +46,7 @@ def test_fp32_vs_fp64(dims, recon):
     rel = np.max(np.abs(a[0] - b[0])) / np.max(np.abs(b[0]))
     # SP-WENO and DSP-WENO select regions/vertices by thresholds; FP32 rounding
     # moves a few stencils across them, which bounds the agreement
-    assert rel < (2e-4 if recon == "sp_weno" else 2e-3), rel
+    assert rel < (2e-3 if recon == "sp_weno_dl" else 2e-4), rel
 
 
 def test_fp32_scalar_linadv_dl():

@@ -60,7 +60,8 @@ def test_initial_state_matches_reference_setup(tmp_path, case):
     assert np.max(np.abs(got - ref) / scale) <= 1e-14, case
 
 
-@pytest.mark.parametrize("case", ["shuosher_sp_weno_dl", "linadv_sp_weno", "tgv_ns", "wall2d", "burgers_wall_dl"])
+@pytest.mark.parametrize("case", ["shuosher_sp_weno_dl", "linadv_sp_weno", "tgv_ns", "wall2d", "burgers_wall_dl",
+                                  "wall2d_eno3", "linadv_wall_eno3"])
 def test_descriptor_matches_python_side(tmp_path, case):
     _need_cli()
     name, kind, cfg, _, _ = next(c for c in run_cases() if c[0] == case)
@@ -184,13 +185,17 @@ def test_errors_are_reported(tmp_path, text, msg):
 
 def test_eno_level(tmp_path):
     """'reconstruct eno <level>' carries its level (parameter.cc:178-184);
-    level 2 fits the two-cell halo, level 3 does not."""
+    levels 2 and 3 are built (eno_pw has coefficients for no other,
+    limiter.h:88-94)."""
     _need_cli()
     p = tmp_path / "param.in"
     p.write_text(HAND_WRITTEN.replace("reconstruct  sp_wenoc", "reconstruct  eno 2"))
     got = json.loads(_run(["-i", p, "--check"], tmp_path).stdout)
     assert got["recon"] == capi.RECON["eno2"]
     p.write_text(HAND_WRITTEN.replace("reconstruct  sp_wenoc", "reconstruct  eno 3"))
+    got = json.loads(_run(["-i", p, "--check"], tmp_path).stdout)
+    assert got["recon"] == capi.RECON["eno3"]
+    p.write_text(HAND_WRITTEN.replace("reconstruct  sp_wenoc", "reconstruct  eno 4"))
     r = _run(["-i", p, "--check"], tmp_path, check=False)
     assert r.returncode == 1 and "reconstruction not supported" in r.stderr
 

@@ -148,8 +148,9 @@ def _simple_keys():
 
 @pytest.mark.parametrize("key", _simple_keys())
 def test_simple_reconstruction_faces_golden(key):
-    """First-order, unlimited MUSCL and minmod / minabs MUSCL inside the TeCNO
-    fluxes (enflo/src/reconstruct.cc:14-79, 162-186) against the reference."""
+    """First-order, unlimited MUSCL, minmod / minabs MUSCL and point-wise ENO of
+    levels 2 and 3 inside the TeCNO fluxes (enflo/src/reconstruct.cc:14-110,
+    162-186) against the reference; eno 3 on six-cell stencils."""
     g = load("faces_simple.npz")
     kind, flux, recon = key.split("|")[:3]
     dx, dy, dz = g[key + "|h"]
@@ -161,7 +162,7 @@ def test_simple_reconstruction_faces_golden(key):
         # layer (parameter.cc:158-162): the reference's stencil is then the two
         # cells P[0], P[1] of the face; here the face sits between rows 1 and 2
         short = recon == "first" and "tecno4" not in flux
-        F = np.zeros((len(P), 5)); V = np.zeros((len(P), 4, 5))
+        F = np.zeros((len(P), 5)); V = np.zeros((len(P), P.shape[1], 5))
         for t in range(len(P)):
             Pt = P[t][[0, 0, 1, 1]] if short else P[t]
             F[t], V[t] = O.euler_face_flux(d, Pt, int(dirs[t]), dx, dy, dz)
