@@ -148,6 +148,7 @@ struct dspw_handle {
   int nrk = 3;
   int time_scheme = 1;
   int has_ns = 0;
+  int has_halo = 0;   // some problem stores halo layers (DSPW_BC_HALO faces)
   int maxdim = 1;
   std::vector<SweepClass> classes;
   std::vector<dspw_desc> desc;
@@ -236,6 +237,22 @@ int problem_dim(const dspw_desc& d) {
   return 1;
 }
 
+// ghost layers per side of a face stencil: 3 for eno 3, else 2
+int ghost_width(const dspw_desc& d) { return d.recon == DSPW_REC_ENO3 ? 3 : 2; }
+
+// halo layers stored on each side of the last swept direction (0: none)
+int halo_layers(const dspw_desc& d) {
+  const int D = problem_dim(d) - 1;
+  return (d.bc[2 * D] == DSPW_BC_HALO || d.bc[2 * D + 1] == DSPW_BC_HALO) ? ghost_width(d) : 0;
+}
+
+// cells of one layer across the last swept direction (the layers are
+// contiguous in memory: that direction is the outermost one of the problem)
+long long layer_cells(const dspw_desc& d) {
+  const int D = problem_dim(d) - 1;
+  return D == 0 ? 1LL : (D == 1 ? (long long)d.nx : (long long)d.nx * d.ny);
+}
+
 int validate(const dspw_desc& d) {
   if (d.abi_version != DSPW_ABI_VERSION) return DSPW_ERR_ARG;
   if (d.model < 0 || d.model > 4) return DSPW_ERR_ARG;
@@ -275,7 +292,14 @@ int validate(const dspw_desc& d) {
     }
   }
   for (int f = 0; f < 6; f++)
-    if (d.bc[f] < 0 || d.bc[f] > 3) return DSPW_ERR_ARG;
+    if (d.bc[f] < 0 || d.bc[f] > DSPW_BC_HALO) return DSPW_ERR_ARG;
+  // halo faces: the two faces of the last swept direction only, for the Euler
+  // and scalar models, with at least one ghost width of interior layers to send
+  for (int f = 0; f < 6; f++) {
+    if (d.bc[f] != DSPW_BC_HALO) continue;
+    if (f / 2 != dim - 1 || d.model == DSPW_NS_ES || d.model == DSPW_NS_KEP) return DSPW_ERR_UNSUPPORTED;
+    if (N[dim - 1] < ghost_width(d)) return DSPW_ERR_UNSUPPORTED;
+  }
   for (int a = 0; a < 3; a++)   // periodic must pair with periodic (enflo/src/parameter.cc:570-581)
     if ((d.bc[2 * a] == DSPW_BC_PERIODIC) != (d.bc[2 * a + 1] == DSPW_BC_PERIODIC)) return DSPW_ERR_ARG;
   if (!(d.cfl > 0.0) || !(d.final_time >= 0.0) || d.max_iter < 1 || d.t_stamps < 1) return DSPW_ERR_ARG;
@@ -306,6 +330,11 @@ ProbDev make_prob(const dspw_desc& d, long long off) {
   P.dx = (d.xmax - d.xmin) / d.nx;   // enflo/src/fv.cc:29-31
   P.dy = (d.ymax - d.ymin) / d.ny;
   P.dz = (d.zmax - d.zmin) / d.nz;
+  // a slab of a decomposed domain keeps the domain's cell size bit for bit
+  // (its own bounds divided by its own cell count need not round to it)
+  if (d.reserved_d[5] > 0.0) P.dx = d.reserved_d[5];
+  if (d.reserved_d[6] > 0.0) P.dy = d.reserved_d[6];
+  if (d.reserved_d[7] > 0.0) P.dz = d.reserved_d[7];
   P.hmin = std::min(P.dx, std::min(P.dy, P.dz));
   P.vol = P.dx * P.dy * P.dz;
   P.node_vol = (d.xmax - d.xmin) / (d.nx + 1) * (d.ymax - d.ymin) / (d.ny + 1) * (d.zmax - d.zmin) / (d.nz + 1);
@@ -507,6 +536,14 @@ int drain_snap(dspw_handle* h) {
   return DSPW_OK;
 }
 
+// state buffer that stage rk reads (0: U^n, 1: Ua, 2: Ub), see stage_args
+int stage_input(const dspw_handle* h, int rk) {
+  static const int in4[4] = {0, 1, 2, 1};
+  if (h->nrk == 1) return 0;
+  if (h->nrk == 3) return rk == 0 ? 0 : (rk == 1 ? 1 : 2);
+  return in4[rk];
+}
+
 // sweep arguments of stage rk (residual_only: write R in every sweep)
 template <typename T>
 SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
@@ -519,11 +556,11 @@ SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
   // U^n -> Ua -> Ub -> Ua -> U^n (the last stage writes in place: every cell
   // reads its own U^n entry before overwriting it, and no sweep of that stage
   // reads U^n); RK1 U^n -> Ua, copied back after the stage
-  static const int in4[4] = {0, 1, 2, 1}, out4[4] = {1, 2, 1, 0};
-  int in, out;
-  if (h->nrk == 1) { in = 0; out = 1; }
-  else if (h->nrk == 3) { in = rk == 0 ? 0 : (rk == 1 ? 1 : 2); out = rk == 0 ? 1 : (rk == 1 ? 2 : 0); }
-  else { in = in4[rk]; out = out4[rk]; }
+  static const int out4[4] = {1, 2, 1, 0};
+  int in = stage_input(h, rk), out;
+  if (h->nrk == 1) out = 1;
+  else if (h->nrk == 3) out = rk == 0 ? 1 : (rk == 1 ? 2 : 0);
+  else out = out4[rk];
   if (residual_only) { in = 0; out = 1; }
   a.Uin = (const T*)buf(h, in);
   a.Un = (const T*)h->Un;
@@ -800,8 +837,12 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
   long long off = 0;
   h->cell_start.push_back(0);
   for (int p = 0; p < nprob; p++) {
-    h->hprob.push_back(make_prob(descs[p], off));
-    off += ncells(descs[p]);
+    // a problem with halo faces stores its ghost layers beside the interior:
+    // its block is [halo, interior, halo]; cell_start bounds whole blocks
+    const long long hc = halo_layers(descs[p]) * layer_cells(descs[p]);
+    if (hc) h->has_halo = 1;
+    h->hprob.push_back(make_prob(descs[p], off + hc));
+    off += ncells(descs[p]) + 2 * hc;
     h->cell_start.push_back(off);
     h->maxcells = std::max(h->maxcells, ncells(descs[p]));
     h->maxdim = std::max(h->maxdim, h->hprob.back().dim);
@@ -1106,6 +1147,7 @@ int dspw_globals(dspw_handle* h, int p, dspw_globals_out* g) {
 
 int dspw_diag_enable(dspw_handle* h, int capacity) {
   if (!h || capacity < 0) return DSPW_ERR_ARG;
+  if (h->has_halo && capacity > 0) return DSPW_ERR_UNSUPPORTED;   // node sums need the whole domain
   CK(cudaStreamSynchronize(h->stream));
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // the step graph changes
   if (h->ddiag) cudaFree(h->ddiag);
@@ -1344,6 +1386,29 @@ int dspw_sync(dspw_handle* h) {
 }
 
 void* dspw_stream(dspw_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int dspw_halo_view(dspw_handle* h, int p, int rk, dspw_halo_out* out) {
+  if (check_p(h, p) || !out || rk < 0 || rk >= h->nrk) return DSPW_ERR_ARG;
+  const dspw_desc& d = h->desc[p];
+  const int ng = halo_layers(d);
+  if (!ng) return DSPW_ERR_ARG;
+  const ProbDev& P = h->hprob[p];
+  const long long lc = layer_cells(d);
+  const int D = P.dim - 1;
+  const long long N = D == 0 ? P.nx : (D == 1 ? P.ny : P.nz);
+  char* base = (char*)buf(h, stage_input(h, rk)) + h->elem * P.off;
+  out->recv_lo = base - h->elem * ng * lc;
+  out->recv_hi = base + h->elem * N * lc;
+  out->send_lo = base;
+  out->send_hi = base + h->elem * (N - ng) * lc;
+  out->count = ng * lc;
+  out->comp_stride = h->ctot;
+  out->ncomp = P.nv;
+  out->elem_bytes = (int)h->elem;
+  out->ng = ng;
+  out->layer_cells = (int)lc;
+  return DSPW_OK;
+}
 
 int dspw_device_state(dspw_handle* h, int p, void** ptr, long long* stride, int* elem_bytes) {
   if (check_p(h, p) || !ptr) return DSPW_ERR_ARG;

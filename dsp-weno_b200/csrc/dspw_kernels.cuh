@@ -336,10 +336,12 @@ DSPW_HD long long cell_index(const ProbDev& P, int i0, int j0, int k0, int c) {
 }
 
 // Ghost handling of apply_bc (enflo/src/fv.cc:121-361): source cell along the
-// line for a (possibly ghost) index c, and the boundary kind used.
+// line for a (possibly ghost) index c, and the boundary kind used.  A halo
+// face (slab decomposition) reads its stored ghost layers in place.
 DSPW_HD int ghost_source(int c, int N, int kind, int& flip) {
   flip = 0;
   if (c >= 0 && c < N) return c;
+  if (kind == DSPW_BC_HALO) return c;   // the stored halo layer beside the interior
   if (kind == DSPW_BC_PERIODIC) return ((c % N) + N) % N;
   if (kind == DSPW_BC_WALL) { flip = 1; return c < 0 ? -1 - c : 2 * N - 1 - c; }
   return c < 0 ? 0 : N - 1;   // neumann (and dirichlet, which ignores it)

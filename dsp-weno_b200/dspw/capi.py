@@ -30,7 +30,7 @@ FLUX = {
 RECON = {"sp_weno": 0, "sp_wenoc": 1, "sp_weno_corr2": 2, "sp_weno_dl": 3,
          "first": 4, "second": 5, "minmod": 6, "minabs": 7, "eno2": 8,
          "eno3": 9}
-BC = {"periodic": 0, "dirichlet": 1, "neumann": 2, "wall": 3}
+BC = {"periodic": 0, "dirichlet": 1, "neumann": 2, "wall": 3, "halo": 4}
 TIME = {"rk1": 0, "ssprk3": 1, "jameson_rk4": 2, "rk4": 3}
 MU = {"constant": 0, "sutherland": 1, "power": 2}
 PRECISION = {"fp64": 0, "fp32_bf16": 1}
@@ -74,6 +74,13 @@ class StatusOut(C.Structure):
     _fields_ = [("code", C.c_int), ("nonfinite_cells", C.c_longlong), ("nonpositive_cells", C.c_longlong),
                 ("sign_violations", C.c_longlong), ("faces_checked", C.c_longlong),
                 ("limiter_acts", C.c_longlong)]
+
+
+class HaloOut(C.Structure):
+    """dspw_halo_out: device addresses of a slab's halo and boundary layers."""
+    _fields_ = [("recv_lo", C.c_void_p), ("recv_hi", C.c_void_p), ("send_lo", C.c_void_p),
+                ("send_hi", C.c_void_p), ("count", C.c_longlong), ("comp_stride", C.c_longlong),
+                ("ncomp", C.c_int), ("elem_bytes", C.c_int), ("ng", C.c_int), ("layer_cells", C.c_int)]
 
 
 class TrainCfg(C.Structure):
@@ -238,6 +245,7 @@ def lib():
         "dspw_snap_read": (I, [P, I, dp, C.POINTER(D), C.POINTER(I)]),
         "dspw_stream": (P, [P]),
         "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),
+        "dspw_halo_view": (I, [P, I, I, C.POINTER(HaloOut)]),
         "dspw_trainer_create": (I, [C.POINTER(TrainCfg), dp, dp, C.POINTER(P)]),
         "dspw_trainer_destroy": (I, [P]),
         "dspw_trainer_set_data": (I, [P, dp, dp, LL]),
@@ -412,6 +420,14 @@ class Solver:
 
     def step(self, n=1, fixed_dt=0.0):
         check(lib().dspw_step(self.h, int(n), float(fixed_dt)), "dspw_step")
+
+    def stage(self, rk, dt=0.0):
+        check(lib().dspw_stage(self.h, int(rk), float(dt)), "dspw_stage")
+
+    def halo_view(self, p=0, rk=0) -> HaloOut:
+        v = HaloOut()
+        check(lib().dspw_halo_view(self.h, int(p), int(rk), C.byref(v)), "dspw_halo_view")
+        return v
 
     def run(self, chunk=64):
         s = C.c_int()

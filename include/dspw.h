@@ -74,7 +74,14 @@ enum dspw_recon {
 /* boundary conditions (enflo/src/ext_constants.h:25).  DIRICHLET is parsed but
  * not implemented by the reference (enflo/src/parameter.cc:558-562); here it
  * means: ghost cells hold the fixed primitive state desc.bc_state[face]. */
-enum dspw_bc { DSPW_BC_PERIODIC = 0, DSPW_BC_DIRICHLET = 1, DSPW_BC_NEUMANN = 2, DSPW_BC_WALL = 3 };
+enum dspw_bc { DSPW_BC_PERIODIC = 0, DSPW_BC_DIRICHLET = 1, DSPW_BC_NEUMANN = 2, DSPW_BC_WALL = 3,
+  /* No counterpart in the reference: the face borders another slab of the same
+   * domain.  Its ghost layers (3 for eno 3, else 2) are stored beside the
+   * interior and filled by the caller before every stage from the
+   * neighbouring slab (dspw_halo_view).  Only on the faces of the problem's
+   * last swept direction (y of a 2-D problem, z of a 3-D one, x of a 1-D one),
+   * for the Euler and scalar models, without the per-step diagnostics. */
+  DSPW_BC_HALO = 4 };
 
 enum dspw_time { DSPW_RK1 = 0, DSPW_SSPRK3 = 1, DSPW_JAMESON_RK4 = 2, DSPW_RK4 = 3 };
 enum dspw_mu { DSPW_MU_CONSTANT = 0, DSPW_MU_SUTHERLAND = 1, DSPW_MU_POWER = 2 };
@@ -123,7 +130,9 @@ typedef struct dspw_desc {
   double bc_state[6][5];     /* DIRICHLET ghost state, primitive (rho,u,v,w,p) or (u) */
   double nn_w[4][5][5];      /* DSP-WENO layer weights, row = output, col = input */
   double nn_b[4][5];         /* DSP-WENO layer biases */
-  double reserved_d[8];
+  double reserved_d[8];      /* [2..4]: training box (reserved_i[0]); [5..7]: when > 0 the cell
+                                sizes dx, dy, dz instead of (max - min) / n, for the slabs of a
+                                decomposed domain (DSPW_BC_HALO), which keep the domain's */
 } dspw_desc;
 
 typedef struct dspw_handle dspw_handle;
@@ -321,6 +330,30 @@ DSPW_API int dspw_sync(dspw_handle* h);
 
 /* The handle's CUDA stream (a cudaStream_t) so callers can order their own work. */
 DSPW_API void* dspw_stream(dspw_handle* h);
+
+/* Halo layers of problem p in the state that stage rk reads (the state of the
+ * step's start for rk 0): per component c (0 .. ncomp-1) the `count`
+ * contiguous elements at recv_lo + c * comp_stride are the ghost layers below
+ * the first interior layer, those at recv_hi + c * comp_stride the ghost
+ * layers above the last; send_lo / send_hi are the first / last `ng` interior
+ * layers, which the lower / upper neighbour receives into its recv_hi /
+ * recv_lo.  Elements are elem_bytes wide (the handle's precision); pointers
+ * are device pointers of the handle's GPU.  A slab decomposition exchanges
+ * these before every dspw_stage and gives every slab the same dt (the minimum
+ * of their dspw_compute_dt).  DSPW_ERR_ARG unless a face of p is DSPW_BC_HALO. */
+typedef struct dspw_halo_out {
+  void* recv_lo;
+  void* recv_hi;
+  void* send_lo;
+  void* send_hi;
+  long long count;           /* elements per component and side: ng x layer cells */
+  long long comp_stride;     /* elements between component planes */
+  int ncomp;
+  int elem_bytes;
+  int ng;                    /* ghost layers per side */
+  int layer_cells;           /* cells of one layer across the decomposed direction */
+} dspw_halo_out;
+DSPW_API int dspw_halo_view(dspw_handle* h, int p, int rk, dspw_halo_out* out);
 
 /* Raw device pointer to the conserved state planes of problem p (component
  * stride in elements returned in *stride) and the element size in bytes (8 or 4). */

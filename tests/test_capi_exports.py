@@ -61,6 +61,18 @@ def test_bad_descriptor_rejected_without_gpu():
     # eno 3 on a wall axis of two cells: the third ghost's mirror leaves the line
     d = capi.make_desc(recon="eno3", nx=16, ny=2, bc=["periodic", "periodic", "wall", "wall", "periodic", "periodic"])
     assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 6
+    # halo faces: only on the last swept direction, not for Navier-Stokes, and
+    # with at least one ghost width of layers
+    d = capi.make_desc(nx=16, ny=8, bc=["halo", "halo", "periodic", "periodic", "periodic", "periodic"])
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 6
+    d = capi.make_desc(model="ns_es", nx=8, ny=8, nz=8, mu_ref=0.01,
+                       bc=["periodic", "periodic", "periodic", "periodic", "halo", "halo"])
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 6
+    d = capi.make_desc(nx=16, ny=2, bc=["periodic", "periodic", "halo", "halo", "periodic", "periodic"],
+                       recon="eno3")
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 6
+    d = capi.make_desc(nx=16, ny=8, bc=["periodic", "periodic", "halo", "periodic", "periodic", "periodic"])
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1   # periodic pairs with periodic only
     # the four-cell reconstruction entry point has no six-cell stencils
     l, r, acts = np.zeros(1), np.zeros(1), ctypes.c_longlong()
     u = np.arange(4, dtype=np.float64)
