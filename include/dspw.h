@@ -80,7 +80,10 @@ enum dspw_bc { DSPW_BC_PERIODIC = 0, DSPW_BC_DIRICHLET = 1, DSPW_BC_NEUMANN = 2,
    * interior and filled by the caller before every stage from the
    * neighbouring slab (dspw_halo_view).  Only on the faces of the problem's
    * last swept direction (y of a 2-D problem, z of a 3-D one, x of a 1-D one),
-   * for the Euler and scalar models, without the per-step diagnostics. */
+   * for the Euler and scalar models, without the per-step diagnostics.
+   * dspw_step / dspw_run do not exchange: a slab steps through dspw_stage with
+   * its layers filled before each call (the stored layers stay inside the
+   * slab's own storage, so stale ones give wrong values, never bad reads). */
   DSPW_BC_HALO = 4 };
 
 enum dspw_time { DSPW_RK1 = 0, DSPW_SSPRK3 = 1, DSPW_JAMESON_RK4 = 2, DSPW_RK4 = 3 };
