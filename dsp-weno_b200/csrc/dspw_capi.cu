@@ -2,6 +2,9 @@
 // device buffers, per-problem tables, the per-step CUDA graph and the
 // host<->device copies.  All arithmetic runs in the kernels of
 // dspw_kernels.cuh (instantiated by dspw_fp64.cu / dspw_fp32.cu).
+#include <dlfcn.h>
+#include <nccl.h>
+
 #include <algorithm>
 #include <cmath>
 #include <deque>
@@ -149,6 +152,10 @@ struct dspw_handle {
   int time_scheme = 1;
   int has_ns = 0;
   int has_halo = 0;   // some problem stores halo layers (DSPW_BC_HALO faces)
+  // slab of a decomposition over NCCL ranks (dspw_slab_connect): the step
+  // graph exchanges halo layers with the neighbours and reduces the CFL speed
+  ncclComm_t comm = nullptr;
+  int rank = 0, nranks = 1, up = -1, down = -1;
   int maxdim = 1;
   std::vector<SweepClass> classes;
   std::vector<dspw_desc> desc;
@@ -605,9 +612,15 @@ cudaError_t launch_class_sweep(dspw_handle* h, SweepArgs<T> a, const SweepClass&
   return Launch<T>::sweep(dir, a, grid, h->stream, c.spec);
 }
 
+int enqueue_halo_exchange(dspw_handle* h, int rk);
+
 template <typename T>
 int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
   SweepArgs<T> a = stage_args<T>(h, rk, residual_only);
+  if (!residual_only) {   // the collective path only (residuals and tuning stay rank-local)
+    int rx = enqueue_halo_exchange(h, rk);
+    if (rx) return rx;
+  }
   if (h->has_ns) {
     CK(Launch<T>::entvars(h->dprob, h->nprob, h->dcell_start, h->ctot, a.Uin, h->ctot, (T*)h->V, h->stream));
     prof_mark(h, "entvars");
@@ -742,8 +755,103 @@ int enqueue_end_step(dspw_handle* h) {
   return h->precision == DSPW_FP64 ? enqueue_end_step_t<double>(h) : enqueue_end_step_t<float>(h);
 }
 
+// NCCL, opened at run time (the process's own libnccl.so.2 when one is loaded,
+// e.g. by torch), so that the library loads and runs without it
+struct NcclApi {
+  bool ok = false;
+  ncclResult_t (*get_unique_id)(ncclUniqueId*) = nullptr;
+  ncclResult_t (*comm_init_rank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+  ncclResult_t (*comm_destroy)(ncclComm_t) = nullptr;
+  ncclResult_t (*send)(const void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*recv)(void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*group_start)() = nullptr;
+  ncclResult_t (*group_end)() = nullptr;
+  ncclResult_t (*all_reduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                             cudaStream_t) = nullptr;
+};
+
+const NcclApi& nccl() {
+  static const NcclApi api = [] {
+    NcclApi a;
+    void* lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!lib) return a;
+    a.get_unique_id = (decltype(a.get_unique_id))dlsym(lib, "ncclGetUniqueId");
+    a.comm_init_rank = (decltype(a.comm_init_rank))dlsym(lib, "ncclCommInitRank");
+    a.comm_destroy = (decltype(a.comm_destroy))dlsym(lib, "ncclCommDestroy");
+    a.send = (decltype(a.send))dlsym(lib, "ncclSend");
+    a.recv = (decltype(a.recv))dlsym(lib, "ncclRecv");
+    a.group_start = (decltype(a.group_start))dlsym(lib, "ncclGroupStart");
+    a.group_end = (decltype(a.group_end))dlsym(lib, "ncclGroupEnd");
+    a.all_reduce = (decltype(a.all_reduce))dlsym(lib, "ncclAllReduce");
+    a.ok = a.get_unique_id && a.comm_init_rank && a.comm_destroy && a.send && a.recv && a.group_start &&
+           a.group_end && a.all_reduce;
+    return a;
+  }();
+  return api;
+}
+
+#define NCK(x)                                                     \
+  do {                                                             \
+    if ((x) != ncclSuccess) {                                      \
+      h->last_error = DSPW_ERR_CUDA;                               \
+      return DSPW_ERR_CUDA;                                        \
+    }                                                              \
+  } while (0)
+
+// CFL speed of the newest state in slot 0 (max of the slots), the others
+// cleared: the value an all-reduce(max) over the ranks combines
+__global__ void k_smax_pack(ProbState* st) {
+  unsigned long long m = 0ull;
+  for (int k = 0; k < EPI_SLOTS; k++) m = st->smax[k] > m ? st->smax[k] : m;
+  for (int k = 1; k < EPI_SLOTS; k++) st->smax[k] = 0ull;
+  st->smax[0] = m;
+}
+
+// the speed of the whole decomposed domain: max over the ranks of each
+// slab's (non-negative doubles order as their bit patterns)
+int enqueue_speed_reduce(dspw_handle* h) {
+  if (!h->comm) return DSPW_OK;
+  k_smax_pack<<<1, 1, 0, h->stream>>>(h->dst);
+  CK(cudaGetLastError());
+  unsigned long long* s0 = (unsigned long long*)((char*)h->dst + offsetof(ProbState, smax));
+  NCK(nccl().all_reduce(s0, s0, 1, ncclUint64, ncclMax, h->comm, h->stream));
+  return DSPW_OK;
+}
+
+// Halo layers of the state stage rk reads, from the neighbouring ranks: phase
+// 1 upwards (send_hi to the upper rank, recv_lo from the lower), phase 2
+// downwards, each one NCCL group in which every pair of ranks has one message
+// per component in component order on both sides, so the pairs match also
+// when both neighbours are one rank (two slabs, periodic) or this rank itself
+// (one periodic slab).
+int enqueue_halo_exchange(dspw_handle* h, int rk) {
+  if (!h->comm) return DSPW_OK;
+  dspw_halo_out v;
+  if (dspw_halo_view(h, 0, rk, &v) != DSPW_OK) return DSPW_OK;   // no halo faces: nothing to exchange
+  const ncclDataType_t t = h->elem == 8 ? ncclFloat64 : ncclFloat32;
+  const size_t cs = (size_t)v.comp_stride * h->elem;
+  const NcclApi& n = nccl();
+  NCK(n.group_start());
+  for (int c = 0; c < v.ncomp; c++) {
+    if (h->up >= 0) NCK(n.send((char*)v.send_hi + c * cs, v.count, t, h->up, h->comm, h->stream));
+    if (h->down >= 0) NCK(n.recv((char*)v.recv_lo + c * cs, v.count, t, h->down, h->comm, h->stream));
+  }
+  NCK(n.group_end());
+  NCK(n.group_start());
+  for (int c = 0; c < v.ncomp; c++) {
+    if (h->down >= 0) NCK(n.send((char*)v.send_lo + c * cs, v.count, t, h->down, h->comm, h->stream));
+    if (h->up >= 0) NCK(n.recv((char*)v.recv_hi + c * cs, v.count, t, h->up, h->comm, h->stream));
+  }
+  NCK(n.group_end());
+  return DSPW_OK;
+}
+
 int enqueue_step(dspw_handle* h, double fixed_dt) {
   CK(cudaMemsetAsync(h->dnactive, 0, sizeof(int), h->stream));
+  if (fixed_dt <= 0) {
+    int rs = enqueue_speed_reduce(h);
+    if (rs) return rs;
+  }
   CK(launch_begin_step(h->dprob, h->dst, h->nprob, fixed_dt, h->dnactive, h->stream));
   prof_mark(h, "begin_step");
   for (int rk = 0; rk < h->nrk; rk++) {
@@ -951,6 +1059,7 @@ int dspw_destroy(dspw_handle* h) {
   if (!h) return DSPW_ERR_ARG;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->comm) nccl().comm_destroy(h->comm);
   void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive,
                   h->Un, h->Ua, h->Ub, h->R, h->R2, h->V, h->node, h->dstage, h->dscratch,
                   h->ddiag, h->drows, h->dnode_start, h->dsnap, h->dsnap_count, h->dsnap_meta};
@@ -1056,6 +1165,10 @@ int dspw_stage(dspw_handle* h, int rk, double dt) {
   if (!h || rk < 0 || rk >= h->nrk) return DSPW_ERR_ARG;
   if (rk == 0) {
     CK(cudaMemsetAsync(h->dnactive, 0, sizeof(int), h->stream));
+    if (dt <= 0) {
+      int rs = enqueue_speed_reduce(h);
+      if (rs) return rs;
+    }
     CK(launch_begin_step(h->dprob, h->dst, h->nprob, dt, h->dnactive, h->stream));
   }
   int r = enqueue_stage_any(h, rk, 0);
@@ -1386,6 +1499,39 @@ int dspw_sync(dspw_handle* h) {
 }
 
 void* dspw_stream(dspw_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int dspw_nccl_id(unsigned char id[128]) {
+  if (!id) return DSPW_ERR_ARG;
+  if (!nccl().ok) return DSPW_ERR_UNSUPPORTED;
+  ncclUniqueId u;
+  if (nccl().get_unique_id(&u) != ncclSuccess) return DSPW_ERR_CUDA;
+  static_assert(sizeof(u) == 128, "ncclUniqueId is 128 bytes");
+  memcpy(id, &u, sizeof(u));
+  return DSPW_OK;
+}
+
+int dspw_slab_connect(dspw_handle* h, const unsigned char id[128], int rank, int nranks) {
+  if (!h || !id || nranks < 1 || rank < 0 || rank >= nranks || h->nprob != 1 || h->comm) return DSPW_ERR_ARG;
+  if (!nccl().ok) return DSPW_ERR_UNSUPPORTED;
+  const dspw_desc& d = h->desc[0];
+  const int D = problem_dim(d) - 1;
+  const bool lo_halo = d.bc[2 * D] == DSPW_BC_HALO, hi_halo = d.bc[2 * D + 1] == DSPW_BC_HALO;
+  // a periodic domain wraps its first and last slab around; an inner slab
+  // has halo faces on both sides
+  if ((rank > 0 && !lo_halo) || (rank + 1 < nranks && !hi_halo)) return DSPW_ERR_ARG;
+  ncclUniqueId u;
+  memcpy(&u, id, sizeof(u));
+  CK(cudaStreamSynchronize(h->stream));
+  ncclComm_t c = nullptr;
+  if (nccl().comm_init_rank(&c, nranks, u, rank) != ncclSuccess) return DSPW_ERR_CUDA;
+  h->comm = c;
+  h->rank = rank;
+  h->nranks = nranks;
+  h->down = lo_halo ? (rank > 0 ? rank - 1 : nranks - 1) : -1;
+  h->up = hi_halo ? (rank + 1 < nranks ? rank + 1 : 0) : -1;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // the step graph changes
+  return DSPW_OK;
+}
 
 int dspw_halo_view(dspw_handle* h, int p, int rk, dspw_halo_out* out) {
   if (check_p(h, p) || !out || rk < 0 || rk >= h->nrk) return DSPW_ERR_ARG;

@@ -246,6 +246,8 @@ def lib():
         "dspw_stream": (P, [P]),
         "dspw_device_state": (I, [P, I, C.POINTER(P), C.POINTER(LL), C.POINTER(I)]),
         "dspw_halo_view": (I, [P, I, I, C.POINTER(HaloOut)]),
+        "dspw_nccl_id": (I, [C.c_char_p]),
+        "dspw_slab_connect": (I, [P, C.c_char_p, I, I]),
         "dspw_trainer_create": (I, [C.POINTER(TrainCfg), dp, dp, C.POINTER(P)]),
         "dspw_trainer_destroy": (I, [P]),
         "dspw_trainer_set_data": (I, [P, dp, dp, LL]),

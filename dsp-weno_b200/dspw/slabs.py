@@ -128,6 +128,26 @@ def exchange_layers(send_lo, send_hi, recv_lo, recv_hi, rank: int, world: int, p
                 r.wait()
 
 
+def connect(sol: Solver, rank: int, world: int, group=None):
+    """Connect a one-slab handle to its neighbours over NCCL (dspw_slab_connect):
+    rank 0 makes the NCCL id and the group hands it to every rank.  The
+    handle's steps then exchange halo layers and reduce the CFL speed on the
+    GPU, inside its step graph."""
+    import ctypes
+
+    from .capi import check, lib
+    buf = ctypes.create_string_buffer(128)
+    if rank == 0:
+        check(lib().dspw_nccl_id(buf), "dspw_nccl_id")
+    raw = buf.raw
+    if world > 1:
+        import torch.distributed as dist
+        obj = [raw]
+        dist.broadcast_object_list(obj, src=0, group=group)
+        raw = obj[0]
+    check(lib().dspw_slab_connect(sol.h, raw, int(rank), int(world)), "dspw_slab_connect")
+
+
 class _SlabsBase:
     def upload_prim(self, prim):
         """prim: the domain's primitive planes (nvar, nz, ny, nx)."""
@@ -207,7 +227,7 @@ class DistSlabs(_SlabsBase):
     Every rank's kernels have finished before its exchange starts: no kernel
     waits on another rank."""
 
-    def __init__(self, desc: Desc, rank: int, world: int, group=None):
+    def __init__(self, desc: Desc, rank: int, world: int, group=None, device_exchange=False):
         import torch
         self.D = problem_dim(desc) - 1
         self.periodic = desc.bc[2 * self.D] == BC["periodic"]
@@ -216,6 +236,17 @@ class DistSlabs(_SlabsBase):
         self.sol, self.lo, self.hi = Solver(d), lo, hi
         self.nrk = {0: 1, 1: 3}.get(desc.time_scheme, 4)
         self.device = torch.device("cuda", torch.cuda.current_device())
+        # device_exchange: the library's NCCL path (halo layers and dt on the
+        # GPU inside the step graph, no host round trip per stage)
+        self.device_exchange = bool(device_exchange)
+        if self.device_exchange:
+            connect(self.sol, rank, world, group)
+
+    def step(self, n=1):
+        if self.device_exchange:
+            self.sol.step(n)
+        else:
+            super().step(n)
 
     def _mine(self):
         return [(self.sol, self.lo, self.hi)]
@@ -260,4 +291,4 @@ class DistSlabs(_SlabsBase):
         return self.sol.cons()
 
 
-__all__ = ["split", "layer_ranges", "exchange_layers", "layer_tensors", "LocalSlabs", "DistSlabs"]
+__all__ = ["split", "layer_ranges", "exchange_layers", "layer_tensors", "connect", "LocalSlabs", "DistSlabs"]

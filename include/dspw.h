@@ -81,9 +81,10 @@ enum dspw_bc { DSPW_BC_PERIODIC = 0, DSPW_BC_DIRICHLET = 1, DSPW_BC_NEUMANN = 2,
    * neighbouring slab (dspw_halo_view).  Only on the faces of the problem's
    * last swept direction (y of a 2-D problem, z of a 3-D one, x of a 1-D one),
    * for the Euler and scalar models, without the per-step diagnostics.
-   * dspw_step / dspw_run do not exchange: a slab steps through dspw_stage with
-   * its layers filled before each call (the stored layers stay inside the
-   * slab's own storage, so stale ones give wrong values, never bad reads). */
+   * Unless the handle is connected (dspw_slab_connect), dspw_step / dspw_run
+   * do not exchange: a slab then steps through dspw_stage with its layers
+   * filled before each call (the stored layers stay inside the slab's own
+   * storage, so stale ones give wrong values, never bad reads). */
   DSPW_BC_HALO = 4 };
 
 enum dspw_time { DSPW_RK1 = 0, DSPW_SSPRK3 = 1, DSPW_JAMESON_RK4 = 2, DSPW_RK4 = 3 };
@@ -357,6 +358,23 @@ typedef struct dspw_halo_out {
   int layer_cells;           /* cells of one layer across the decomposed direction */
 } dspw_halo_out;
 DSPW_API int dspw_halo_view(dspw_handle* h, int p, int rk, dspw_halo_out* out);
+
+/* A new NCCL unique id (128 bytes) for dspw_slab_connect: one rank makes it
+ * and the caller hands it to every rank.  NCCL is opened at run time
+ * (libnccl.so.2); DSPW_ERR_UNSUPPORTED without it. */
+DSPW_API int dspw_nccl_id(unsigned char id[128]);
+
+/* Make the one-problem handle h slab `rank` of `nranks` (one GPU each) of a
+ * decomposed domain.  From then on every step of dspw_step / dspw_run, and
+ * dspw_stage, fills the halo layers from the neighbouring ranks with NCCL
+ * sends and receives on the handle's stream before every stage (inside the
+ * step graph), and a step's CFL dt is the domain's: an NCCL all-reduce(max)
+ * of the wave speed.  Those calls are then collective: every rank makes them
+ * in the same order with the same arguments.  Residuals, dspw_compute_dt and
+ * dspw_tune stay local.  Neighbours: rank - 1 below and rank + 1 above through
+ * the DSPW_BC_HALO faces, wrapping around when the first slab's lower face
+ * (and the last's upper face) is a halo face. */
+DSPW_API int dspw_slab_connect(dspw_handle* h, const unsigned char id[128], int rank, int nranks);
 
 /* Raw device pointer to the conserved state planes of problem p (component
  * stride in elements returned in *stride) and the element size in bytes (8 or 4). */

@@ -148,3 +148,33 @@ def test_rank_slabs_reproduce_the_undivided_problem(name, world):
     for rank, lo, hi, local in parts:
         want = ref[:, lo:hi] if D == 2 else ref[:, :, lo:hi]
         assert np.array_equal(local, want), (name, rank)
+
+
+@pytest.mark.parametrize("name", ["kh2d_fp64_3slabs", "kh2d_fp32_dl_4slabs", "euler3d_eno3_3slabs",
+                                  "burgers1d_3slabs", "kh2d_rk4_3slabs"])
+def test_nccl_slab_in_the_step_graph(name):
+    """One slab connected over NCCL (dspw_slab_connect, one rank): a periodic
+    domain's slab sends its boundary layers to itself and receives them as
+    its halo, and all-reduces its CFL speed, inside the step graph; a walled
+    domain's slab has no halo faces and only reduces.  Both equal the
+    undivided problem's own graph steps bit for bit, and so do stages issued
+    one by one (dspw_stage with the dt of the graph's rule)."""
+    from dspw.slabs import connect, split
+    kw, _ = CASES[name]
+    d = make_desc(network=net(), cfl=0.4, final_time=10.0, **dict(kw))
+    nv = 1 if kw.get("model") == "burgers" else 5
+    p0 = state(nv, d.nx, d.ny, d.nz, seed=len(name))
+    ref = Solver(d)
+    ref.upload_prim(p0)
+    ref.step(5)
+    sd, lo, hi = split(d, 1)[0]
+    s = Solver(sd)
+    s.upload_prim(p0)
+    connect(s, 0, 1)
+    s.step(3)
+    nrk = {"rk4": 4}.get(kw.get("time_scheme", "ssprk3"), 3)
+    for _ in range(2):
+        for rk in range(nrk):
+            s.stage(rk, 0.0)
+    assert np.array_equal(s.cons(), ref.cons()), name
+    assert s.globals().time == ref.globals().time and s.globals().iter == 5
