@@ -207,6 +207,45 @@ def build_workload(args, precision, recon, rank, world):
     return d, p, c, sum(cells), "strong"
 
 
+def measure_slabs(args, torch, dist, rank, world, config):
+    """One KH domain cut into `world` slabs along y, one per rank, connected
+    over NCCL: each rank's step graph exchanges its halo layers before every
+    stage and all-reduces the CFL speed (strong scaling of one problem).
+    Returns the JSON line (rank 0) or None."""
+    from dspw import load_network_file, workloads as W
+    from dspw.slabs import DistSlabs
+
+    n = args.n or 2048
+    (d,), (p0,), _ = W.kh(n, args.precision, args.recon, load_network_file(NET_FILE), seed=12345)
+    sl = DistSlabs(d, rank, world, device_exchange=True)
+    sl.upload_prim(p0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.ExternalStream(sl.sol.stream_ptr(), device=dev)
+    sl.step(args.warmup)
+    sl.sol.sync()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sl.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    st = sl.sol.status()
+    if rank != 0:
+        return None
+    return {"metric": METRIC, "value": n * n * args.steps / (ms * 1e-3), "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32_bf16" else "f64",
+            "data": "synthetic", "config": config, "slab_layers": [sl.lo, sl.hi],
+            "health": {"code": st.code, "nonfinite": st.nonfinite_cells, "sign_violations": st.sign_violations}}
+
+
 def kernel_class(d, dim):
     """Sweep kernel class of a problem (the library's spec_of): Euler / NS with a
     kepes_tecno4 flux run the kernels specialised for their dimension and
@@ -414,11 +453,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="kh", choices=["kh", "shu_osher", "batched", "tgv", "matched_error"],
+    ap.add_argument("--workload", default="kh",
+                    choices=["kh", "shu_osher", "batched", "tgv", "matched_error", "kh_slabs"],
                     help="kh: 2-D Euler KH (the headline); shu_osher: 1-D Euler; batched: vortex OOC list plus "
                          "4096 Burgers problems in one batch (shared out over ranks); tgv: 3-D Navier-Stokes "
                          "Taylor-Green vortex; matched_error: time to equal L1 error of the two forms on "
-                         "Shu-Osher and the isentropic vortex (its own JSON line)")
+                         "Shu-Osher and the isentropic vortex (its own JSON line); kh_slabs: one KH domain "
+                         "cut into one slab per rank, halo layers over NCCL inside the step graphs")
     ap.add_argument("--n", type=int, default=None, help="grid size (kh 2048, shu_osher 25600, tgv 256)")
     ap.add_argument("--precision", default="fp32_bf16", choices=["fp32_bf16", "fp64"])
     ap.add_argument("--recon", default="sp_weno_dl")
@@ -452,6 +493,11 @@ def main():
         config = {"workload": f"shu_osher{n}_{args.precision}_{args.recon}_kepes_tecno4_roe", "grid": [n],
                   "model": "euler1d", "flux": "kepes_tecno4_roe", "recon": args.recon, "precision": args.precision,
                   "cfl": 0.4}
+    elif args.workload == "kh_slabs":
+        n = args.n or 2048
+        config = {"workload": f"kh{n}_slabs{world}_{args.precision}_{args.recon}_kepes_tecno4_roe", "grid": [n, n],
+                  "model": "euler2d", "flux": "kepes_tecno4_roe", "recon": args.recon, "precision": args.precision,
+                  "cfl": 0.4, "decomposition": f"{world} slabs of y rows, one per rank, 2 halo rows per side"}
     elif args.workload == "batched":
         config = {"workload": f"batched_vortex_ooc_burgers4096_{args.precision}_{args.recon}",
                   "problems": "isentropic vortex at 64..2048^2 (6 levels, kepes_tecno4_roe) + 4096 Burgers "
@@ -523,6 +569,17 @@ def main():
         dist = tdist
     else:
         torch.cuda.set_device(0)
+    if args.workload == "kh_slabs":
+        line = measure_slabs(args, torch, dist, rank, world, config)
+        if dist is not None:
+            dist.barrier()
+        if line is not None:
+            print(json.dumps(line))
+        import gc
+        gc.collect()   # the slab's handle (and its NCCL communicator) before the process group
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     r = measure_gpu(args, torch, dist, rank, world)
     if r is None:
         return
