@@ -73,6 +73,10 @@ def test_bad_descriptor_rejected_without_gpu():
     assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 6
     d = capi.make_desc(nx=16, ny=8, bc=["periodic", "periodic", "halo", "periodic", "periodic", "periodic"])
     assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1   # periodic pairs with periodic only
+    # slab entry points: bad handles and views are refused on the host
+    assert lib.dspw_slab_connect(None, b"\0" * 128, 0, 1) == 1
+    assert lib.dspw_halo_view(None, 0, 0, ctypes.byref(capi.HaloOut())) == 1
+    assert lib.dspw_nccl_id(None) == 1
     # the four-cell reconstruction entry point has no six-cell stencils
     l, r, acts = np.zeros(1), np.zeros(1), ctypes.c_longlong()
     u = np.arange(4, dtype=np.float64)
