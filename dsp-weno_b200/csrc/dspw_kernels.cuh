@@ -1265,22 +1265,29 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   // group 1: staged rows q = 0 .. ncell+3 (cells c0-2 .. c0+ncell+1)
   const int nrow = ncell + 4;
   if (aligned) {
-    for (int idx = tid; idx < nv * nrow * CH; idx += WARPS_PER_BLOCK * 32) {
-      const int comp = idx / (nrow * CH), rem = idx - comp * nrow * CH, q = rem / CH, ch = rem - q * CH;
+    // one thread per (row, 16-byte chunk): its ghost source is found once and
+    // it issues the copies of every component (no division by the row count)
+    static_assert((SEG_CELLS + 4) * CH <= WARPS_PER_BLOCK * 32, "one pass of the block covers the staged rows");
+    if (tid < nrow * CH) {
+      const int q = tid / CH, ch = tid - q * CH;
       const int c = c0 - 2 + q;
       const int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + (c < 0 ? 0 : 1)];
-      if (kind == DSPW_BC_DIRICHLET) continue;
-      int flip;
-      const int src = ghost_source(c, N, kind, flip);
-      cp_async16(&tl.U[comp][q][ch * VEC], A.Uin + comp * A.ctot + cell_index<DIR>(P, i0 + ch * VEC, j0, k0, src));
+      if (kind != DSPW_BC_DIRICHLET) {
+        int flip;
+        const int src = ghost_source(c, N, kind, flip);
+        const long long base = cell_index<DIR>(P, i0 + ch * VEC, j0, k0, src);
+        for (int comp = 0; comp < nv; comp++) cp_async16(&tl.U[comp][q][ch * VEC], A.Uin + comp * A.ctot + base);
+      }
     }
     cp_async_commit();
     // group 2: residual (the previous sweep's) and U^n of the cells
-    for (int idx = tid; idx < nv * ncell * CH; idx += WARPS_PER_BLOCK * 32) {
-      const int comp = idx / (ncell * CH), rem = idx - comp * ncell * CH, q = rem / CH, ch = rem - q * CH;
-      const long long off = comp * A.ctot + cell_index<DIR>(P, i0 + ch * VEC, j0, k0, c0 + q);
-      cp_async16(&tl.R[comp][q][ch * VEC], A.R + off);
-      if (final_sweep) cp_async16(&tl.Un[comp][q][ch * VEC], A.Un + off);
+    if (tid < ncell * CH) {
+      const int q = tid / CH, ch = tid - q * CH;
+      const long long base = cell_index<DIR>(P, i0 + ch * VEC, j0, k0, c0 + q);
+      for (int comp = 0; comp < nv; comp++) {
+        cp_async16(&tl.R[comp][q][ch * VEC], A.R + comp * A.ctot + base);
+        if (final_sweep) cp_async16(&tl.Un[comp][q][ch * VEC], A.Un + comp * A.ctot + base);
+      }
     }
     cp_async_commit();
     cp_async_wait<1>();
