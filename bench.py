@@ -48,9 +48,9 @@ NET_FILE = REPO / "tests" / "golden" / "dsp_weno.txt"
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant
 # launch per cell, from one ncu capture of that launch
 # (profiles/sweep_kernels_kh2048.md): KH 2048^2 FP32 DSP-WENO, last-stage y sweep,
-# 202.82 MB + 47.24 MB for 4194304 cells
+# 202.84 MB + 46.66 MB for 4194304 cells
 NCU_TRAFFIC_BYTES_PER_CELL = {
-    ("kh2048_fp32_bf16_sp_weno_dl_kepes_tecno4_roe", "sweep_y"): (202.824448e6 + 47.239680e6) / 4194304,
+    ("kh2048_fp32_bf16_sp_weno_dl_kepes_tecno4_roe", "sweep_y"): (202.842624e6 + 46.659328e6) / 4194304,
 }
 
 
