@@ -116,9 +116,20 @@ __global__ void k_check_prim(const double* prim, long long n, int nv, unsigned l
   }
 }
 
+int device_sms() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 148;
+  if (dev < 64 && cache[dev] > 0) return cache[dev];
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+  if (dev < 64) cache[dev] = n;
+  return n;
+}
+
 cudaError_t launch_check_prim(const double* prim, long long n, int nv, unsigned long long* bad, cudaStream_t s) {
   long long g = (n + 255) / 256;
-  if (g > 148LL * 8) g = 148LL * 8;
+  if (g > device_sms() * 8LL) g = device_sms() * 8LL;
   k_check_prim<<<(int)(g < 1 ? 1 : g), 256, 0, s>>>(prim, n, nv, bad);
   return cudaGetLastError();
 }
@@ -199,6 +210,7 @@ struct dspw_handle {
   void* node = nullptr;
   double* dstage = nullptr;
   double* dscratch = nullptr;
+  double* dred = nullptr;         // block rows of the deterministic reductions (reduce_rows_max() x 8)
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   double graph_dt = -1.0;
@@ -310,6 +322,18 @@ int validate(const dspw_desc& d) {
   for (int a = 0; a < 3; a++)   // periodic must pair with periodic (enflo/src/parameter.cc:570-581)
     if ((d.bc[2 * a] == DSPW_BC_PERIODIC) != (d.bc[2 * a + 1] == DSPW_BC_PERIODIC)) return DSPW_ERR_ARG;
   if (!(d.cfl > 0.0) || !(d.final_time >= 0.0) || d.max_iter < 1 || d.t_stamps < 1) return DSPW_ERR_ARG;
+  if (d.nn_use_box != 0 && d.nn_use_box != 1) return DSPW_ERR_ARG;
+  if (d.nn_use_box)
+    for (int k = 0; k < 5; k++)
+      if (!(d.nn_feat_lo[k] <= d.nn_feat_hi[k])) return DSPW_ERR_ARG;   // also rejects NaN bounds
+  if (d.generic_kernels != 0 && d.generic_kernels != 1) return DSPW_ERR_ARG;
+  for (int k = 0; k < 3; k++)
+    if (!(d.cell_size[k] >= 0.0) || !std::isfinite(d.cell_size[k])) return DSPW_ERR_ARG;
+  // unused slots stay zero, so that a later ABI version can give them a meaning
+  for (int k = 0; k < 6; k++)
+    if (d.reserved_i[k] != 0) return DSPW_ERR_ARG;
+  for (int k = 0; k < 5; k++)
+    if (d.reserved_d[k] != 0.0) return DSPW_ERR_ARG;
   return DSPW_OK;
 }
 
@@ -339,9 +363,9 @@ ProbDev make_prob(const dspw_desc& d, long long off) {
   P.dz = (d.zmax - d.zmin) / d.nz;
   // a slab of a decomposed domain keeps the domain's cell size bit for bit
   // (its own bounds divided by its own cell count need not round to it)
-  if (d.reserved_d[5] > 0.0) P.dx = d.reserved_d[5];
-  if (d.reserved_d[6] > 0.0) P.dy = d.reserved_d[6];
-  if (d.reserved_d[7] > 0.0) P.dz = d.reserved_d[7];
+  if (d.cell_size[0] > 0.0) P.dx = d.cell_size[0];
+  if (d.cell_size[1] > 0.0) P.dy = d.cell_size[1];
+  if (d.cell_size[2] > 0.0) P.dz = d.cell_size[2];
   P.hmin = std::min(P.dx, std::min(P.dy, P.dz));
   P.vol = P.dx * P.dy * P.dz;
   P.node_vol = (d.xmax - d.xmin) / (d.nx + 1) * (d.ymax - d.ymin) / (d.ny + 1) * (d.zmax - d.zmin) / (d.nz + 1);
@@ -404,15 +428,12 @@ NetParams make_net(const dspw_desc& dn) {
         np.wf[l][j][k] = (float)dn.nn_w[l][j][k];
       }
     }
-  // reserved_i[0] != 0: the network carries a training box of its inputs,
-  // upper bounds of the three delta features in reserved_d[2..4] (the tanh
-  // features are always in [-1, 1]); inputs outside use plain SP-WENO
-  np.use_box = dn.reserved_i[0];
+  // nn_use_box: the network carries a training box of its inputs; inputs
+  // outside it use plain SP-WENO
+  np.use_box = dn.nn_use_box ? 1 : 0;
   for (int k = 0; k < 5; k++) { np.feat_lo[k] = -1e30f; np.feat_hi[k] = 1e30f; }
-  if (np.use_box) {
-    for (int k = 0; k < 2; k++) { np.feat_lo[k] = -1.0f; np.feat_hi[k] = 1.0f; }
-    for (int k = 2; k < 5; k++) { np.feat_lo[k] = 0.0f; np.feat_hi[k] = (float)dn.reserved_d[k]; }
-  }
+  if (np.use_box)
+    for (int k = 0; k < 5; k++) { np.feat_lo[k] = (float)dn.nn_feat_lo[k]; np.feat_hi[k] = (float)dn.nn_feat_hi[k]; }
   return np;
 }
 
@@ -420,7 +441,7 @@ NetParams make_net(const dspw_desc& dn) {
 // central part plus TeCNO dissipation run the kernels specialised for their
 // dimension and reconstruction family; every other problem the generic ones.
 int spec_of(const ProbDev& P, const dspw_desc& d) {
-  if (d.reserved_i[1] == 1) return 0;   // generic kernels requested
+  if (d.generic_kernels == 1) return 0;   // generic kernels requested
   if (P.is_scalar)   // 1-D linear advection / Burgers with an SP-WENO-family or network reconstruction
     return (P.dim == 1 && P.recon < DSPW_REC_FIRST) ? scalar_spec_code(P.spw_corr < 0 ? 2 : 1) : 0;
   if (P.central != 0 || !P.fourth || !P.tecno || P.recon >= DSPW_REC_FIRST) return 0;
@@ -831,18 +852,29 @@ int enqueue_halo_exchange(dspw_handle* h, int rk) {
   const ncclDataType_t t = h->elem == 8 ? ncclFloat64 : ncclFloat32;
   const size_t cs = (size_t)v.comp_stride * h->elem;
   const NcclApi& n = nccl();
+  // a failed send / recv still closes its group, so that no NCCL group stays
+  // open on this thread
+#define NCKG(x)                                  \
+  do {                                           \
+    if ((x) != ncclSuccess) {                    \
+      n.group_end();                             \
+      h->last_error = DSPW_ERR_CUDA;             \
+      return DSPW_ERR_CUDA;                      \
+    }                                            \
+  } while (0)
   NCK(n.group_start());
   for (int c = 0; c < v.ncomp; c++) {
-    if (h->up >= 0) NCK(n.send((char*)v.send_hi + c * cs, v.count, t, h->up, h->comm, h->stream));
-    if (h->down >= 0) NCK(n.recv((char*)v.recv_lo + c * cs, v.count, t, h->down, h->comm, h->stream));
+    if (h->up >= 0) NCKG(n.send((char*)v.send_hi + c * cs, v.count, t, h->up, h->comm, h->stream));
+    if (h->down >= 0) NCKG(n.recv((char*)v.recv_lo + c * cs, v.count, t, h->down, h->comm, h->stream));
   }
   NCK(n.group_end());
   NCK(n.group_start());
   for (int c = 0; c < v.ncomp; c++) {
-    if (h->down >= 0) NCK(n.send((char*)v.send_lo + c * cs, v.count, t, h->down, h->comm, h->stream));
-    if (h->up >= 0) NCK(n.recv((char*)v.recv_hi + c * cs, v.count, t, h->up, h->comm, h->stream));
+    if (h->down >= 0) NCKG(n.send((char*)v.send_lo + c * cs, v.count, t, h->down, h->comm, h->stream));
+    if (h->up >= 0) NCKG(n.recv((char*)v.recv_hi + c * cs, v.count, t, h->up, h->comm, h->stream));
   }
   NCK(n.group_end());
+#undef NCKG
   return DSPW_OK;
 }
 
@@ -1023,6 +1055,7 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
     }
     CKC(cudaMalloc(&h->dstage, sizeof(double) * 5 * (size_t)std::max<long long>(h->maxcells, 1)));
     CKC(cudaMalloc(&h->dscratch, sizeof(double) * 16));
+    CKC(cudaMalloc(&h->dred, sizeof(double) * 8 * (size_t)reduce_rows_max()));
     CKC(cudaMemcpy(h->dprob, h->hprob.data(), sizeof(ProbDev) * nprob, cudaMemcpyHostToDevice));
     CKC(cudaMemset(h->dst, 0, sizeof(ProbState) * nprob));
     CKC(cudaMemset(h->dstatus, 0, sizeof(StatusDev)));
@@ -1061,7 +1094,7 @@ int dspw_destroy(dspw_handle* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   if (h->comm) nccl().comm_destroy(h->comm);
   void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive,
-                  h->Un, h->Ua, h->Ub, h->R, h->R2, h->V, h->node, h->dstage, h->dscratch,
+                  h->Un, h->Ua, h->Ub, h->R, h->R2, h->V, h->node, h->dstage, h->dscratch, h->dred,
                   h->ddiag, h->drows, h->dnode_start, h->dsnap, h->dsnap_count, h->dsnap_meta};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1161,6 +1194,16 @@ int dspw_residual(dspw_handle* h, int p, double* res) {
   return download(h, p, res, 0, h->R);
 }
 
+// first health error the device recorded since the last dspw_last_status
+// (DSPW_ERR_NONFINITE / DSPW_ERR_NONPOSITIVE), DSPW_OK if none; the counters
+// are left for dspw_last_status
+static int device_health(dspw_handle* h) {
+  int code = 0;
+  CK(cudaMemcpyAsync(&code, &h->dstatus->code, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return code;
+}
+
 int dspw_stage(dspw_handle* h, int rk, double dt) {
   if (!h || rk < 0 || rk >= h->nrk) return DSPW_ERR_ARG;
   if (rk == 0) {
@@ -1177,8 +1220,7 @@ int dspw_stage(dspw_handle* h, int rk, double dt) {
     r = enqueue_end_step(h);
     if (r) return r;
   }
-  CK(cudaStreamSynchronize(h->stream));
-  return DSPW_OK;
+  return device_health(h);
 }
 
 int dspw_step(dspw_handle* h, int nsteps, double fixed_dt) {
@@ -1194,7 +1236,9 @@ int dspw_step(dspw_handle* h, int nsteps, double fixed_dt) {
   CK(cudaStreamSynchronize(h->stream));
   r = drain_diag(h);
   if (r) return r;
-  return drain_snap(h);
+  r = drain_snap(h);
+  if (r) return r;
+  return device_health(h);
 }
 
 int dspw_run(dspw_handle* h, int chunk, int* steps) {
@@ -1237,11 +1281,10 @@ int dspw_run(dspw_handle* h, int chunk, int* steps) {
 int dspw_globals(dspw_handle* h, int p, dspw_globals_out* g) {
   if (check_p(h, p) || !g) return DSPW_ERR_ARG;
   long long n = ncells(h->desc[p]);
-  CK(cudaMemsetAsync(h->dscratch, 0, sizeof(double) * 8, h->stream));
   if (h->precision == DSPW_FP64)
-    CK(Launch<double>::globals(h->dprob, p, (const double*)h->Un, h->ctot, n, h->dscratch, h->stream));
+    CK(Launch<double>::globals(h->dprob, p, (const double*)h->Un, h->ctot, n, h->dred, h->dscratch, h->stream));
   else
-    CK(Launch<float>::globals(h->dprob, p, (const float*)h->Un, h->ctot, n, h->dscratch, h->stream));
+    CK(Launch<float>::globals(h->dprob, p, (const float*)h->Un, h->ctot, n, h->dred, h->dscratch, h->stream));
   double acc[8];
   ProbState s;
   CK(cudaMemcpyAsync(acc, h->dscratch, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
@@ -1397,11 +1440,12 @@ int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, double err
   if (check_p(h, p) || !exact || !err || comp < 0 || comp > 4) return DSPW_ERR_ARG;
   long long n = ncells(h->desc[p]);
   CK(cudaMemcpyAsync(h->dstage, exact, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemsetAsync(h->dscratch, 0, sizeof(double) * 3, h->stream));
   if (h->precision == DSPW_FP64)
-    CK(Launch<double>::errors(h->dprob, p, (const double*)h->Un, h->ctot, n, comp, h->dstage, h->dscratch, h->stream));
+    CK(Launch<double>::errors(h->dprob, p, (const double*)h->Un, h->ctot, n, comp, h->dstage, h->dred, h->dscratch,
+                              h->stream));
   else
-    CK(Launch<float>::errors(h->dprob, p, (const float*)h->Un, h->ctot, n, comp, h->dstage, h->dscratch, h->stream));
+    CK(Launch<float>::errors(h->dprob, p, (const float*)h->Un, h->ctot, n, comp, h->dstage, h->dred, h->dscratch,
+                             h->stream));
   double acc[3];
   CK(cudaMemcpyAsync(acc, h->dscratch, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));

@@ -984,7 +984,7 @@ __device__ inline void stage_combine(const SweepArgs<T>& A, const ProbDev& P, co
 // that yields U^(n+1).
 template <typename T>
 __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
-                                         const T R[5], T u[5], const T un[5], double& smax, T& ent,
+                                         const T R[5], T u[5], const T un[5], double& smax, double& ent,
                                          unsigned& bad_fin, unsigned& bad_pos) {
   stage_combine<T>(A, P, S, cell, R, u, un);
   store_cons<T>(A.Uout, A.ctot, cell, P.nv, u);
@@ -997,9 +997,10 @@ __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P
     double rho = p[0], pr = p[4];
     if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
     if (!isfinite(rho) || !isfinite(pr) || !isfinite((double)u[1]) || !isfinite((double)u[4])) bad_fin++;
-    // entropy -rho s / (gamma - 1), s = ln p - gamma ln rho, in the state's type
+    // entropy -rho s / (gamma - 1), s = ln p - gamma ln rho: the cell's term in
+    // the state's type, the sum in FP64
     const T sT = Mth<T>::log(p[4]) - T(P.gamma) * Mth<T>::log(p[0]);
-    ent += -p[0] * sT / T(P.gamma - 1.0);
+    ent += (double)(-p[0] * sT / T(P.gamma - 1.0));
   }
 }
 
@@ -1010,7 +1011,7 @@ __device__ inline void update_euler_cell(const SweepArgs<T>& A, const ProbDev& P
 template <typename T>
 __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, long long cell,
                                    bool first, bool final_sweep, const T Fl[5], const T Fr[5], int nv_eff,
-                                   double& smax, T& ent, unsigned& bad_fin, unsigned& bad_pos) {
+                                   double& smax, double& ent, unsigned& bad_fin, unsigned& bad_pos) {
   T R[5];
   if (first) {
 #pragma unroll
@@ -1054,7 +1055,7 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
       T pp[5] = {x, T(0), T(0), T(0), T(0)};
       double sp = wave_speed<T>(P, pp);
       if (sp > smax) smax = sp;   // NaN speeds are skipped, as std::min skips them in compute_dt
-      ent += T(0.5) * x * x;   // entropy u^2 / 2
+      ent += 0.5 * (double)x * (double)x;   // entropy u^2 / 2, summed in FP64
       if (!isfinite((double)x)) bad_fin++;
     }
     return;
@@ -1066,13 +1067,13 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
 }
 
 template <typename T>
-__device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax, T ent,
+__device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax, double ent,
                                      unsigned bad_fin, unsigned bad_pos, unsigned long long signv, int viol,
                                      unsigned checked) {
   if (A.final_stage && !A.residual_only) {
     unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
     warp_max_u64_lane0(sb);
-    const double es = warp_sum((double)ent);
+    const double es = warp_sum(ent);
     if (lane == 0) {
       const int sl = blockIdx.x & (EPI_SLOTS - 1);
       atomicMax(&S.smax[sl], sb);
@@ -1174,7 +1175,7 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
   double smax = 0.0;
-  T ent = T(0);
+  double ent = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
   if (lane < ncell) {
     T Fl[5], Fr[5];
@@ -1183,7 +1184,7 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
     long long cell = cell_index<DIR>(P, i0, j0, k0, c0 + lane);
     finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, P.nv, smax, ent, bad_fin, bad_pos);
   }
-  if (!final_sweep) { smax = 0.0; ent = T(0); }
+  if (!final_sweep) { smax = 0.0; ent = 0.0; }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
   warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
@@ -1344,7 +1345,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   if (aligned) cp_async_wait<0>();
   __syncthreads();
   double smax = 0.0;
-  T ent = T(0);
+  double ent = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
   for (int row = tid / COOP_COLS; row < ncell && col < ncols; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
     WarpSmem<T>* sc = sm0 + col;
@@ -1362,7 +1363,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
       update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
     }
   }
-  if (!final_sweep) { smax = 0.0; ent = T(0); }
+  if (!final_sweep) { smax = 0.0; ent = 0.0; }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
   warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
@@ -1435,7 +1436,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
   const bool first = (DIR == 0);
   const bool final_sweep = !A.residual_only && (DIR == P.dim - 1);
   double smax = 0.0;
-  T ent = T(0);
+  double ent = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
   if (lane < ncell) {
     T Fl[5] = {sm->F[0][lane], T(0), T(0), T(0), T(0)};
@@ -1633,62 +1634,119 @@ __global__ void k_download(const ProbDev* prob, int p, const T* U, long long cto
 
 // FP64 sums for dspw_globals: entropy (enflo/src/compute_global.cc:18-28 /
 // enflo_scalar/src_scalar/compute_global.cc:12-21), conserved totals, kinetic energy
+// Deterministic FP64 reductions.  Each block reduces its threads' values in a
+// fixed order (warp shuffles, then the warps in order) and stores one row of K
+// partials per block; k_sum_rows combines the rows in a fixed order.  The
+// grid of a launch depends only on the cell count and the device, so a state
+// gives the same bits on every call, whatever the scheduling.  Slots whose bit
+// is set in MAXMASK are maxima (a NaN wins), the others sums.
+template <int K, unsigned MAXMASK>
+__device__ inline void block_rows_store(double (&v)[K], double* rows) {
+  __shared__ double sh[K][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    if ((MAXMASK >> k) & 1u) {
+      for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_xor_sync(0xffffffffu, v[k], o);
+        v[k] = (x != x || x > v[k]) ? x : v[k];
+      }
+    } else {
+      v[k] = warp_sum(v[k]);
+    }
+    if (lane == 0) sh[k][w] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    const int k = threadIdx.x;
+    double s = sh[k][0];
+    for (int i = 1; i < nw; i++) {
+      const double x = sh[k][i];
+      s = ((MAXMASK >> k) & 1u) ? ((x != x || x > s) ? x : s) : s + x;
+    }
+    rows[(long long)blockIdx.x * K + k] = s;
+  }
+}
+
+// one block of 256 threads: thread t combines rows t, t + 256, ... in order,
+// then a fixed pairwise tree; out[k] receives slot k
+template <typename T, int K, unsigned MAXMASK>
+__global__ void __launch_bounds__(256) k_sum_rows(const double* rows, int nrows, double* out) {
+  __shared__ double sh[K][256];
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const bool mx = (MAXMASK >> k) & 1u;
+    double s = 0.0;
+    for (int i = t; i < nrows; i += 256) {
+      const double x = rows[(long long)i * K + k];
+      s = mx ? ((x != x || x > s) ? x : s) : s + x;
+    }
+    sh[k][t] = s;
+  }
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (t < h) {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const double a = sh[k][t], b = sh[k][t + h];
+        sh[k][t] = ((MAXMASK >> k) & 1u) ? ((b != b || b > a) ? b : a) : a + b;
+      }
+    }
+    __syncthreads();
+  }
+  if (t < K) out[t] = sh[t][0];
+}
+
+// total entropy, kinetic energy and conserved totals of problem p: one row of
+// 7 partials per block (rows), to be combined by k_sum_rows
 template <typename T>
-__global__ void k_globals(const ProbDev* prob, int p, const T* U, long long ctot, double* acc /* 7 */) {
+__global__ void __launch_bounds__(256) k_globals(const ProbDev* prob, int p, const T* U, long long ctot,
+                                                 double* rows /* 7 per block */) {
   const ProbDev& P = prob[p];
   long long n = (long long)P.nx * P.ny * P.nz;
-  double e = 0, ke = 0, tot[5] = {0, 0, 0, 0, 0};
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};   // entropy, ke, conserved 0..4
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     if (P.is_scalar) {
       double u = U[P.off + c];
-      e += 0.5 * u * u;
-      tot[0] += u;
+      v[0] += 0.5 * u * u;
+      v[2] += u;
     } else {
       T u[5], pr[5];
       load_cons<T>(U, ctot, P.off + c, P.nv, P.dim, u);
       cons_to_prim<T>(u, T(P.gamma), pr);
       double rho = pr[0], prs = pr[4];
       double s = ::log(prs) - P.gamma * ::log(rho);
-      e += -rho * s / (P.gamma - 1.0);
-      ke += 0.5 * rho * ((double)pr[1] * pr[1] + (double)pr[2] * pr[2] + (double)pr[3] * pr[3]);
-      for (int v = 0; v < 5; v++) tot[v] += (double)u[v];
+      v[0] += -rho * s / (P.gamma - 1.0);
+      v[1] += 0.5 * rho * ((double)pr[1] * pr[1] + (double)pr[2] * pr[2] + (double)pr[3] * pr[3]);
+      for (int k = 0; k < 5; k++) v[2 + k] += (double)u[k];
     }
   }
-  e = warp_sum(e); ke = warp_sum(ke);
-  for (int v = 0; v < 5; v++) tot[v] = warp_sum(tot[v]);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(acc + 0, e);
-    atomicAdd(acc + 1, ke);
-    for (int v = 0; v < 5; v++) atomicAdd(acc + 2 + v, tot[v]);
-  }
+  block_rows_store<7, 0u>(v, rows);
 }
 
-// L1 / L2^2 / Linf of (component comp of the primitive state) - exact
+// L1 / L2^2 / Linf of (component comp of the primitive state) - exact: one row
+// of 3 partials per block
 template <typename T>
-__global__ void k_errors(const ProbDev* prob, int p, const T* U, long long ctot, int comp, const double* exact,
-                         double* acc /* 3 */) {
+__global__ void __launch_bounds__(256) k_errors(const ProbDev* prob, int p, const T* U, long long ctot, int comp,
+                                                const double* exact, double* rows /* 3 per block */) {
   const ProbDev& P = prob[p];
   long long n = (long long)P.nx * P.ny * P.nz;
-  double l1 = 0, l2 = 0, li = 0;
+  double v[3] = {0, 0, 0};
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-    double v;
-    if (P.is_scalar) v = U[P.off + c];
+    double x;
+    if (P.is_scalar) x = U[P.off + c];
     else {
       T u[5], pr[5];
       load_cons<T>(U, ctot, P.off + c, P.nv, P.dim, u);
       cons_to_prim<T>(u, T(P.gamma), pr);
-      v = pr[comp];
+      x = pr[comp];
     }
-    double d = fabs(exact[c] - v);
-    l1 += d; l2 += d * d; li = fmax(li, d);
+    double d = fabs(exact[c] - x);
+    v[0] += d; v[1] += d * d;
+    v[2] = (d != d || d > v[2]) ? d : v[2];
   }
-  l1 = warp_sum(l1); l2 = warp_sum(l2);
-  for (int o = 16; o > 0; o >>= 1) li = fmax(li, __shfl_xor_sync(0xffffffffu, li, o));
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(acc + 0, l1);
-    atomicAdd(acc + 1, l2);
-    atomicMax((unsigned long long*)(acc + 2), (unsigned long long)__double_as_longlong(li));
-  }
+  block_rows_store<3, 4u>(v, rows);
 }
 
 // ---------------------------------------------------- Navier-Stokes (ES) --
@@ -1885,7 +1943,7 @@ template <typename T>
 __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const T* node) {
   long long total = cell_start[A.nprob];
   double smax = 0.0;
-  T ent = T(0);
+  double ent = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
   int pcur = -1;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
@@ -1936,7 +1994,7 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
       if (!(rho > 0.0) || !(pr > 0.0)) bad_pos++;
       if (!isfinite(rho) || !isfinite(pr)) bad_fin++;
       const T sT = Mth<T>::log(p[4]) - T(P.gamma) * Mth<T>::log(p[0]);
-      ent += -p[0] * sT / T(P.gamma - 1.0);
+      ent += (double)(-p[0] * sT / T(P.gamma - 1.0));
     }
   }
   // one speed-max and entropy flush per thread, warp-aggregated when the warp
@@ -1947,7 +2005,7 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
     if (uniform) {
       unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
       warp_max_u64_lane0(sb);
-      const double es = warp_sum((double)ent);
+      const double es = warp_sum(ent);
       if ((threadIdx.x & 31) == 0 && p0 >= 0) {
         const int sl = blockIdx.x & (EPI_SLOTS - 1);
         atomicMax(&A.st[p0].smax[sl], sb);
@@ -1956,7 +2014,7 @@ __global__ void k_visc_update(SweepArgs<T> A, const long long* cell_start, const
     } else if (pcur >= 0) {
       const int sl = blockIdx.x & (EPI_SLOTS - 1);
       atomicMax(&A.st[pcur].smax[sl], (unsigned long long)__double_as_longlong(smax));
-      atomicAdd(&A.st[pcur].ent_acc[sl], (double)ent);
+      atomicAdd(&A.st[pcur].ent_acc[sl], ent);
     }
   }
   if (bad_fin) { atomicAdd(&A.status->nonfinite, (unsigned long long)bad_fin); atomicCAS(&A.status->code, 0, DSPW_ERR_NONFINITE); }

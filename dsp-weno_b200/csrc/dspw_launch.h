@@ -22,10 +22,12 @@ struct Launch {
                            double* out, cudaStream_t s);
   static cudaError_t download(const ProbDev* prob, int p, const T* U, long long ctot, long long ncell, double* out,
                               int prim, cudaStream_t s);
-  static cudaError_t globals(const ProbDev* prob, int p, const T* U, long long ctot, long long ncell, double* acc,
-                             cudaStream_t s);
+  // deterministic FP64 sums: block partials in rows (reduce_rows_max() x 8
+  // doubles), combined in a fixed order into acc
+  static cudaError_t globals(const ProbDev* prob, int p, const T* U, long long ctot, long long ncell, double* rows,
+                             double* acc, cudaStream_t s);
   static cudaError_t errors(const ProbDev* prob, int p, const T* U, long long ctot, long long ncell, int comp,
-                            const double* exact, double* acc, cudaStream_t s);
+                            const double* exact, double* rows, double* acc, cudaStream_t s);
   static cudaError_t entvars(const ProbDev* prob, int nprob, const long long* cell_start, long long ncell_total,
                              const T* U, long long ctot, T* V, cudaStream_t s);
   static cudaError_t visc_nodes(const ProbDev* prob, int nprob, const long long* cell_start, long long ncell_total,
@@ -42,6 +44,12 @@ struct Launch {
   // snapshot of the problems that ended the step on a time stamp
   static cudaError_t snap(const SnapArgs<T>& a, long long ncell_total, cudaStream_t s);
 };
+
+// streaming multiprocessors of the current device (cached per device; 148
+// on a B200), for grid-stride launch sizes
+int device_sms();
+// most block rows of a deterministic reduction launch (grid_for's cap)
+inline long long reduce_rows_max() { return device_sms() * 32LL; }
 
 cudaError_t launch_begin_step(const ProbDev* prob, ProbState* st, int nprob, double fixed_dt, int* nactive,
                               cudaStream_t s);

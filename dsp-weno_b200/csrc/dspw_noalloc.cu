@@ -24,7 +24,11 @@
 // names a host-side stand-in).  The device address is obtained once per device
 // with cudaGetSymbolAddress, with that device current, on the first call made
 // on that device; that first call should therefore not be made while a stream
-// is being captured.
+// is being captured.  The address is kept together with the id of the CUDA
+// context it was taken in: after a cudaDeviceReset the device gets a new
+// context, where the library's module (and the array) may sit elsewhere, so
+// the first call in the new context looks the address up again (and, like the
+// very first call, should not be made during stream capture).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -119,16 +123,50 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_final_sums(const double (*r
 
 std::mutex g_setup_mutex;
 void* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+unsigned long long g_scratch_ctx[NOALLOC_MAX_DEVICES] = {};   // context id the address belongs to
 
-// device address of g_block_sums for the current device (set up once per device)
+// id of the current CUDA context (driver entry points cuCtxGetCurrent and
+// cuCtxGetId, found through the runtime; unique for the life of the process)
+int current_context_id(unsigned long long* id) {
+  typedef int (*GetCurrentFn)(void**);
+  typedef int (*GetIdFn)(void*, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || !f1)
+      return DSPW_ERR_CUDA;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess || !f2)
+      return DSPW_ERR_CUDA;
+    get_current = (GetCurrentFn)f1;
+    get_id = (GetIdFn)f2;
+  }
+  void* ctx = nullptr;
+  if (get_current(&ctx) != 0 || !ctx) return DSPW_ERR_CUDA;
+  if (get_id(ctx, id) != 0) return DSPW_ERR_CUDA;
+  return DSPW_OK;
+}
+
+// device address of g_block_sums for the current device, looked up once per
+// device and context
 int scratch_for_current_device(void** addr) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return DSPW_ERR_CUDA;
+  // cudaFree(0) makes the device's primary context current (a no-op when it is)
+  if (cudaFree(0) != cudaSuccess) return DSPW_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
+  unsigned long long ctx = 0;
+  int r = current_context_id(&ctx);
+  if (r) return r;
+  if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_block_sums) != cudaSuccess || !p) return DSPW_ERR_CUDA;
     g_scratch_addr[dev] = p;
+    g_scratch_ctx[dev] = ctx;
   }
   *addr = g_scratch_addr[dev];
   return DSPW_OK;
@@ -139,6 +177,8 @@ int scratch_for_current_device(void** addr) {
 extern "C" DSPW_API int dspw_globals_noalloc(const dspw_desc* desc, const void* d_cons, long long stride,
                                              int elem_bytes, double* d_out, void* stream) {
   if (!desc || !d_cons || !d_out || (elem_bytes != 4 && elem_bytes != 8)) return DSPW_ERR_ARG;
+  if (desc->abi_version != DSPW_ABI_VERSION) return DSPW_ERR_ARG;
+  if (desc->model < DSPW_LINADV || desc->model > DSPW_NS_KEP) return DSPW_ERR_ARG;
   if (desc->nx < 1 || desc->ny < 1 || desc->nz < 1) return DSPW_ERR_ARG;
   if (!(desc->xmax > desc->xmin) || !(desc->ymax > desc->ymin) || !(desc->zmax > desc->zmin)) return DSPW_ERR_ARG;
   SumParams p;
@@ -151,8 +191,15 @@ extern "C" DSPW_API int dspw_globals_noalloc(const dspw_desc* desc, const void* 
   p.nv = p.scalar ? 1 : dim + 2;
   p.gamma = desc->gamma;
   if (!p.scalar && !(p.gamma > 1.0)) return DSPW_ERR_ARG;
-  p.vol = ((desc->xmax - desc->xmin) / desc->nx) * ((desc->ymax - desc->ymin) / desc->ny) *
-          ((desc->zmax - desc->zmin) / desc->nz);
+  // cell sizes as the handle path takes them: a slab of a decomposed domain
+  // carries the domain's own in cell_size
+  double h[3] = {(desc->xmax - desc->xmin) / desc->nx, (desc->ymax - desc->ymin) / desc->ny,
+                 (desc->zmax - desc->zmin) / desc->nz};
+  for (int k = 0; k < 3; k++) {
+    if (!(desc->cell_size[k] >= 0.0)) return DSPW_ERR_ARG;
+    if (desc->cell_size[k] > 0.0) h[k] = desc->cell_size[k];
+  }
+  p.vol = h[0] * h[1] * h[2];
   void* scratch = nullptr;
   int r = scratch_for_current_device(&scratch);
   if (r) return r;

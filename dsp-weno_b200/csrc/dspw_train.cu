@@ -216,6 +216,32 @@ __global__ void k_feature_max(const float* data, long long cap, long long n, uns
   for (int k = 0; k < 5; k++) atomicMax(&out[k], __float_as_uint(fabsf(data[k * cap + i])));
 }
 
+// order-preserving map of a float onto an unsigned integer (negative values
+// reversed below the positive ones), so that unsigned atomicMin / atomicMax
+// find the smallest and largest float
+__device__ inline unsigned float_key(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+inline float key_float(unsigned k) {
+  const unsigned u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  float f;
+  memcpy(&f, &u, sizeof(f));
+  return f;
+}
+
+// smallest and largest value of each feature over the valid samples
+// (out[0..4] minima, out[5..9] maxima, as float_key)
+__global__ void k_feature_box(const float* data, long long cap, long long n, unsigned* out /* 10 */) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n || data[21 * cap + i] == 0.f) return;
+  for (int k = 0; k < 5; k++) {
+    const unsigned key = float_key(data[k * cap + i]);
+    atomicMin(&out[k], key);
+    atomicMax(&out[5 + k], key);
+  }
+}
+
 // One row of the reference trainer's data file per sample, in the column
 // order its reader slices (DSP-WENO_trainer/DSP-WENO_network_trainer.py:305-333
 // with tanh_theta: cell values 0-3, theta-, theta+ 4-5, the network inputs
@@ -538,6 +564,29 @@ int dspw_trainer_info(dspw_trainer* t, long long* nsamples, double* feature_max)
       memcpy(&f, &hmax[k], sizeof(f));
       feature_max[k] = f;
     }
+  }
+  return DSPW_OK;
+}
+
+int dspw_trainer_box(dspw_trainer* t, double lo[5], double hi[5]) {
+  if (!t || !lo || !hi || t->n < 1) return DSPW_ERR_ARG;
+  unsigned* d = nullptr;
+  unsigned h[10];
+  for (int k = 0; k < 5; k++) { h[k] = 0xffffffffu; h[5 + k] = 0u; }
+  if (cudaMalloc(&d, sizeof(h)) != cudaSuccess) return DSPW_ERR_NOMEM;
+  cudaError_t e = cudaMemcpyAsync(d, h, sizeof(h), cudaMemcpyHostToDevice, t->stream);
+  if (e == cudaSuccess) {
+    k_feature_box<<<(int)((t->n + TPB - 1) / TPB), TPB, 0, t->stream>>>(t->data, t->cap, t->n, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, t->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return DSPW_ERR_CUDA;
+  if (h[0] == 0xffffffffu) return DSPW_ERR_ARG;   // no valid sample
+  for (int k = 0; k < 5; k++) {
+    lo[k] = key_float(h[k]);
+    hi[k] = key_float(h[5 + k]);
   }
   return DSPW_OK;
 }

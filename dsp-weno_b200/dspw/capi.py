@@ -15,7 +15,7 @@ import numpy as np
 PKG_DIR = Path(__file__).resolve().parent.parent          # dsp-weno_b200/
 LIB_PATH = PKG_DIR / "libdspw.so"
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 MODEL = {"linadv": 0, "burgers": 1, "euler": 2, "ns_es": 3, "ns_kep": 4}
 FLUX = {
@@ -51,7 +51,8 @@ class Desc(C.Structure):
         ("time_scheme", C.c_int), ("precision", C.c_int),
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
         ("bc", C.c_int * 6), ("ec1_fix", C.c_int), ("mu_model", C.c_int),
-        ("max_iter", C.c_int), ("t_stamps", C.c_int), ("reserved_i", C.c_int * 8),
+        ("max_iter", C.c_int), ("t_stamps", C.c_int), ("nn_use_box", C.c_int), ("generic_kernels", C.c_int),
+        ("reserved_i", C.c_int * 6),
         ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
         ("zmin", C.c_double), ("zmax", C.c_double),
         ("gamma", C.c_double), ("gas_const", C.c_double), ("prandtl", C.c_double),
@@ -60,7 +61,9 @@ class Desc(C.Structure):
         ("bc_state", (C.c_double * 5) * 6),
         ("nn_w", ((C.c_double * 5) * 5) * 4),
         ("nn_b", (C.c_double * 5) * 4),
-        ("reserved_d", C.c_double * 8),
+        ("nn_feat_lo", C.c_double * 5), ("nn_feat_hi", C.c_double * 5),
+        ("cell_size", C.c_double * 3),
+        ("reserved_d", C.c_double * 5),
     ]
 
 
@@ -195,6 +198,17 @@ def make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=64, ny
     return d
 
 
+def set_training_box(d: Desc, lo, hi) -> Desc:
+    """Give the descriptor's network a training box (nn_use_box): stencils
+    whose five network inputs fall outside [lo, hi] are reconstructed by plain
+    SP-WENO in the FP32 form.  lo / hi usually come from Trainer.box()."""
+    d.nn_use_box = 1
+    for k in range(5):
+        d.nn_feat_lo[k] = float(lo[k])
+        d.nn_feat_hi[k] = float(hi[k])
+    return d
+
+
 def nvar(d: Desc) -> int:
     return 1 if d.model in (0, 1) else 5
 
@@ -256,6 +270,7 @@ def lib():
         "dspw_trainer_loss_grad": (I, [P, dp, dp, I, C.POINTER(D), dp, dp]),
         "dspw_trainer_get_params": (I, [P, dp, dp]),
         "dspw_trainer_info": (I, [P, C.POINTER(LL), dp]),
+        "dspw_trainer_box": (I, [P, dp, dp]),
         "dspw_trainer_eval": (I, [P, C.POINTER(D)]),
         "dspw_trainer_export": (I, [P, C.c_void_p, LL, C.POINTER(LL)]),
     }
@@ -355,6 +370,13 @@ class Trainer:
         fm = np.zeros(5)
         check(lib().dspw_trainer_info(self.h, C.byref(n), fm), "dspw_trainer_info")
         return n.value, fm
+
+    def box(self):
+        """(lo, hi): the range of each network input over the training data
+        (dspw_trainer_box), for set_training_box."""
+        lo, hi = np.zeros(5), np.zeros(5)
+        check(lib().dspw_trainer_box(self.h, lo, hi), "dspw_trainer_box")
+        return lo, hi
 
 
 class DspwError(RuntimeError):

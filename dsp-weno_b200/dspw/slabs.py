@@ -72,10 +72,10 @@ def split(desc: Desc, nslab: int) -> list[tuple[Desc, int, int]]:
         setattr(d, "n" + _AXIS[D], hi - lo)
         setattr(d, _AXIS[D] + "min", lo_b + lo * h)
         setattr(d, _AXIS[D] + "max", lo_b + hi * h)
-        # the slab keeps the domain's cell sizes exactly (descriptor reserved_d[5..7])
+        # the slab keeps the domain's cell sizes exactly (descriptor cell_size)
         for k in range(3):
-            if d.reserved_d[5 + k] <= 0.0:
-                d.reserved_d[5 + k] = cell[k]
+            if d.cell_size[k] <= 0.0:
+                d.cell_size[k] = cell[k]
         if nslab > 1 or periodic:
             if s > 0 or periodic:
                 d.bc[2 * D] = BC["halo"]

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define DSPW_ABI_VERSION 1
+#define DSPW_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define DSPW_API __attribute__((visibility("default")))
@@ -124,9 +124,12 @@ typedef struct dspw_desc {
   int mu_model;              /* enum dspw_mu */
   int max_iter;
   int t_stamps;              /* output time_stamps; dt is clipped to them like FV::run */
-  int reserved_i[8];          /* [0]: the network carries a training box of its inputs (bounds in
-                                reserved_d[2..4]); [1]: 1 = run this problem on the generic sweep
-                                kernels even when specialised ones exist (validation) */
+  int nn_use_box;            /* 1: the network has a training box (nn_feat_lo / nn_feat_hi); a
+                                stencil whose network inputs fall outside it is reconstructed by
+                                plain SP-WENO (FP32 form) */
+  int generic_kernels;       /* 1: run this problem on the generic sweep kernels even when
+                                specialised ones exist (validation) */
+  int reserved_i[6];         /* zero */
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double gamma, gas_const, prandtl, mu_ref, T_ref, T_0, omega;
   double lin_vel[3];         /* linadv velocity */
@@ -134,9 +137,15 @@ typedef struct dspw_desc {
   double bc_state[6][5];     /* DIRICHLET ghost state, primitive (rho,u,v,w,p) or (u) */
   double nn_w[4][5][5];      /* DSP-WENO layer weights, row = output, col = input */
   double nn_b[4][5];         /* DSP-WENO layer biases */
-  double reserved_d[8];      /* [2..4]: training box (reserved_i[0]); [5..7]: when > 0 the cell
-                                sizes dx, dy, dz instead of (max - min) / n, for the slabs of a
-                                decomposed domain (DSPW_BC_HALO), which keep the domain's */
+  double nn_feat_lo[5];      /* training box of the five network inputs (tanh theta-, tanh theta+,
+                                |del1|, |del2|, |del3| of the scaled stencil,
+                                enflo/src/neural_network.cc:16-38); used when nn_use_box == 1,
+                                e.g. filled from dspw_trainer_box after training */
+  double nn_feat_hi[5];
+  double cell_size[3];       /* when > 0: the cell sizes dx, dy, dz instead of (max - min) / n, for
+                                the slabs of a decomposed domain (DSPW_BC_HALO), which keep the
+                                domain's own */
+  double reserved_d[5];      /* zero */
 } dspw_desc;
 
 typedef struct dspw_handle dspw_handle;
@@ -415,8 +424,16 @@ DSPW_API int dspw_trainer_get_params(dspw_trainer* t, double* w /* 4*25 */, doub
 /* Mean loss over the trainer's data set with the current parameters, no update. */
 DSPW_API int dspw_trainer_eval(dspw_trainer* t, double* mean_loss);
 /* Number of samples and the largest |feature| of each of the 5 network inputs
- * over the valid samples: the training box used for the SP-WENO fallback. */
+ * over the valid samples. */
 DSPW_API int dspw_trainer_info(dspw_trainer* t, long long* nsamples, double* feature_max /* 5 */);
+/* The training box of the network: the smallest and largest value of each of
+ * the 5 network inputs over the trainer's valid samples, ready for a
+ * descriptor's nn_feat_lo / nn_feat_hi (with nn_use_box = 1), so that the
+ * solver reconstructs stencils outside the data the network was fitted on by
+ * plain SP-WENO.  No counterpart in the reference, whose network is applied
+ * to every stencil (enflo/src/reconstruct.cc:138-157).  DSPW_ERR_ARG when the
+ * trainer holds no valid sample. */
+DSPW_API int dspw_trainer_box(dspw_trainer* t, double lo[5], double hi[5]);
 /* The trainer's valid samples as rows of the reference trainer's data file
  * (23 doubles each, the column order its reader slices with tanh_theta,
  * DSP-WENO_trainer/DSP-WENO_network_trainer.py:305-333: cell values u0..u3,

@@ -55,3 +55,17 @@ def rel_err(a, b):
     a = np.asarray(a); b = np.asarray(b)
     scale = np.maximum(np.abs(b), 1e-300)
     return float(np.max(np.abs(a - b) / np.maximum(scale, np.max(np.abs(b)) * 1e-3 + 1e-300)))
+
+
+def oracle_kh_cons(n, recon, steps, dt, seed=12345):
+    """Conserved state of the CPU oracle after `steps` steps of size dt of the
+    Kelvin-Helmholtz workload (FP64 plain form of recon) on an n x n grid.
+    Runs in a worker process (spawned), so the larger grids proceed in
+    parallel while the GPU side runs."""
+    import oracle as O
+    from dspw import workloads as W
+    (d,), (p,), _ = W.kh(n, "fp64", recon, net(), seed=seed)
+    o = O.Oracle(d)
+    o.set_prim(p)
+    o.step(steps, fixed_dt=dt)
+    return o.cons()

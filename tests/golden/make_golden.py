@@ -18,10 +18,13 @@ code, never by the project's oracle or kernels:
   ooc.npz           config-1 L1/L2/Linf errors (LinAdvTest2, Nx=100..400)
   dsp_weno.txt      the shipped network weights (enflo/networks/dsp_weno.txt)
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root (after `make -C oracle ref REF=DIR`):
+
+    python tests/golden/make_golden.py --ref DIR
 """
 from __future__ import annotations
 
+import os
 import shutil
 import sys
 from pathlib import Path
@@ -33,9 +36,19 @@ sys.path.insert(0, str(REPO / "oracle"))
 sys.path.insert(0, str(REPO / "dsp-weno_b200"))
 import oracle as O  # noqa: E402
 
-REF_TREE = Path("/root/reference")
+def _ref_tree() -> Path:
+    """The reference project tree: argument --ref DIR, else the environment
+    variable DSPW_REFERENCE_DIR (the same tree oracle/Makefile compiles)."""
+    if "--ref" in sys.argv:
+        return Path(sys.argv[sys.argv.index("--ref") + 1])
+    env = os.environ.get("DSPW_REFERENCE_DIR")
+    if not env:
+        raise SystemExit("make_golden.py: give the reference tree with --ref DIR or DSPW_REFERENCE_DIR")
+    return Path(env)
+
+
+REF_TREE = _ref_tree() if __name__ == "__main__" else None
 OUT = Path(__file__).resolve().parent
-NET_SRC = REF_TREE / "enflo" / "networks" / "dsp_weno.txt"
 NET = str(OUT / "dsp_weno.txt")
 
 EULER_FLUXES = ["kepes_tecno4_roe", "kepes_tecno_roe", "kepes_tecno4_rusanov", "kepes_tecno_rusanov",
@@ -457,7 +470,7 @@ def gen_ooc():
 def main():
     if not O.ref_available():
         raise SystemExit("build the reference checker first: make -C oracle ref")
-    shutil.copyfile(NET_SRC, OUT / "dsp_weno.txt")
+    shutil.copyfile(REF_TREE / "enflo" / "networks" / "dsp_weno.txt", OUT / "dsp_weno.txt")
     rng = np.random.default_rng(20240611)
     gen_faces_euler(rng)
     gen_faces_scalar(rng)

@@ -2,6 +2,8 @@
 include/dspw.h declares; the ctypes descriptor matches the C layout."""
 import ctypes
 import re
+import shutil
+import subprocess
 from pathlib import Path
 
 import numpy as np
@@ -38,11 +40,34 @@ def test_error_strings():
         assert s.startswith(capi.STATUS[code])
 
 
-def test_descriptor_layout():
-    # offsets of the C struct (x86-64 SysV): 23 ints + 8 reserved ints, then doubles
-    d = capi.Desc
-    assert d.xmin.offset == 4 * (15 + 8 + 8) + 4 * 0 or d.xmin.offset % 8 == 0
-    assert ctypes.sizeof(capi.Desc) == d.reserved_d.offset + 8 * 8
+def _c_offsets(struct, fields, tmp_path):
+    """offsetof() of each field and sizeof() of a struct of include/dspw.h, as
+    the host C compiler lays it out."""
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dspw.h"', "int main(void) {"]
+    for f in fields:
+        lines.append(f'  printf("%zu\\n", offsetof({struct}, {f}));')
+    lines.append(f'  printf("%zu\\n", sizeof({struct}));')
+    lines.append("  return 0; }")
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(REPO / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    return [int(v) for v in out]
+
+
+@pytest.mark.parametrize("struct,cls", [("dspw_desc", "Desc"), ("dspw_globals_out", "Globals"),
+                                        ("dspw_status_out", "StatusOut"), ("dspw_halo_out", "HaloOut"),
+                                        ("dspw_train_cfg", "TrainCfg")])
+def test_struct_layouts_match_the_header(struct, cls, tmp_path):
+    """Every field of the ctypes mirror sits at the C compiler's offset."""
+    if shutil.which("gcc") is None:
+        pytest.skip("no host C compiler")
+    c = getattr(capi, cls)
+    names = [f[0] for f in c._fields_]
+    offs = _c_offsets(struct, names, tmp_path)
+    assert offs[:-1] == [getattr(c, n).offset for n in names]
+    assert offs[-1] == ctypes.sizeof(c)
 
 
 def test_bad_descriptor_rejected_without_gpu():
@@ -57,6 +82,23 @@ def test_bad_descriptor_rejected_without_gpu():
     assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
     d = capi.make_desc()
     d.abi_version = 99
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d = capi.make_desc()
+    d.abi_version = 1   # the layout before the named box / kernel / cell-size fields
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    # unused slots must stay zero; named fields are range-checked
+    for field, idx, val in (("reserved_i", 0, 1), ("reserved_d", 4, 1.0), ("cell_size", 1, -1.0),
+                            ("cell_size", 2, float("inf"))):
+        d = capi.make_desc()
+        getattr(d, field)[idx] = val
+        assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1, field
+    d = capi.make_desc()
+    d.generic_kernels = 2
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d = capi.set_training_box(capi.make_desc(), [0, 0, 0, 0, 0], [1, 1, 1, 1, 1])
+    d.nn_feat_lo[3] = 2.0   # lo above hi
+    assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d.nn_feat_lo[3] = float("nan")
     assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
     # eno 3 on a wall axis of two cells: the third ghost's mirror leaves the line
     d = capi.make_desc(recon="eno3", nx=16, ny=2, bc=["periodic", "periodic", "wall", "wall", "periodic", "periodic"])

@@ -249,7 +249,7 @@ def test_batch_mixed_ghost_widths_equals_single():
 @pytest.mark.parametrize("dims", [(40, 1, 1), (24, 40, 1), (16, 12, 10), (12, 12, 10)])
 def test_specialised_kernels_equal_generic(precision, recon, dims):
     """A kepes_tecno4 problem runs the compile-time specialised sweep kernels;
-    with descriptor reserved_i[1] = 1 it runs the generic ones (here batched
+    with descriptor generic_kernels = 1 it runs the generic ones (here batched
     with a Burgers problem, a second kernel class).  FP64 gives the same bits;
     FP32 (built with FMA contraction, whose choices may differ between the two
     instantiations, and with BF16 network layers whose roundings then flip now
@@ -265,7 +265,7 @@ def test_specialised_kernels_equal_generic(precision, recon, dims):
     a.step(5)
     dg = make_desc(model="euler", flux="kepes_tecno4_roe", recon=recon, nx=nx, ny=ny, nz=nz, bc="periodic",
                    network=net(), precision=precision, ec1_fix=True)
-    dg.reserved_i[1] = 1
+    dg.generic_kernels = 1
     b = Solver([dg, dummy])
     b.upload_prim(st, 0)
     b.upload_prim(np.sin(np.linspace(0, 6, 33)).reshape(1, 1, 1, 33), 1)
@@ -343,7 +343,7 @@ def test_upload_rejects_bad_states():
 @pytest.mark.parametrize("recon", ["sp_weno", "sp_wenoc", "sp_weno_dl"])
 def test_scalar_kernel_equals_generic(precision, model, flux, recon):
     """1-D scalar problems run k_sweep_scalar (reconstruction family fixed at
-    compile time); with reserved_i[1] = 1 they run the generic kernel.  Two
+    compile time); with generic_kernels = 1 they run the generic kernel.  Two
     problems of different sizes and boundary conditions in one batch: FP64
     gives the same bits, FP32 agrees to rounding."""
     rng = np.random.default_rng(5)
@@ -354,7 +354,7 @@ def test_scalar_kernel_equals_generic(precision, model, flux, recon):
     for generic in (False, True):
         ds = [make_desc(nx=nx, ny=1, nz=1, bc=bc, **kw) for nx, bc in shapes]
         for d in ds:
-            d.reserved_i[1] = int(generic)
+            d.generic_kernels = int(generic)
         s = Solver(ds)
         for p, st in enumerate(states):
             s.upload_prim(st, p)

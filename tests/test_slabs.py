@@ -29,12 +29,12 @@ def test_layer_ranges_cover_the_domain():
 @pytest.mark.parametrize("bounds", [(0.0, 1.0), (0.0, 2 * np.pi), (-5.0, 5.0), (-0.37, 1.91)])
 @pytest.mark.parametrize("n,k", [(2048, 3), (100, 7), (37, 4), (12, 2)])
 def test_slabs_keep_the_cell_size(bounds, n, k):
-    """Each slab carries the domain's cell sizes (reserved_d[5..7]), since
+    """Each slab carries the domain's cell sizes (descriptor cell_size), since
     its own bounds over its own cell count need not round to them."""
     d = make_desc(nx=16, ny=n, nz=1, y=bounds, x=(0.0, 0.3))
     h = [(d.xmax - d.xmin) / d.nx, (d.ymax - d.ymin) / d.ny, (d.zmax - d.zmin) / d.nz]
     for s, lo, hi in split(d, k):
-        assert list(s.reserved_d[5:8]) == h             # bit for bit
+        assert list(s.cell_size) == h             # bit for bit
         assert s.ny == hi - lo and abs(s.ymin - (d.ymin + lo * h[1])) <= 1e-12 * max(1.0, abs(d.ymin))
         assert (s.nx, s.nz) == (d.nx, d.nz) and (s.xmin, s.xmax) == (d.xmin, d.xmax)
 

@@ -5,38 +5,78 @@ dspw_globals on the same state, twice in a row, because every call reuses the
 library's one fixed scratch array.  This file is collected last on purpose.
 """
 import ctypes
+import math
 
 import numpy as np
 import pytest
 
 from dspw import Solver, capi, make_desc
+from dspw.slabs import split
 
 pytestmark = pytest.mark.gpu
 
 
-def _state(nx, ny):
+def _state(nx, ny, nz=1, scalar=False):
     x = (np.arange(nx) + 0.5) / nx
     y = (np.arange(ny) + 0.5) / ny
-    X, Y = np.meshgrid(x, y)
-    p = np.zeros((5, 1, ny, nx))
-    p[0, 0] = 1.0 + 0.3 * np.sin(2 * np.pi * (X + Y))
-    p[1, 0] = 0.4 * np.cos(2 * np.pi * X)
-    p[2, 0] = -0.2 * np.sin(2 * np.pi * Y)
-    p[4, 0] = 1.0 + 0.1 * np.cos(2 * np.pi * (X - Y))
+    z = (np.arange(nz) + 0.5) / nz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    if scalar:
+        return (0.5 + 0.4 * np.sin(2 * np.pi * X)).reshape(1, nz, ny, nx)
+    p = np.zeros((5, nz, ny, nx))
+    p[0] = 1.0 + 0.3 * np.sin(2 * np.pi * (X + Y + Z))
+    p[1] = 0.4 * np.cos(2 * np.pi * X)
+    if ny > 1:
+        p[2] = -0.2 * np.sin(2 * np.pi * Y)
+    if nz > 1:
+        p[3] = 0.1 * np.cos(2 * np.pi * Z)
+    p[4] = 1.0 + 0.1 * np.cos(2 * np.pi * (X - Y))
     return p
 
 
+def _slab_desc(precision):
+    """The middle slab of a 3-slab cut of a 2-D domain whose bounds over its
+    cell count do not round to the domain's cell size (descriptor cell_size)."""
+    dom = make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=40, ny=37, nz=1,
+                    x=(-0.37, 1.91), y=(-0.37, 1.91), precision=precision)
+    d, lo, hi = split(dom, 3)[1]
+    return d
+
+
+# (name, descriptor builder): two calls in a row per case, different sizes and
+# component layouts (nv = 1, 3, 4, 5)
+CASES = {
+    "euler2d": lambda pr: [make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=96, ny=80, nz=1,
+                                     precision=pr),
+                           make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=300, ny=7, nz=1,
+                                     precision=pr)],
+    "burgers1d": lambda pr: [make_desc(model="burgers", flux="bur_tecno4", recon="sp_weno", nx=500,
+                                       x=(-math.pi, math.pi), precision=pr),
+                             make_desc(model="burgers", flux="bur_tecno4", recon="sp_weno", nx=77,
+                                       x=(-math.pi, math.pi), precision=pr)],
+    "euler1d": lambda pr: [make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=400, x=(-5, 5),
+                                     precision=pr),
+                           make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=123, x=(-5, 5),
+                                     precision=pr)],
+    "euler3d": lambda pr: [make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=20, ny=18, nz=16,
+                                     precision=pr),
+                           make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=9, ny=12, nz=10,
+                                     precision=pr)],
+    "slab2d": lambda pr: [_slab_desc(pr), _slab_desc(pr)],
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
 @pytest.mark.parametrize("precision", ["fp64", "fp32_bf16"])
-def test_globals_noalloc_matches_globals_twice(precision):
+def test_globals_noalloc_matches_globals_twice(case, precision):
     import torch
 
     lib = capi.lib()
-    for call, (nx, ny) in enumerate(((96, 80), (300, 7))):   # two calls in a row, different sizes
-        d = make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=nx, ny=ny, nz=1,
-                      precision=precision)
+    for call, d in enumerate(CASES[case](precision)):
         s = Solver(d)
-        s.upload_prim(_state(nx, ny))
-        s.step(2)
+        s.upload_prim(_state(d.nx, d.ny, d.nz, scalar=d.model <= 1))
+        if case != "slab2d":   # a slab's halo layers are the caller's: no steps
+            s.step(2)
         ref = s.globals()
         ptr, stride, eb = ctypes.c_void_p(), ctypes.c_longlong(), ctypes.c_int()
         capi.check(lib.dspw_device_state(s.h, 0, ctypes.byref(ptr), ctypes.byref(stride), ctypes.byref(eb)),
@@ -52,16 +92,21 @@ def test_globals_noalloc_matches_globals_twice(precision):
         # dspw_globals evaluates the pressure of an FP32 state in FP32 before the
         # log; this entry point evaluates it in FP64 from the same FP32 values
         rtol = 1e-12 if precision == "fp64" else 1e-5
-        assert np.all(np.abs(got - want) <= rtol * scale), (call, got, want)
+        assert np.all(np.abs(got - want) <= rtol * scale), (case, call, got, want)
 
 
-def test_globals_noalloc_rejects_oversize_state():
+def test_globals_noalloc_rejects_bad_arguments():
     import torch
 
     lib = capi.lib()
-    d = make_desc(model="euler", nx=4096, ny=4097, nz=1)   # above 16,777,216 cells
     out = torch.zeros(7, dtype=torch.float64, device="cuda")
     buf = torch.zeros(16, dtype=torch.float64, device="cuda")
+    d = make_desc(model="euler", nx=4096, ny=4097, nz=1)   # above 16,777,216 cells
     rc = lib.dspw_globals_noalloc(ctypes.byref(d), ctypes.c_void_p(buf.data_ptr()), 4096 * 4097, 8,
                                   ctypes.c_void_p(out.data_ptr()), None)
     assert rc == 1   # DSPW_ERR_ARG
+    d = make_desc(model="euler", nx=4, ny=4, nz=1)
+    d.model = 7      # no such model
+    rc = lib.dspw_globals_noalloc(ctypes.byref(d), ctypes.c_void_p(buf.data_ptr()), 16, 8,
+                                  ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == 1
