@@ -45,13 +45,44 @@ sys.path.insert(0, str(REPO / "oracle"))
 
 METRIC = "cell-updates/s"
 NET_FILE = REPO / "tests" / "golden" / "dsp_weno.txt"
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant
-# launch per cell, from one ncu capture of that launch
-# (profiles/sweep_kernels_kh2048.md): KH 2048^2 FP32 DSP-WENO, last-stage y sweep,
-# 202.84 MB + 46.66 MB for 4194304 cells
-NCU_TRAFFIC_BYTES_PER_CELL = {
-    ("kh2048_fp32_bf16_sp_weno_dl_kepes_tecno4_roe", "sweep_y"): (202.842624e6 + 46.659328e6) / 4194304,
-}
+# Measurements that need another tool or a long run are recorded, one line
+# each, in profiles/bench_records.txt together with the hash of the device
+# sources they were taken with; the JSON line attaches a record only when that
+# hash equals the current sources' (else the field says that no record of this
+# build exists).
+RECORDS = REPO / "profiles" / "bench_records.txt"
+SOURCES = sorted((REPO / "dsp-weno_b200" / "csrc").glob("*")) + [REPO / "include" / "dspw.h"]
+
+
+def source_hash() -> str:
+    """sha256 (16 hex digits) of the device sources and the C ABI header."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in SOURCES:
+        h.update(f.name.encode())
+        h.update(f.read_bytes())
+    return h.hexdigest()[:16]
+
+
+def read_records(kind: str) -> list[dict]:
+    """Records of one kind: lines `<kind> key=value ...` (values without
+    spaces, or double-quoted)."""
+    import shlex
+    out = []
+    if not RECORDS.exists():
+        return out
+    for line in RECORDS.read_text().splitlines():
+        if not line.startswith(kind + " "):
+            continue
+        rec = {}
+        for tok in shlex.split(line)[1:]:
+            k, _, v = tok.partition("=")
+            try:
+                rec[k] = float(v)
+            except ValueError:
+                rec[k] = v
+        out.append(rec)
+    return out
 
 
 # ------------------------------------------------------------------ CPU legs
@@ -93,6 +124,23 @@ class RefPool:
     def close(self):
         self.pool.close()
         self.pool.join()
+
+
+def reference_sample(args, procs, warmup):
+    """The reference's CPU solver (oracle/_ref) on all host cores: one process
+    per core, each a cpu_sample_n^2 KH grid, `warmup` untimed then args.steps
+    timed steps.  Returns (cell-updates/s, seconds, description)."""
+    pool = RefPool(args.cpu_sample_n, args.recon, procs)
+    for _ in range(warmup):
+        pool.step(1)
+    t = 0.0
+    for _ in range(args.steps):
+        t += pool.step(1)
+    pool.close()
+    v = procs * args.cpu_sample_n ** 2 * args.steps / t
+    sample = (f"{procs} processes x reference enflo solver on a {args.cpu_sample_n}^2 (x2 in z, the reference's "
+              f"2-D layout) KH grid, {args.recon}, FP64, {args.steps} steps each, physical cells counted")
+    return v, t, sample
 
 
 def cpu_cores():
@@ -153,35 +201,42 @@ class ClockSampler:
 
 
 def algorithmic_bytes(name, stage, probs, w):
-    """Minimum HBM bytes of one launch of kernel ``name`` in SSPRK3 stage
-    ``stage`` over problems ``probs`` = [(cells, nv, dim, ns, kernel class)], nv
-    the stored components, w the word size.  A sweep launch of a mixed batch is
-    named ``sweep_<d>.c<class>`` and covers the problems of that class only.  Euler / scalar: the x sweep reads U^k and
-    writes R, middle sweeps read U^k and R and write R, the last sweep reads U^k,
-    R (absent in 1-D) and, in stages 2-3, U^n and writes U^(k+1).  Navier-Stokes:
-    entropy variables read U and write V; node fluxes read V and write 3 nv per
-    node; the sweeps only accumulate R; the viscous update reads the node fluxes,
-    R, U^k (and U^n) and writes U^(k+1)."""
+    """(algorithmic, moved) HBM bytes of one launch of kernel ``name`` in stage
+    ``stage`` over problems ``probs`` = [(cells, nv, dim, ns, kernel class)],
+    nv the stored components, w the word size.  A sweep launch of a mixed batch
+    is named ``sweep_<d>.c<class>`` and covers the problems of that class only.
+
+    Algorithmic bytes follow the fully fused stage: it reads U^k (and U^n from
+    the second SSPRK3 stage on) and writes U^(k+1) once, 2 or 3 nv w per cell,
+    8 nv w per cell-update over the three stages.  They are counted on the
+    stage's last sweep (or the viscous update, for Navier-Stokes), which is
+    where the fused form's reads and write happen.  `moved` adds what this
+    implementation moves beyond that: the x (and for 3-D, y) sweeps read U^k
+    and write the residual R, the last sweep reads R, and the Navier-Stokes
+    kernels go through the entropy-variable and node-flux buffers."""
     base, _, cls = name.partition(".c")
     name = base
-    tot = 0
+    alg = moved = 0
     for cells, nv, dim, ns, kcls in probs:
         if cls and int(cls) != kcls:
             continue
-        upd = 4 if stage > 0 else 3
-        b = 0
+        fused = 3 if stage > 0 else 2   # read U^k (+ U^n), write U^(k+1)
+        a = m = 0
         if ns:
-            b = {"entvars": 2, "visc_nodes": 4, "sweep_x": 2, "sweep_y": 3, "sweep_z": 3,
-                 "visc_update": 3 + upd}.get(name, 0)
+            m = {"entvars": 2, "visc_nodes": 4, "sweep_x": 2, "sweep_y": 3, "sweep_z": 3,
+                 "visc_update": 3 + fused}.get(name, 0)
+            a = fused if name == "visc_update" else 0
         elif name.startswith("sweep_"):
             axis = "xyz".index(name[-1])
             if axis < dim:
                 if axis == dim - 1:
-                    b = upd if dim > 1 else upd - 1
+                    a = fused
+                    m = fused + (1 if dim > 1 else 0)   # + the residual of the earlier sweeps
                 else:
-                    b = 2 if axis == 0 else 3
-        tot += cells * nv * w * b
-    return tot
+                    m = 2 if axis == 0 else 3
+        alg += cells * nv * w * a
+        moved += cells * nv * w * m
+    return alg, moved
 
 
 def build_workload(args, precision, recon, rank, world):
@@ -331,10 +386,15 @@ def measure_gpu(args, torch, dist, rank, world):
         prev = base
         rows.append((name, stage, kms))
     dom = max(rows, key=lambda r: r[2])
-    dom_bytes = algorithmic_bytes(dom[0], dom[1], probs, w)
+    dom_bytes, dom_moved = algorithmic_bytes(dom[0], dom[1], probs, w)
     peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text()) if (REPO / "MEASURED_PEAKS.json").exists() else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peak = peaks.get("hbm_gbs")
+    peak_src = "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    if not peak:
+        peak, peak_src = 6650.0, "fallback 6650 GB/s, an earlier measurement on this pool (of fallback)"
     achieved = dom_bytes / (dom[2] * 1e-3) / 1e9
+    # the whole step: 8 nv w per cell-update of the fused form
+    step_bytes = sum(c * nv * w * 8 for c, nv, dim, ns, kc in probs)
     # e2e through the C ABI with host buffers: upload every problem (pinned
     # H2D), one step, download every problem (D2H) per step
     pinned, outs = [], []
@@ -363,19 +423,27 @@ def measure_gpu(args, torch, dist, rank, world):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     del s
-    # FP64 plain form (SP-WENO, no network) on the same workload for the ratio
-    fp64_ms = None
+    # FP64 plain form (SP-WENO, no network) on the same workload for the
+    # ratio, and the FP64 form of the network (the reference's arithmetic)
+    fp64_ms = fp64_dl_ms = None
     if args.precision == "fp32_bf16" and not args.no_fp64:
+        k64 = max(1, args.steps // 4)
         d64, p64, _, _, _ = build_workload(args, "fp64", "sp_weno", rank, world)
         s64 = solver(d64, p64)
-        k64 = max(1, args.steps // 4)
         fp64_ms = timed(s64, k64, max(1, args.warmup // 2)) / k64
         del s64
+        if args.recon == "sp_weno_dl":
+            d64, p64, _, _, _ = build_workload(args, "fp64", "sp_weno_dl", rank, world)
+            s64 = solver(d64, p64)
+            fp64_dl_ms = timed(s64, k64, max(1, args.warmup // 2)) / k64
+            del s64
     nbytes = sum(a.nbytes for a in prims)
     tune_ms = tuned.get("ms")
-    return dict(tune_ms=tune_ms, ms=ms, clk=clk, status=st, prof=rows, dom=dom, dom_bytes=dom_bytes, achieved=achieved,
-                peak=peak, e2e_s=e2e_s, e2e_steps=e2e_steps, ncell=ncell, ncell_all=ncell_all, scaling=scaling,
-                launches=len(prof), fp64_ms=fp64_ms, h2d=nbytes, d2h=nbytes, nprob=len(descs))
+    return dict(tune_ms=tune_ms, ms=ms, clk=clk, status=st, prof=rows, dom=dom, dom_bytes=dom_bytes,
+                dom_moved=dom_moved, achieved=achieved, peak=peak, peak_src=peak_src, step_bytes=step_bytes,
+                e2e_s=e2e_s, e2e_steps=e2e_steps, ncell=ncell, ncell_all=ncell_all, scaling=scaling,
+                launches=len(prof), fp64_ms=fp64_ms, fp64_dl_ms=fp64_dl_ms, h2d=nbytes, d2h=nbytes,
+                nprob=len(descs))
 
 
 def matched_error(torch):
@@ -447,6 +515,78 @@ def matched_error(torch):
             "columns": ["n", "l1_err", "device_ms_per_run", "steps"], "summary": summary}
 
 
+def kh_accuracy(torch, grids=(1024, 2048), n_ref=4096, t_end=1.0):
+    """Accuracy of the forms on the headline problem: Kelvin-Helmholtz to
+    t = 1 on 1024^2 and 2048^2 in FP32 + BF16 DSP-WENO, FP64 DSP-WENO and the
+    FP64 plain form (SP-WENO), against the FP64 plain form on 4096^2
+    (box-averaged to each grid).  All grids start from one noise field
+    (workloads.kh_prim_nested).  L1 is the reference's volume-weighted error
+    (compute_errors.cc:9-33), i.e. the mean over the unit square; L-inf the
+    largest cell error; both of the density.  Device time of every run (CUDA
+    events around dspw_run) and its sign-property violations are reported."""
+    from dspw import Solver, load_network_file, make_desc
+    from dspw.workloads import kh_prim_nested
+
+    net = load_network_file(NET_FILE)
+
+    def run(n, prec, recon):
+        d = make_desc(model="euler", flux="kepes_tecno4_roe", recon=recon, nx=n, ny=n, nz=1, x=(0, 1), y=(0, 1),
+                      bc="periodic", cfl=0.4, final_time=t_end, network=net, precision=prec)
+        s = Solver(d)
+        s.upload_prim(kh_prim_nested(n, n_ref))
+        st = torch.cuda.ExternalStream(s.stream_ptr())
+        s.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        steps = s.run(chunk=512)
+        e1.record(st)
+        e1.synchronize()
+        rho = s.prim()[0, 0]
+        stat = s.status()
+        g = s.globals()
+        out = {"n": n, "precision": prec, "recon": recon, "steps": steps, "t": g.time,
+               "device_ms": e0.elapsed_time(e1), "sign_violations": stat.sign_violations,
+               "faces_checked": stat.faces_checked, "code": stat.code}
+        del s
+        return rho, out
+
+    rho_ref, ref_info = run(n_ref, "fp64", "sp_weno")
+    runs, pairs, summary = [ref_info], [], []
+    for n in grids:
+        r = n_ref // n
+        ref = rho_ref.reshape(n, r, n, r).mean(axis=(1, 3))
+        got = {}
+        for prec, recon in (("fp64", "sp_weno"), ("fp64", "sp_weno_dl"), ("fp32_bf16", "sp_weno_dl")):
+            rho, info = run(n, prec, recon)
+            e = np.abs(rho - ref)
+            info.update({"l1_vs_ref": float(e.mean()), "linf_vs_ref": float(e.max())})
+            runs.append(info)
+            got[(prec, recon)] = rho
+        for a, b in ((("fp32_bf16", "sp_weno_dl"), ("fp64", "sp_weno_dl")),
+                     (("fp64", "sp_weno_dl"), ("fp64", "sp_weno")),
+                     (("fp32_bf16", "sp_weno_dl"), ("fp64", "sp_weno"))):
+            e = np.abs(got[a] - got[b])
+            pairs.append({"n": n, "a": "/".join(a), "b": "/".join(b), "l1": float(e.mean()), "linf": float(e.max())})
+        by = {(x["precision"], x["recon"]): x for x in runs if x["n"] == n}
+        l1_32 = by[("fp32_bf16", "sp_weno_dl")]["l1_vs_ref"]
+        l1_64 = by[("fp64", "sp_weno")]["l1_vs_ref"]
+        summary.append({"n": n, "l1_fp32_dl": l1_32, "l1_fp64_plain": l1_64, "l1_ratio": l1_32 / l1_64,
+                        "linf_fp32_dl": by[("fp32_bf16", "sp_weno_dl")]["linf_vs_ref"],
+                        "linf_fp64_plain": by[("fp64", "sp_weno")]["linf_vs_ref"],
+                        "sign_violations_fp32_dl": by[("fp32_bf16", "sp_weno_dl")]["sign_violations"],
+                        "time_ratio_fp64_plain_over_fp32_dl": by[("fp64", "sp_weno")]["device_ms"] /
+                        by[("fp32_bf16", "sp_weno_dl")]["device_ms"]})
+    return {"metric": "L1 / L-inf density error at t = 1 vs FP64 SP-WENO on 4096^2, KH", "unit": "density",
+            "n_gpus": 1, "data": "synthetic", "source_hash": source_hash(), "reference_grid": n_ref,
+            "runs": runs, "pairs": pairs, "summary": summary,
+            "records": [f"accuracy n={s['n']} t=1.0 l1_fp32_dl={s['l1_fp32_dl']:.6e} "
+                        f"l1_fp64_plain={s['l1_fp64_plain']:.6e} l1_ratio={s['l1_ratio']:.4f} "
+                        f"linf_fp32_dl={s['linf_fp32_dl']:.6e} linf_fp64_plain={s['linf_fp64_plain']:.6e} "
+                        f"sign_violations_fp32_dl={int(s['sign_violations_fp32_dl'])} "
+                        f"time_ratio={s['time_ratio_fp64_plain_over_fp32_dl']:.4f} ref_grid={n_ref} "
+                        f"src={source_hash()}" for s in summary]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -454,12 +594,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="kh",
-                    choices=["kh", "shu_osher", "batched", "tgv", "matched_error", "kh_slabs"],
+                    choices=["kh", "shu_osher", "batched", "tgv", "matched_error", "kh_slabs", "kh_accuracy"],
                     help="kh: 2-D Euler KH (the headline); shu_osher: 1-D Euler; batched: vortex OOC list plus "
                          "4096 Burgers problems in one batch (shared out over ranks); tgv: 3-D Navier-Stokes "
                          "Taylor-Green vortex; matched_error: time to equal L1 error of the two forms on "
                          "Shu-Osher and the isentropic vortex (its own JSON line); kh_slabs: one KH domain "
-                         "cut into one slab per rank, halo layers over NCCL inside the step graphs")
+                         "cut into one slab per rank, halo layers over NCCL inside the step graphs; "
+                         "kh_accuracy: L1 / L-inf density error of the forms on KH 1024^2 and 2048^2 at t = 1 "
+                         "against FP64 SP-WENO on 4096^2 (its own JSON line; long)")
     ap.add_argument("--n", type=int, default=None, help="grid size (kh 2048, shu_osher 25600, tgv 256)")
     ap.add_argument("--precision", default="fp32_bf16", choices=["fp32_bf16", "fp64"])
     ap.add_argument("--recon", default="sp_weno_dl")
@@ -476,12 +618,12 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.workload == "matched_error":
+    if args.workload in ("matched_error", "kh_accuracy"):
         if args.impl == "reference" or rank != 0:
             return
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps(matched_error(torch)))
+        print(json.dumps(matched_error(torch) if args.workload == "matched_error" else kh_accuracy(torch)))
         return
     if args.workload == "kh":
         n = args.n or 2048
@@ -517,21 +659,18 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm samples the KH workload only"}))
             return
         procs = cpu_cores()
-        pool = RefPool(args.cpu_sample_n, args.recon, procs)
-        for _ in range(args.warmup):
-            pool.step(1)
-        t = 0.0
-        for _ in range(args.steps):
-            t += pool.step(1)
-        pool.close()
-        cells = procs * args.cpu_sample_n ** 2
-        v = cells * args.steps / t
-        sample = (f"{procs} processes x reference enflo solver on a {args.cpu_sample_n}^2 (x2 in z, the reference's "
-                  f"2-D layout) KH grid, {args.steps} steps, physical cells counted")
+        v, t, sample = reference_sample(args, procs, args.warmup)
+        # the sample's own configuration: the GPU arm's workload, on the grid
+        # the CPU samples (physical cells counted, as the GPU arm counts them)
+        ref_config = dict(config)
+        ref_config.update({"workload": f"kh{args.cpu_sample_n}_fp64_{args.recon}_kepes_tecno4_roe_reference_cpu",
+                           "grid": [args.cpu_sample_n, args.cpu_sample_n], "precision": "fp64",
+                           "sample_of": config["workload"],
+                           "layout": "the reference's 2-D layout: Nz = 2 cells, periodic"})
         print(json.dumps({"metric": METRIC, "value": v, "unit": "cell-updates/s", "impl": "reference",
                           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                           "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
-                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": ref_config,
                           "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
                                            "sample": sample},
                           "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
@@ -546,15 +685,8 @@ def main():
     elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             procs = cpu_cores()
-            pool = RefPool(args.cpu_sample_n, args.recon, procs)
-            pool.step(1)
-            k = 3
-            t = sum(pool.step(1) for _ in range(k))
-            pool.close()
-            cpu = {"value": procs * args.cpu_sample_n ** 2 * k / t, "unit": "cell-updates/s", "cores": procs,
-                   "kind": "reference",
-                   "sample": f"{procs} processes x reference solver, {args.cpu_sample_n}^2 (x2) KH grid, "
-                             f"{args.recon}, {k} steps each"}
+            v, _, sample = reference_sample(args, procs, 1)
+            cpu = {"value": v, "unit": "cell-updates/s", "cores": procs, "kind": "reference", "sample": sample}
         except Exception as e:  # the checker may be unbuilt on a bare box
             cpu = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
@@ -592,10 +724,17 @@ def main():
     value = r["ncell_all"] * steps / (r["ms"] * 1e-3)
     e2e_v = r["ncell_all"] * r["e2e_steps"] / r["e2e_s"]
     dom = r["dom"]
-    traffic = None
-    per_cell = NCU_TRAFFIC_BYTES_PER_CELL.get((config.get("workload"), dom[0]))
-    if per_cell:
-        traffic = per_cell * r["ncell"]
+    src = source_hash()
+    # DRAM traffic and issue activity of the dominant launch from an ncu
+    # capture of this very build (records with the current source hash)
+    traffic = issue = None
+    traffic_note = "no ncu record of this build for this launch"
+    for rec in read_records("traffic"):
+        if rec.get("workload") == config.get("workload") and rec.get("kernel") == dom[0] and \
+                int(rec.get("stage", -9)) == dom[1] and rec.get("src") == src:
+            traffic = (rec["dram_read"] + rec["dram_write"]) / rec["cells"] * r["ncell"]
+            issue = rec.get("issue_active_pct")
+            traffic_note = f"ncu capture: {rec.get('capture', '')}"
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": r["ms"] / steps, "higher_is_better": True, "scaling": r["scaling"],
@@ -603,8 +742,15 @@ def main():
         "config": config,
         "roofline": {"bound": "hbm", "kernel": dom[0], "stage": dom[1], "achieved": r["achieved"],
                      "peak": r["peak"], "unit": "GB/s", "frac": r["achieved"] / r["peak"],
-                     "traffic": traffic, "algorithmic_bytes": r["dom_bytes"], "launch_ms": dom[2],
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                     "traffic": traffic, "traffic_source": traffic_note,
+                     "algorithmic_bytes": r["dom_bytes"],
+                     "extra_bytes": r["dom_moved"] - r["dom_bytes"],
+                     "launch_ms": dom[2], "peak_source": r["peak_src"],
+                     "issue_frac": issue / 100.0 if issue is not None else None,
+                     "step_achieved": r["step_bytes"] * steps / (r["ms"] * 1e-3) / 1e9,
+                     "step_frac": r["step_bytes"] * steps / (r["ms"] * 1e-3) / 1e9 / r["peak"],
+                     "bytes_rule": "fused stage: read U^k (+U^n), write U^(k+1); 8 nv w per cell-update"},
+        "source_hash": src,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_v, "unit": "cell-updates/s", "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "api": "dspw_upload_prim + dspw_step(1) + dspw_download_cons"},
@@ -620,6 +766,17 @@ def main():
     if r["fp64_ms"]:
         line["fp64_plain"] = {"value": r["ncell_all"] / (r["fp64_ms"] * 1e-3), "ms_per_step": r["fp64_ms"],
                               "recon": "sp_weno", "speedup_fp32_bf16_dl_over_fp64_plain": r["fp64_ms"] / (r["ms"] / steps)}
+    if r["fp64_dl_ms"]:
+        line["fp64_dl"] = {"value": r["ncell_all"] / (r["fp64_dl_ms"] * 1e-3), "ms_per_step": r["fp64_dl_ms"],
+                           "recon": "sp_weno_dl", "note": "the FP64 form of the network, the reference's arithmetic"}
+    if args.workload == "kh" and args.precision == "fp32_bf16":
+        # the accuracy half of the metric at this workload's grid, from the
+        # long runs of `bench.py --workload kh_accuracy`
+        acc = [a for a in read_records("accuracy") if int(a.get("n", 0)) == (args.n or 2048)]
+        if acc:
+            a = acc[-1]
+            line["accuracy"] = {k: a[k] for k in a}
+            line["accuracy"]["same_build"] = a.get("src") == src
     if args.workload == "kh" and world == 1 and args.precision == "fp32_bf16" and not args.no_matched_error:
         # the metric's other half: time to the same L1 density error, FP64 plain
         # over FP32 + BF16 DSP-WENO (bench.py --workload matched_error for the runs)

@@ -7,7 +7,8 @@ cells the batch advances per step.  The states follow the reference's example
 set-ups (enflo/examples, enflo_scalar/examples); seeded noise and random
 Fourier data stand in for inputs that a param.in expression cannot state.
 
-    kh        Kelvin-Helmholtz on the periodic unit square (2-D Euler)
+    kh        Kelvin-Helmholtz on the periodic unit square (2-D Euler); a
+              grid-nested variant for convergence studies (kh_prim_nested)
     shu_osher Shu-Osher shock / entropy-wave interaction on [-5, 5] (1-D Euler)
     batched   isentropic vortex OOC mesh list plus many 1-D Burgers problems of
               uneven sizes, all in one batch
@@ -34,6 +35,35 @@ def kh_prim(n: int, seed: int = 12345) -> np.ndarray:
     p[0, 0] = np.where(inner, 2.0, 1.0)
     p[1, 0] = np.where(inner, 0.5, -0.5)
     p[2, 0] = 0.01 * np.sin(4 * np.pi * X) + rng.uniform(-1e-3, 1e-3, (n, n))
+    p[4, 0] = 2.5
+    return p
+
+
+def kh_prim_nested(n: int, n_fine: int, seed: int = 12345) -> np.ndarray:
+    """The Kelvin-Helmholtz state of kh_prim with one noise field for every
+    grid: the U(-1e-3, 1e-3) noise is drawn once per cell of the n_fine grid
+    and averaged over the fine cells of each n x n cell (n divides n_fine), so
+    that the grids of a convergence study start from the same function.  The
+    density / velocity jumps at |y - 0.5| = 0.25 lie on cell faces when 4
+    divides n; v = 0.01 sin(4 pi x) is taken as the cell-average of the fine
+    grid's point values too."""
+    if n_fine % n:
+        raise ValueError("n must divide n_fine")
+    r = n_fine // n
+    rng = np.random.default_rng(seed)
+    noise = rng.uniform(-1e-3, 1e-3, (n_fine, n_fine))
+    hf = 1.0 / n_fine
+    xf = (np.arange(n_fine) + 0.5) * hf
+    vf = 0.01 * np.sin(4 * np.pi * xf)[None, :] + noise
+    v = vf.reshape(n, r, n, r).mean(axis=(1, 3))
+    h = 1.0 / n
+    x = (np.arange(n) + 0.5) * h
+    X, Y = np.meshgrid(x, x)
+    inner = np.abs(Y - 0.5) < 0.25
+    p = np.zeros((5, 1, n, n))
+    p[0, 0] = np.where(inner, 2.0, 1.0)
+    p[1, 0] = np.where(inner, 0.5, -0.5)
+    p[2, 0] = v
     p[4, 0] = 2.5
     return p
 

@@ -206,7 +206,11 @@ DSPW_API int dspw_stage(dspw_handle* h, int rk, double dt);
 /* Up to nsteps steps of the FV::run loop body on every unfinished problem:
  * CFL dt, clipping to the next time stamp, all stages, time += dt.  With
  * fixed_dt > 0 the CFL step is replaced by fixed_dt.  Steps run as one CUDA
- * graph per step; nothing is copied to the host. */
+ * graph per step; nothing is copied to the host.  After the final
+ * synchronisation the call returns the first health error the device has
+ * recorded since the last dspw_last_status (DSPW_ERR_NONFINITE or
+ * DSPW_ERR_NONPOSITIVE from the last stage's check of every cell), DSPW_OK if
+ * none; dspw_stage does the same after its stage. */
 DSPW_API int dspw_step(dspw_handle* h, int nsteps, double fixed_dt);
 
 /* Advance every problem until final_time/max_iter, checking completion every
