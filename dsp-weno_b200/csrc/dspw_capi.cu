@@ -419,13 +419,16 @@ ProbDev make_prob(const dspw_desc& d, long long off) {
 NetParams make_net(const dspw_desc& dn) {
   NetParams np;
   memset(&np, 0, sizeof(np));
+  // the FP32 form's last layer yields base-2 logits (its softmax uses 2^x)
+  const double log2e = 1.4426950408889634;
   for (int l = 0; l < 4; l++)
     for (int j = 0; j < 5; j++) {
+      const double f = l == 3 ? log2e : 1.0;
       np.b[l][j] = dn.nn_b[l][j];
-      np.bf[l][j] = (float)dn.nn_b[l][j];
+      np.bf[l][j] = (float)(dn.nn_b[l][j] * f);
       for (int k = 0; k < 5; k++) {
         np.w[l][j][k] = dn.nn_w[l][j][k];
-        np.wf[l][j][k] = (float)dn.nn_w[l][j][k];
+        np.wf[l][j][k] = (float)(dn.nn_w[l][j][k] * f);
       }
     }
   // nn_use_box: the network carries a training box of its inputs; inputs

@@ -719,38 +719,40 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>*
   bool guard = fabsf(u2 - u1) < fmaxf(1e-15f, 4.0f * 1.1920929e-07f * mag);
   float feat[5], vx[5], vy[5];
   nn_features<float>(u0, u1, u2, u3, feat, vx, vy);
-  // one finiteness test of the sum: a NaN or infinity anywhere propagates into
-  // it (an overflow of the sum of huge finite vertices also lands on the
-  // SP-WENO fallback, which is a valid reconstruction)
-  float sum = 0.f;
-#pragma unroll
-  for (int k = 0; k < 5; k++) sum += (feat[k] + vx[k]) + vy[k];
-  const bool finite = isfinite(sum);
-  bool use = valid && !guard && finite;
-  if (!use) { feat[0] = feat[1] = feat[2] = feat[3] = feat[4] = 0.f; }
   bool inbox = true;
   if (NP.use_box) {
 #pragma unroll
     for (int k = 0; k < 5; k++) inbox = inbox && feat[k] >= NP.feat_lo[k] && feat[k] <= NP.feat_hi[k];
   }
+  // Every lane's features go through the tiles, whatever they hold: each
+  // instance is one row of the A operand, so a NaN or infinity of one lane (a
+  // guard lane, an invalid lane, degenerate features) reaches only that lane's
+  // logits and never another's.
   float lg[5];
   warp_mlp_bf16(sm->ns, feat, lg, lane);
   if (!valid) return 0;
   if (guard) { l = 0.f; r = 0.f; return 0; }
-  if (!finite || !inbox) {   // degenerate features or outside the training range: plain SP-WENO
-    sp_weno<float>(u0, u1, u2, u3, 0, l, r);
-    if (sign_violation<float>(u0, u1, u2, u3, l, r)) signv++;   // not limited: checked here
-    return 0;
+  if (inbox) {
+    nn_finish<float>(lg, vx, vy, u0, u1, u2, u3, l, r);
+    // non-finite features or vertices (the only way to a non-finite
+    // reconstruction of a finite stencil) fall back to SP-WENO below; so does
+    // an overflow of l + r of huge finite values, which SP-WENO also handles
+    if (isfinite(l + r)) {
+      // sign-preserving limiter: the reconstructed jump must not oppose the
+      // cell jump; an opposing jump is replaced by zero, so the property holds
+      // exactly.
+      const float dj = u2 - u1, rj = r - l;
+      if (dj * rj < 0.f) {
+        const float c = 0.5f * (l + r);
+        l = c; r = c;
+        return 1;
+      }
+      return 0;
+    }
   }
-  nn_finish<float>(lg, vx, vy, u0, u1, u2, u3, l, r);
-  // sign-preserving limiter: the reconstructed jump must not oppose the cell
-  // jump; an opposing jump is replaced by zero, so the property holds exactly.
-  float dj = u2 - u1, rj = r - l;
-  if (dj * rj < 0.f) {
-    float c = 0.5f * (l + r);
-    l = c; r = c;
-    return 1;
-  }
+  // degenerate features or outside the training range: plain SP-WENO
+  sp_weno<float>(u0, u1, u2, u3, 0, l, r);
+  if (sign_violation<float>(u0, u1, u2, u3, l, r)) signv++;   // not limited: checked here
   return 0;
 }
 

@@ -35,6 +35,13 @@ template <> struct Mth<float> {
   static DSPW_HD float rcp(float a) { return __frcp_rn(a); }
   static DSPW_HD float log(float a) { return __logf(a); }
   static DSPW_HD float exp(float a) { return __expf(a); }
+  // 2^a on the special-function unit (one instruction; the FP32 network's
+  // last layer is scaled by log2 e so that its softmax needs no other factor)
+  static DSPW_HD float exp2(float a) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+  }
   static DSPW_HD float tanh(float a) {
     float r;
     asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(a));
@@ -214,6 +221,8 @@ DSPW_HD void sp_weno(T s0, T s1, T s2, T s3, int corr, T& recl, T& recr) {
 struct NetParams {
   double w[4][5][5];
   double b[4][5];
+  // FP32 copies for the tensor-core form; the last layer (l = 3) times log2 e,
+  // so that its logits are base-2 (nn_finish)
   float wf[4][5][5];
   float bf[4][5];
   float feat_lo[5], feat_hi[5];   // training box of the network inputs (FP32 form fallback)
@@ -305,7 +314,10 @@ DSPW_HD void nn_features(T u0, T u1, T u2, T u3, T feat[5], T vx[5], T vy[5]) {
 }
 
 // softmax (neural_network.cc:276-295) and the vertex combination / weights /
-// compute_recon (:62-76, :320-325) from the 5 output logits
+// compute_recon (:62-76, :320-325) from the 5 output logits.  The FP32 form's
+// logits are in base 2 (its last layer carries the factor log2 e, NetParams),
+// so its softmax weights are 2^(lg - max): the same weights as e^(lg' - max')
+// of the unscaled logits lg'.
 template <typename T>
 DSPW_HD void nn_finish(const T lg[5], const T vx[5], const T vy[5], T u0, T u1, T u2, T u3, T& recl,
                        T& recr) {
@@ -316,7 +328,11 @@ DSPW_HD void nn_finish(const T lg[5], const T vx[5], const T vy[5], T u0, T u1, 
   for (int i = 0; i < 5; i++) mxv = m::max(mxv, lg[i]);
   T sum = T(0);
 #pragma unroll
-  for (int i = 0; i < 5; i++) { s[i] = m::exp(lg[i] - mxv); sum += s[i]; }
+  for (int i = 0; i < 5; i++) {
+    if constexpr (sizeof(T) == 4) s[i] = m::exp2(lg[i] - mxv);
+    else s[i] = m::exp(lg[i] - mxv);
+    sum += s[i];
+  }
   T C1 = T(0.0), C2 = T(0.0);
   if constexpr (sizeof(T) == 4) {
     // FP32 form: normalise the two weighted sums instead of the five weights
