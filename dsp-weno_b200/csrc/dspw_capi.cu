@@ -2,6 +2,7 @@
 // device buffers, per-problem tables, the per-step CUDA graph and the
 // host<->device copies.  All arithmetic runs in the kernels of
 // dspw_kernels.cuh (instantiated by dspw_fp64.cu / dspw_fp32.cu).
+#include <cuda.h>
 #include <dlfcn.h>
 #include <nccl.h>
 
@@ -154,6 +155,12 @@ struct SweepClass {
   int* dtask[3] = {nullptr, nullptr, nullptr};
   int* dpmap = nullptr;
   int grid[3] = {0, 0, 0};             // launch grid chosen by dspw_tune (0: one block per block-worth of tasks)
+  // TMA staging of the specialised y / z sweeps: the class's tensor maps
+  // (tma_map_index layout; null when the class does not qualify) and, per
+  // direction, whether the sweep stages with TMA (1, the default) or with
+  // per-thread cp.async copies (0), as dspw_tune picks
+  void* dtmap = nullptr;
+  int use_tma[3] = {1, 1, 1};
 };
 
 struct dspw_handle {
@@ -327,10 +334,11 @@ int validate(const dspw_desc& d) {
     for (int k = 0; k < 5; k++)
       if (!(d.nn_feat_lo[k] <= d.nn_feat_hi[k])) return DSPW_ERR_ARG;   // also rejects NaN bounds
   if (d.generic_kernels != 0 && d.generic_kernels != 1) return DSPW_ERR_ARG;
+  if (d.tile_staging != 0 && d.tile_staging != 1) return DSPW_ERR_ARG;
   for (int k = 0; k < 3; k++)
     if (!(d.cell_size[k] >= 0.0) || !std::isfinite(d.cell_size[k])) return DSPW_ERR_ARG;
   // unused slots stay zero, so that a later ABI version can give them a meaning
-  for (int k = 0; k < 6; k++)
+  for (int k = 0; k < 5; k++)
     if (d.reserved_i[k] != 0) return DSPW_ERR_ARG;
   for (int k = 0; k < 5; k++)
     if (d.reserved_d[k] != 0.0) return DSPW_ERR_ARG;
@@ -594,6 +602,7 @@ SweepArgs<T> stage_args(dspw_handle* h, int rk, int residual_only) {
   else out = out4[rk];
   if (residual_only) { in = 0; out = 1; }
   a.Uin = (const T*)buf(h, in);
+  a.tma_in = in;
   a.Un = (const T*)h->Un;
   a.Uout = (T*)buf(h, out);
   a.R = (T*)h->R;
@@ -632,11 +641,83 @@ cudaError_t launch_class_sweep(dspw_handle* h, SweepArgs<T> a, const SweepClass&
   a.pmap = c.dpmap;
   a.nprob = (int)c.probs.size();
   a.ntask = c.task_start[dir].back();
+  a.tmaps = c.dtmap;
+  a.tma = (c.dtmap && dir >= 1 && c.use_tma[dir]) ? 1 : 0;
   int grid = c.grid[dir] ? c.grid[dir] : default_grid(c, dir);
   return Launch<T>::sweep(dir, a, grid, h->stream, c.spec);
 }
 
 int enqueue_halo_exchange(dspw_handle* h, int rk);
+
+// cuTensorMapEncodeTiled of the driver, found through the runtime (no link
+// against libcuda); null when the driver does not offer it
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return (EncodeTiledFn)f;
+  }();
+  return fn;
+}
+
+// Tensor maps of the TMA staging for every specialised class of dimension 2
+// or 3 whose problems all have nx a multiple of 8 and 16-byte aligned rows and
+// planes: per problem and y / z direction, the three stage inputs with a box of
+// 8 x SEG_LOAD rows x nv planes, the residual and U^n with a box of
+// 8 x SEG_CELLS rows (tma_map_index).  The tensor of a problem is its interior
+// (nx, ny, nz) x nv planes; the box moves along the sweep direction.  A class
+// that does not qualify, or any encoding failure, keeps dtmap null: its sweeps
+// stage with cp.async.
+void build_tma_maps(dspw_handle* h) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return;
+  const int w = (int)h->elem, vec = 16 / w;
+  void* bufs[5] = {h->Un, h->Ua, h->Ub, h->R, h->Un};
+  for (SweepClass& c : h->classes) {
+    const int dim = c.spec >= 100 ? 1 : c.spec / 10;
+    if (c.spec == 0 || dim < 2) continue;
+    bool ok = h->ctot % vec == 0;
+    for (int p : c.probs) {
+      const ProbDev& P = h->hprob[p];
+      ok = ok && P.nx % COOP_COLS == 0 && P.off % vec == 0 && h->desc[p].tile_staging == 0;
+    }
+    if (!ok) continue;
+    const size_t n = c.probs.size();
+    std::vector<CUtensorMap> maps(n * 2 * TMA_SLOTS);
+    static_assert(sizeof(CUtensorMap) == TMA_MAP_BYTES, "tensor map size");
+    for (size_t i = 0; i < n && ok; i++) {
+      const ProbDev& P = h->hprob[c.probs[i]];
+      const cuuint64_t gdim[4] = {(cuuint64_t)P.nx, (cuuint64_t)P.ny, (cuuint64_t)P.nz, (cuuint64_t)P.nv};
+      const cuuint64_t gstride[3] = {(cuuint64_t)P.nx * w, (cuuint64_t)P.nx * P.ny * w, (cuuint64_t)h->ctot * w};
+      const cuuint32_t estride[4] = {1, 1, 1, 1};
+      for (int dir = 1; dir < dim && ok; dir++)
+        for (int slot = 0; slot < TMA_SLOTS && ok; slot++) {
+          const cuuint32_t rows = slot < 3 ? SEG_LOAD : SEG_CELLS;
+          const cuuint32_t box[4] = {(cuuint32_t)COOP_COLS, dir == 1 ? rows : 1u, dir == 2 ? rows : 1u,
+                                     (cuuint32_t)P.nv};
+          void* addr = (char*)bufs[slot] + (size_t)w * P.off;
+          ok = enc(&maps[tma_map_index((int)i, dir, slot)],
+                   w == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, addr, gdim, gstride,
+                   box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        }
+    }
+    if (!ok) continue;
+    void* d = nullptr;
+    if (cudaMalloc(&d, maps.size() * sizeof(CUtensorMap)) != cudaSuccess) continue;
+    if (cudaMemcpy(d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFree(d);
+      continue;
+    }
+    c.dtmap = d;
+  }
+}
 
 template <typename T>
 int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
@@ -710,13 +791,22 @@ int tune_grids(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
       if (c.task_start[dir].back() == 0) continue;
       const int g0 = default_grid(c, dir);
       const int bpsm = Launch<T>::sweep_blocks_per_sm(dir, c.spec);
-      std::vector<int> cand = {0};
+      std::vector<int> grids = {0};
       for (int k : {1, 2, 4})
-        if (bpsm > 0 && (long long)nsm * bpsm * k < g0) cand.push_back(nsm * bpsm * k);
+        if (bpsm > 0 && (long long)nsm * bpsm * k < g0) grids.push_back(nsm * bpsm * k);
+      // candidates (grid, staging): the y / z sweeps of a class with tensor
+      // maps also try per-thread cp.async staging instead of TMA
+      const int tma0 = c.use_tma[dir];
+      std::vector<std::pair<int, int>> cand;
+      for (int g : grids) {
+        cand.push_back({g, tma0});
+        if (c.dtmap && dir >= 1) cand.push_back({g, 1 - tma0});
+      }
       double best = 1e300;
-      int best_grid = 0;
-      for (int g : cand) {
+      int best_grid = 0, best_tma = tma0;
+      for (auto [g, tm] : cand) {
         c.grid[dir] = g;
+        c.use_tma[dir] = tm;
         std::vector<float> t(reps);
         for (int r = 0; r < reps && ret == DSPW_OK; r++) {
           if (cudaEventRecord(e0, h->stream) != cudaSuccess ||
@@ -728,17 +818,23 @@ int tune_grids(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
         if (ret) break;
         std::sort(t.begin(), t.end());
         const double med = t[reps / 2];
-        if (g == 0) tot_before += med;
-        if (med < best) { best = med; best_grid = g; }
+        if (g == 0 && tm == tma0) tot_before += med;
+        if (med < best) { best = med; best_grid = g; best_tma = tm; }
       }
       c.grid[dir] = best_grid;
+      c.use_tma[dir] = best_tma;
       if (ret) break;
       tot_after += best;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (ret) { for (SweepClass& c : h->classes) c.grid[0] = c.grid[1] = c.grid[2] = 0; }
+  if (ret) {
+    for (SweepClass& c : h->classes) {
+      c.grid[0] = c.grid[1] = c.grid[2] = 0;
+      c.use_tma[0] = c.use_tma[1] = c.use_tma[2] = 1;
+    }
+  }
   // the timing runs counted faces; the status is the solver's, not the tuner's
   if (cudaMemcpy(h->dstatus, &saved, sizeof(saved), cudaMemcpyHostToDevice) != cudaSuccess) ret = DSPW_ERR_CUDA;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
@@ -1083,6 +1179,7 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
     }
     CKC(cudaMemcpy(h->dst, hs.data(), sizeof(ProbState) * nprob, cudaMemcpyHostToDevice));
   }
+  build_tma_maps(h);
   *out = h;
   return DSPW_OK;
 fail:
@@ -1105,6 +1202,7 @@ int dspw_destroy(dspw_handle* h) {
     for (int dir = 0; dir < 3; dir++)
       if (c.dtask[dir]) cudaFree(c.dtask[dir]);
     if (c.dpmap) cudaFree(c.dpmap);
+    if (c.dtmap) cudaFree(c.dtmap);
   }
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;

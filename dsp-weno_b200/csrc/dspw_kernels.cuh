@@ -138,7 +138,20 @@ struct SweepArgs {
   unsigned long long* collect_count;
   unsigned long long collect_cap;
   unsigned collect_stride;
+  // TMA staging of the specialised y / z sweeps (tma = 1): tensor maps of the
+  // class's problems in global memory, TMA_SLOTS per problem and direction
+  // (tma_map_index), and the slot of the state this stage reads
+  const void* tmaps;
+  int tma;
+  int tma_in;              // 0: U^n, 1: Ua, 2: Ub
 };
+
+// Tensor maps of the TMA staging, per (class problem, direction 1 / 2):
+// slots 0-2 the stage input U^n / Ua / Ub with a box of SEG_LOAD rows, slot 3
+// the residual and slot 4 U^n with a box of SEG_CELLS rows.  A map is 128 bytes.
+constexpr int TMA_SLOTS = 5;
+constexpr int TMA_MAP_BYTES = 128;
+__host__ __device__ constexpr inline int tma_map_index(int p, int dir, int slot) { return (p * 2 + (dir - 1)) * TMA_SLOTS + slot; }
 
 // append one training pair (sampled by a hash of the reconstruction's position)
 template <typename T>
@@ -1248,6 +1261,78 @@ __device__ inline void tile_cons(const T (*U)[SEG_CELLS][COOP_COLS], int nv, int
 // epilogue from shared memory.  When the rows are not 16-byte aligned in
 // global memory (nx, the problem offset or the plane stride not a multiple of
 // 16 bytes) the same tiles are filled by plain loads.
+// Conversion of the staged rows of a block task: row q = tid / 8 (+ 32) of
+// column col, from the tile U (ghost rows already resolved to their source
+// rows), into the per-warp primitive / entropy rows of warp `col`.
+template <typename T, int DIR>
+__device__ inline void coop_convert(const ProbDev& P, WarpSmem<T>* sm0, const T (*U)[SEG_LOAD][COOP_COLS], int c0,
+                                    int nrow, int ncols) {
+  const int tid = threadIdx.x, col = tid % COOP_COLS;
+  const int N = dir_len<DIR>(P);
+  const T G = T(P.gamma);
+  for (int q = tid / COOP_COLS; q < nrow && col < ncols; q += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
+    const int c = c0 - 2 + q;
+    const int side = c < 0 ? 0 : 1;
+    const int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
+    T p[5];
+    if (kind == DSPW_BC_DIRICHLET) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) p[v] = T(P.bc_state[2 * DIR + side][v]);
+    } else {
+      int flip;
+      ghost_source(c, N, kind, flip);
+      T u[5];
+      tile_cons<T>(U, P.nv, q, col, u);
+      cons_to_prim<T>(u, G, p);
+      if (flip) p[1 + DIR] = -p[1 + DIR];
+    }
+    T v[5];
+    prim_to_ent<T>(p, G, v);
+    WarpSmem<T>* sc = sm0 + col;
+#pragma unroll
+    for (int w = 0; w < 5; w++) { sc->P[w][q] = p[w]; sc->V[w][q] = v[w]; }
+  }
+}
+
+// Cell epilogue of a block task: residual from the tile R and the warps' face
+// fluxes, then either the stored residual or the stage update from the tiles
+// U (rows + 2) and Un, with threads laid out as 4 rows x 8 columns per warp
+// instruction (coalesced stores).
+template <typename T, int DIR>
+__device__ inline void coop_epilogue(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, WarpSmem<T>* sm0,
+                                     const T (*U)[SEG_LOAD][COOP_COLS], const T (*Rt)[SEG_CELLS][COOP_COLS],
+                                     const T (*Unt)[SEG_CELLS][COOP_COLS], int i0, int j0, int k0, int c0,
+                                     int ncell, int ncols, bool final_sweep, double& smax, double& ent,
+                                     unsigned& bad_fin, unsigned& bad_pos) {
+  const int tid = threadIdx.x, col = tid % COOP_COLS;
+  const int nv = P.nv;
+  for (int row = tid / COOP_COLS; row < ncell && col < ncols; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
+    WarpSmem<T>* sc = sm0 + col;
+    T R[5], r0[5];
+    tile_cons<T>(Rt, nv, row, col, r0);
+#pragma unroll
+    for (int v = 0; v < 5; v++) R[v] = (r0[v] - sc->F[v][row]) + sc->F[v][row + 1];
+    const long long cell = cell_index<DIR>(P, i0 + col, j0, k0, c0 + row);
+    if (!final_sweep) {
+      store_cons<T>(A.R, A.ctot, cell, nv, R);
+    } else {
+      T u[5], un[5];
+      tile_cons<T>(U, nv, row + 2, col, u);
+      tile_cons<T>(Unt, nv, row, col, un);
+      update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
+    }
+  }
+}
+
+// Block-cooperative variant for the y and z sweeps: the 8 warps of the block
+// hold 8 adjacent x-columns of the same line segment.  The block first issues
+// asynchronous row copies (8 adjacent x per row and plane) of the staged cells
+// and, as a second group, of the residual and U^n of its cells; it converts the
+// staged rows once the first group has landed, evaluates the faces per warp as
+// in euler_task while the second group is in flight, and runs the cell
+// epilogue from shared memory.  When the rows are not 16-byte aligned in
+// global memory (nx, the problem offset or the plane stride not a multiple of
+// 16 bytes) the same tiles are filled by plain loads.
 template <typename T, int DIR, int DIM, typename Sp>
 __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbState& S,
                                  WarpSmem<T>* sm0, int lt0, bool group) {
@@ -1257,8 +1342,6 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   if (group) decode_group<DIR>(P, lt0, i0, j0, k0, c0, ncell, ncols);
   else decode_task<DIR>(P, lt0, i0, j0, k0, c0, ncell);
   const int N = dir_len<DIR>(P);
-  const T G = T(P.gamma);
-  const int col = tid % COOP_COLS;
   const int nv = P.nv;
   CoopTiles<T>& tl = *reinterpret_cast<CoopTiles<T>*>(sm0 + WARPS_PER_BLOCK);
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
@@ -1315,29 +1398,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
     }
   }
   __syncthreads();
-  // conversion of the staged rows: row q = tid / 8 (+ 32) of column col
-  for (int q = tid / COOP_COLS; q < nrow && col < ncols; q += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
-    const int c = c0 - 2 + q;
-    const int side = c < 0 ? 0 : 1;
-    const int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
-    T p[5];
-    if (kind == DSPW_BC_DIRICHLET) {
-#pragma unroll
-      for (int v = 0; v < 5; v++) p[v] = T(P.bc_state[2 * DIR + side][v]);
-    } else {
-      int flip;
-      ghost_source(c, N, kind, flip);
-      T u[5];
-      tile_cons<T>(tl.U, nv, q, col, u);
-      cons_to_prim<T>(u, G, p);
-      if (flip) p[1 + DIR] = -p[1 + DIR];
-    }
-    T v[5];
-    prim_to_ent<T>(p, G, v);
-    WarpSmem<T>* sc = sm0 + col;
-#pragma unroll
-    for (int w = 0; w < 5; w++) { sc->P[w][q] = p[w]; sc->V[w][q] = v[w]; }
-  }
+  coop_convert<T, DIR>(P, sm0, tl.U, c0, nrow, ncols);
   __syncthreads();
   int viol = 0;
   unsigned long long signv = 0;
@@ -1349,27 +1410,229 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   double smax = 0.0;
   double ent = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
-  for (int row = tid / COOP_COLS; row < ncell && col < ncols; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
-    WarpSmem<T>* sc = sm0 + col;
-    T R[5], r0[5];
-    tile_cons<T>(tl.R, nv, row, col, r0);
-#pragma unroll
-    for (int v = 0; v < 5; v++) R[v] = (r0[v] - sc->F[v][row]) + sc->F[v][row + 1];
-    const long long cell = cell_index<DIR>(P, i0 + col, j0, k0, c0 + row);
-    if (!final_sweep) {
-      store_cons<T>(A.R, A.ctot, cell, nv, R);
-    } else {
-      T u[5], un[5];
-      tile_cons<T>(tl.U, nv, row + 2, col, u);
-      tile_cons<T>(tl.Un, nv, row, col, un);
-      update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
-    }
-  }
+  coop_epilogue<T, DIR>(A, P, S, sm0, tl.U, tl.R, tl.Un, i0, j0, k0, c0, ncell, ncols, final_sweep, smax, ent,
+                        bad_fin, bad_pos);
   if (!final_sweep) { smax = 0.0; ent = 0.0; }
   SweepArgs<T> A2 = A;
   A2.final_stage = A.final_stage && final_sweep;
   warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
   __syncthreads();
+}
+
+// --------------------------------------------------- TMA staging (y / z) --
+//
+// The specialised y and z sweeps can stage their tiles with the Tensor Memory
+// Accelerator instead of per-thread cp.async copies: one thread issues one
+// cp.async.bulk.tensor per tile (box of 8 columns x rows x nv planes of this
+// GPU's own state, no multicast) that signals an mbarrier when its bytes have
+// landed.  Each block runs its tasks in a loop that prefetches the next task's
+// staged rows into a second buffer while the current task's faces are
+// evaluated, and loads the residual and U^n of a task at the task's start (they
+// are read only by its epilogue).  Rows outside the problem (the two ghost rows
+// of a segment at a domain face) are outside the tensor map, so the box fills
+// them with zeros; they are then replaced by their boundary-condition source
+// rows with plain loads, as the cp.async path stages them.  Every wait on an
+// mbarrier is bounded: after TMA_WAIT_LIMIT tries the block records
+// DSPW_ERR_TIMEOUT in the status word and leaves the loop.
+
+// byte layout of the TMA region (behind the per-warp scratch, 128-byte
+// aligned): three mbarriers, two staged-row tiles, the residual tile, the U^n tile
+template <typename T>
+struct TmaLayout {
+  static constexpr size_t round128(size_t b) { return (b + 127) / 128 * 128; }
+  static constexpr size_t u_bytes = round128(sizeof(T) * 5 * SEG_LOAD * COOP_COLS);
+  static constexpr size_t r_bytes = round128(sizeof(T) * 5 * SEG_CELLS * COOP_COLS);
+  static constexpr size_t bars = 128;
+  static constexpr size_t total = bars + 2 * u_bytes + 2 * r_bytes + 128;   // + alignment slack
+};
+
+constexpr long long TMA_WAIT_LIMIT = 1LL << 24;
+
+__device__ inline unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ inline void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ inline void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ inline bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the phase of the given parity; false after TMA_WAIT_LIMIT tries
+__device__ inline bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (long long i = 0; i < TMA_WAIT_LIMIT; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// generic-proxy accesses of shared memory before this point are ordered before
+// later asynchronous-proxy (TMA) accesses
+__device__ inline void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 4-D tiled load (x, y, z, component) of this GPU's global memory into shared
+// memory, completion counted on the mbarrier; x is a multiple of 8 elements
+// (16-byte aligned), y / z may lie outside the tensor (zero fill)
+__device__ inline void tma_load_4d(void* dst, const void* map, int x, int y, int z, int c, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(c), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// the next task >= g of this block's stride whose problem is stepping (or any
+// task for a residual evaluation); A.ntask when none is left
+template <typename T>
+__device__ inline int next_live_task(const SweepArgs<T>& A, int g) {
+  for (; g < A.ntask; g += gridDim.x) {
+    if (A.residual_only) return g;
+    const int p = find_problem(A.task_start, A.nprob, g);
+    const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+    if (*((volatile int*)&A.st[pp].active)) return g;
+  }
+  return A.ntask;
+}
+
+// coordinates of task g's tile origin: problem (class index), column i0 and
+// the (y, z) of its first cell row
+template <typename T, int DIR>
+__device__ inline void tma_task(const SweepArgs<T>& A, int g, int& p, int& i0, int& j0, int& k0, int& c0, int& ncell) {
+  p = find_problem(A.task_start, A.nprob, g);
+  const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+  int ncols;
+  decode_group<DIR>(A.prob[pp], g - __ldg(A.task_start + p), i0, j0, k0, c0, ncell, ncols);
+}
+
+template <typename T, int DIR>
+__device__ inline void tma_issue_rows(const SweepArgs<T>& A, int g, unsigned char* ubuf, unsigned long long* bar) {
+  int p, i0, j0, k0, c0, ncell;
+  tma_task<T, DIR>(A, g, p, i0, j0, k0, c0, ncell);
+  const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+  const int nv = A.prob[pp].nv;
+  const unsigned char* maps = (const unsigned char*)A.tmaps;
+  mbar_expect_tx(bar, (unsigned)(sizeof(T) * COOP_COLS * SEG_LOAD * nv));
+  const int y = DIR == 1 ? c0 - 2 : j0, z = DIR == 1 ? k0 : c0 - 2;
+  tma_load_4d(ubuf, maps + (size_t)TMA_MAP_BYTES * tma_map_index(p, DIR, A.tma_in), i0, y, z, 0, bar);
+}
+
+template <typename T, int DIR>
+__device__ inline void tma_issue_cells(const SweepArgs<T>& A, int g, bool final_sweep, unsigned char* rbuf,
+                                       unsigned char* unbuf, unsigned long long* bar) {
+  int p, i0, j0, k0, c0, ncell;
+  tma_task<T, DIR>(A, g, p, i0, j0, k0, c0, ncell);
+  const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+  const int nv = A.prob[pp].nv;
+  const unsigned char* maps = (const unsigned char*)A.tmaps;
+  const unsigned bytes = (unsigned)(sizeof(T) * COOP_COLS * SEG_CELLS * nv);
+  mbar_expect_tx(bar, final_sweep ? 2 * bytes : bytes);
+  const int y = DIR == 1 ? c0 : j0, z = DIR == 1 ? k0 : c0;
+  tma_load_4d(rbuf, maps + (size_t)TMA_MAP_BYTES * tma_map_index(p, DIR, 3), i0, y, z, 0, bar);
+  if (final_sweep) tma_load_4d(unbuf, maps + (size_t)TMA_MAP_BYTES * tma_map_index(p, DIR, 4), i0, y, z, 0, bar);
+}
+
+// The task loop of a specialised y / z sweep with TMA staging (see above).
+// Every problem of the class has nx a multiple of 8 and 16-byte aligned rows
+// (the host builds the tensor maps only then), so every task is a full group
+// of 8 columns.
+template <typename T, int DIR, int DIM, typename Sp>
+__device__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpSmem<T>* sm0) {
+  typedef TmaLayout<T> L;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned char* base = reinterpret_cast<unsigned char*>(sm0 + WARPS_PER_BLOCK);
+  base = reinterpret_cast<unsigned char*>(((size_t)base + 127) & ~(size_t)127);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);   // [0], [1]: rows; [2]: cells
+  unsigned char* ubuf[2] = {base + L::bars, base + L::bars + L::u_bytes};
+  unsigned char* rbuf = base + L::bars + 2 * L::u_bytes;
+  unsigned char* unbuf = rbuf + L::r_bytes;
+  typedef const T(*UTile)[SEG_LOAD][COOP_COLS];
+  typedef const T(*CTile)[SEG_CELLS][COOP_COLS];
+  const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async_smem();
+  }
+  __syncthreads();
+  unsigned ph_u[2] = {0u, 0u}, ph_c = 0u;
+  int g = next_live_task(A, blockIdx.x);
+  if (tid == 0 && g < A.ntask) tma_issue_rows<T, DIR>(A, g, ubuf[0], &bar[0]);
+  int b = 0;
+  bool timed_out = false;
+  while (g < A.ntask) {
+    const int gn = next_live_task(A, g + gridDim.x);
+    int p, i0, j0, k0, c0, ncell;
+    tma_task<T, DIR>(A, g, p, i0, j0, k0, c0, ncell);
+    const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+    const ProbDev& P = A.prob[pp];
+    ProbState& S = A.st[pp];
+    const int N = dir_len<DIR>(P);
+    const int nrow = ncell + 4;
+    // the cell tiles of this task (free: the previous task ended at a barrier)
+    if (tid == 0) {
+      fence_proxy_async_smem();
+      tma_issue_cells<T, DIR>(A, g, final_sweep, rbuf, unbuf, &bar[2]);
+    }
+    // staged rows of this task (prefetched)
+    if (!mbar_wait(&bar[b], ph_u[b])) timed_out = true;
+    ph_u[b] ^= 1u;
+    // rows outside the problem: their boundary-condition source rows
+    T(*U)[SEG_LOAD][COOP_COLS] = reinterpret_cast<T(*)[SEG_LOAD][COOP_COLS]>(ubuf[b]);
+    for (int idx = tid; idx < nrow * COOP_COLS; idx += WARPS_PER_BLOCK * 32) {
+      const int q = idx / COOP_COLS, cc = idx - q * COOP_COLS;
+      const int c = c0 - 2 + q;
+      if (c >= 0 && c < N) continue;
+      const int kind = P.bc[2 * DIR + (c < 0 ? 0 : 1)];
+      if (kind == DSPW_BC_DIRICHLET) continue;
+      int flip;
+      const int src = ghost_source(c, N, kind, flip);
+      const long long cell = cell_index<DIR>(P, i0 + cc, j0, k0, src);
+      for (int comp = 0; comp < P.nv; comp++) U[comp][q][cc] = A.Uin[comp * A.ctot + cell];
+    }
+    __syncthreads();
+    coop_convert<T, DIR>(P, sm0, (UTile)U, c0, nrow, COOP_COLS);
+    __syncthreads();
+    // the next task's rows into the other buffer, behind this task's faces
+    if (tid == 0 && gn < A.ntask) {
+      fence_proxy_async_smem();
+      tma_issue_rows<T, DIR>(A, gn, ubuf[b ^ 1], &bar[b ^ 1]);
+    }
+    int viol = 0;
+    unsigned long long signv = 0;
+    unsigned checked = 0;
+    const int lt0 = g - __ldg(A.task_start + p);
+    euler_faces<T, DIR, DIM, Sp>(A, P, sm0 + warp, lane, ncell, viol, signv, checked, (unsigned)(lt0 + warp));
+    if (!mbar_wait(&bar[2], ph_c)) timed_out = true;
+    ph_c ^= 1u;
+    __syncthreads();
+    double smax = 0.0, ent = 0.0;
+    unsigned bad_fin = 0, bad_pos = 0;
+    coop_epilogue<T, DIR>(A, P, S, sm0, (UTile)U, (CTile)rbuf, (CTile)unbuf, i0, j0, k0, c0, ncell, COOP_COLS,
+                          final_sweep, smax, ent, bad_fin, bad_pos);
+    if (!final_sweep) { smax = 0.0; ent = 0.0; }
+    SweepArgs<T> A2 = A;
+    A2.final_stage = A.final_stage && final_sweep;
+    warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
+    // this task's shared-memory accesses (the ghost-row stores among them) are
+    // ordered before the TMA writes that refill the tiles; the barrier ends
+    // the task for every thread
+    fence_proxy_async_smem();
+    if (__syncthreads_or(timed_out)) {
+      // a copy that did not complete: record it and wait (bounded) for the
+      // prefetch still in flight before the block leaves
+      if (tid == 0) atomicCAS(&A.status->code, 0, DSPW_ERR_TIMEOUT);
+      if (gn < A.ntask) mbar_wait(&bar[b ^ 1], ph_u[b ^ 1]);
+      break;
+    }
+    g = gn;
+    b ^= 1;
+  }
 }
 
 // scalar laws: lin_/bur_ fluxes (enflo_scalar/src_scalar/num_flux.cc:12-57,
@@ -1465,6 +1728,10 @@ k_sweep(SweepArgs<T> A) {
   if (!Sp::fixed || Sp::rec == 2) net_frag_stage<T>(*A.net, lane, sm->ns);
   if constexpr (Sp::fixed && DIR >= 1) {
     // specialised y / z sweeps: every task is one block-cooperative column group
+    if (A.tma) {
+      euler_coop_tma_loop<T, DIR, Sp::dim, Sp>(A, sm0);
+      return;
+    }
     for (int g = blockIdx.x; g < A.ntask; g += gridDim.x) {
       const int p = find_problem(A.task_start, A.nprob, g);
       const int pp = A.pmap ? __ldg(A.pmap + p) : p;

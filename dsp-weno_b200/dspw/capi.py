@@ -52,7 +52,7 @@ class Desc(C.Structure):
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
         ("bc", C.c_int * 6), ("ec1_fix", C.c_int), ("mu_model", C.c_int),
         ("max_iter", C.c_int), ("t_stamps", C.c_int), ("nn_use_box", C.c_int), ("generic_kernels", C.c_int),
-        ("reserved_i", C.c_int * 6),
+        ("tile_staging", C.c_int), ("reserved_i", C.c_int * 5),
         ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double),
         ("zmin", C.c_double), ("zmax", C.c_double),
         ("gamma", C.c_double), ("gas_const", C.c_double), ("prandtl", C.c_double),
