@@ -196,6 +196,7 @@ struct dspw_handle {
   // (slot-major, diag_cap slots of nprob rows) and the rows drained to the host
   int diag_cap = 0;
   DiagAcc* ddiag = nullptr;
+  double* ddiag_part = nullptr;        // block partial rows of one diagnostics launch
   double* drows = nullptr;
   long long* dnode_start = nullptr;
   long long nodes_tot = 0;
@@ -486,6 +487,7 @@ DiagArgs<T> diag_args(dspw_handle* h, const long long* start, const T* U) {
   d.prob = h->dprob;
   d.st = h->dst;
   d.acc = h->ddiag;
+  d.part = h->ddiag_part;
   d.nprob = h->nprob;
   d.start = start;
   d.U = U;
@@ -1195,7 +1197,7 @@ int dspw_destroy(dspw_handle* h) {
   if (h->comm) nccl().comm_destroy(h->comm);
   void* ptrs[] = {h->dprob, h->dst, h->dstatus, h->dnet, h->dcell_start, h->dnactive,
                   h->Un, h->Ua, h->Ub, h->R, h->R2, h->V, h->node, h->dstage, h->dscratch, h->dred,
-                  h->ddiag, h->drows, h->dnode_start, h->dsnap, h->dsnap_count, h->dsnap_meta};
+                  h->ddiag, h->ddiag_part, h->drows, h->dnode_start, h->dsnap, h->dsnap_count, h->dsnap_meta};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (SweepClass& c : h->classes) {
@@ -1408,9 +1410,10 @@ int dspw_diag_enable(dspw_handle* h, int capacity) {
   CK(cudaStreamSynchronize(h->stream));
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // the step graph changes
   if (h->ddiag) cudaFree(h->ddiag);
+  if (h->ddiag_part) cudaFree(h->ddiag_part);
   if (h->drows) cudaFree(h->drows);
   if (h->dnode_start) cudaFree(h->dnode_start);
-  h->ddiag = nullptr; h->drows = nullptr; h->dnode_start = nullptr;
+  h->ddiag = nullptr; h->ddiag_part = nullptr; h->drows = nullptr; h->dnode_start = nullptr;
   h->diag_cap = 0;
   h->nodes_tot = 0;
   h->diag_taken.assign(h->nprob, 0);
@@ -1424,13 +1427,17 @@ int dspw_diag_enable(dspw_handle* h, int capacity) {
     ns[p + 1] = ns[p] + (P.is_scalar ? 0 : (long long)(P.nx + 1) * (P.ny + 1) * (P.nz + 1));
   }
   const size_t ring = sizeof(double) * DIAG_COLS * (size_t)h->nprob * (size_t)capacity;
+  // partial rows: (blocks + problems) of the largest diagnostics launch
+  const size_t part = sizeof(double) * DIAG_NACC * (size_t)(device_sms() * 8LL + h->nprob);
   if (cudaMalloc(&h->ddiag, sizeof(DiagAcc) * h->nprob) != cudaSuccess ||
+      cudaMalloc(&h->ddiag_part, part) != cudaSuccess ||
       cudaMalloc(&h->drows, ring) != cudaSuccess ||
       cudaMalloc(&h->dnode_start, sizeof(long long) * (h->nprob + 1)) != cudaSuccess) {
     if (h->ddiag) cudaFree(h->ddiag);
+    if (h->ddiag_part) cudaFree(h->ddiag_part);
     if (h->drows) cudaFree(h->drows);
     if (h->dnode_start) cudaFree(h->dnode_start);
-    h->ddiag = nullptr; h->drows = nullptr; h->dnode_start = nullptr;
+    h->ddiag = nullptr; h->ddiag_part = nullptr; h->drows = nullptr; h->dnode_start = nullptr;
     h->last_error = DSPW_ERR_CUDA;
     return DSPW_ERR_CUDA;
   }

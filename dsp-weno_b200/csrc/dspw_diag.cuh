@@ -14,11 +14,14 @@
 //   scalar (enflo_scalar/src_scalar/fv.cc:572-576): after the step, of U^(n+1)
 //     total entropy  sum u^2 / 2 * vol, residual norm sqrt(sum R^2)
 //
-// Every sum is reduced per block and added to a per-problem FP64 accumulator
-// (one atomic per block and problem); a row kernel turns the accumulators into
-// one row per problem and step in a device ring that the host drains.  The
-// summation order differs from the reference's sequential loops, so the values
-// agree to rounding (about 1e-13 relative for FP64 states), not bit for bit.
+// Every sum is deterministic: each block covers a fixed contiguous range of
+// cells (or nodes) and reduces, in a fixed order, one row of partial sums per
+// problem it overlaps; a fold kernel adds a problem's rows in block order to
+// its FP64 accumulator; a row kernel turns the accumulators into one row per
+// problem and step in a device ring that the host drains.  The same state
+// gives the same bits on every run.  The summation order differs from the
+// reference's sequential loops, so the values agree with the reference's to
+// rounding (about 1e-13 relative for FP64 states), not bit for bit.
 #pragma once
 #include "dspw_kernels.cuh"
 
@@ -47,6 +50,10 @@ struct DiagArgs {
   long long ctot;
   double* rows;             // ring, slot-major: rows[(slot * nprob + p) * DIAG_COLS]
   int cap;
+  // partial sums of one launch, one row of DIAG_NACC per (block b, problem p)
+  // the block overlaps, at row b + p (a block's problems are consecutive, so
+  // b + p is different for every overlapping pair): (blocks + nprob) rows
+  double* part;
 };
 
 DSPW_HD int find_problem_ll(const long long* start, int nprob, long long g) {
@@ -58,8 +65,9 @@ DSPW_HD int find_problem_ll(const long long* start, int nprob, long long g) {
   return lo;
 }
 
-// sum v over the block and add the totals to acc[p] (every thread calls it)
-__device__ inline void block_add(double (&v)[DIAG_NACC], DiagAcc* acc, int p) {
+// block-wide sum of v[k] in a fixed order (warp shuffles, then the warps in
+// order); every thread calls it, thread 0 receives the totals
+__device__ inline void block_sum_fixed(double (&v)[DIAG_NACC]) {
   __shared__ double red[DIAG_NACC][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
@@ -68,29 +76,46 @@ __device__ inline void block_add(double (&v)[DIAG_NACC], DiagAcc* acc, int p) {
     if (lane == 0) red[k][warp] = s;
   }
   __syncthreads();
-  if (warp == 0) {
+  if (threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < DIAG_NACC; k++) {
-      double s = warp_sum(lane < nw ? red[k][lane] : 0.0);
-      if (lane == 0 && s != 0.0) atomicAdd(&acc[p].v[k], s);
+      double s = red[k][0];
+      for (int w = 1; w < nw; w++) s += red[k][w];
+      v[k] = s;
     }
   }
   __syncthreads();
 }
 
-// Walk a block-contiguous range of the flat index space [0, start[nprob]) in
-// tiles of blockDim.x; terms(p, g, t) fills the accumulator terms of item g of
-// problem p.  Tiles of one problem are summed in registers and reduced per
-// block when the problem changes; a tile that straddles problems adds its
-// items atomically.
+// row b + p of the partial sums: the block total of v (every thread calls it)
+__device__ inline void block_store(double (&v)[DIAG_NACC], double* part, int p) {
+  block_sum_fixed(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < DIAG_NACC; k++) part[((long long)blockIdx.x + p) * DIAG_NACC + k] = v[k];
+  }
+}
+
+// the block-contiguous range of block b of a launch of `nblocks` blocks over
+// [0, total): tiles of 256 items
+DSPW_HD long long diag_chunk(long long total, int nblocks) {
+  const long long per = (total + nblocks - 1) / nblocks;
+  return ((per + 255) / 256) * 256;
+}
+
+// Walk block b's range of the flat index space [0, start[nprob]) in tiles of
+// blockDim.x (256); terms(p, g, t) fills the accumulator terms of item g of
+// problem p.  The items of one problem accumulate per thread while the tiles
+// stay inside it; a tile that straddles problems is split by problem with
+// fixed-order block sums.  Every (block, problem) overlap ends in exactly one
+// row of partial sums (block_store), zeros included.
 template <typename F>
-__device__ inline void block_range_sums(const long long* start, int nprob, DiagAcc* acc, F terms) {
+__device__ inline void block_range_sums(const long long* start, int nprob, double* part, F terms) {
   const long long total = start[nprob];
-  const long long per = (total + gridDim.x - 1) / gridDim.x;
-  const long long chunk = ((per + blockDim.x - 1) / blockDim.x) * blockDim.x;
+  const long long chunk = diag_chunk(total, gridDim.x);
   const long long begin = (long long)blockIdx.x * chunk;
   const long long end = begin + chunk < total ? begin + chunk : total;
-  __shared__ int s_p0;
+  __shared__ int s_p0, s_pmax;
   int pend = -1;
   double sum[DIAG_NACC];
 #pragma unroll
@@ -106,13 +131,16 @@ __device__ inline void block_range_sums(const long long* start, int nprob, DiagA
       terms(p, g, t);
     }
     if (threadIdx.x == 0) s_p0 = p;
+    // the last valid item of the tile has the largest problem
+    const long long glast = (base + blockDim.x < end ? base + blockDim.x : end) - 1;
+    if (threadIdx.x == (int)(glast - base)) s_pmax = p;
     __syncthreads();
-    const int p0 = s_p0;
-    const bool uniform = __syncthreads_and(g >= end || p == p0);
-    if (uniform) {
+    const int p0 = s_p0, pmax = s_pmax;
+    __syncthreads();
+    if (p0 == pmax) {   // the tile lies in one problem
       if (p0 != pend) {
         if (pend >= 0) {
-          block_add(sum, acc, pend);
+          block_store(sum, part, pend);
 #pragma unroll
           for (int k = 0; k < DIAG_NACC; k++) sum[k] = 0.0;
         }
@@ -120,13 +148,55 @@ __device__ inline void block_range_sums(const long long* start, int nprob, DiagA
       }
 #pragma unroll
       for (int k = 0; k < DIAG_NACC; k++) sum[k] += t[k];
-    } else if (p >= 0) {
+    } else {
+      // problems p0 < ... < pmax (every one of them has items here): all but
+      // the last end in this tile.  A pending run of an earlier problem ended
+      // with the previous tile.
+      if (pend >= 0 && pend != p0) {
+        block_store(sum, part, pend);
 #pragma unroll
-      for (int k = 0; k < DIAG_NACC; k++)
-        if (t[k] != 0.0) atomicAdd(&acc[p].v[k], t[k]);
+        for (int k = 0; k < DIAG_NACC; k++) sum[k] = 0.0;
+        pend = -1;
+      }
+      for (int q = p0; q <= pmax; q++) {
+        double v[DIAG_NACC];
+#pragma unroll
+        for (int k = 0; k < DIAG_NACC; k++) v[k] = (q == pend ? sum[k] : 0.0) + (p == q ? t[k] : 0.0);
+        if (q < pmax) {
+          block_store(v, part, q);
+        } else {
+          // the last problem of the tile stays pending: its per-thread sums
+#pragma unroll
+          for (int k = 0; k < DIAG_NACC; k++) sum[k] = v[k];
+        }
+      }
+      pend = pmax;
     }
   }
-  if (pend >= 0) block_add(sum, acc, pend);
+  if (pend >= 0) block_store(sum, part, pend);
+}
+
+// fold the partial rows of one launch into each problem's accumulator, in
+// block order: one warp per problem (T: the state type of the launch's unit)
+template <typename T>
+__global__ void k_diag_fold(const long long* start, int nprob, const double* part, int nblocks, DiagAcc* acc) {
+  const int p = blockIdx.x;
+  if (p >= nprob) return;
+  const long long total = start[nprob];
+  const long long chunk = diag_chunk(total, nblocks);
+  if (start[p + 1] <= start[p]) return;
+  const int b0 = (int)(start[p] / chunk), b1 = (int)((start[p + 1] - 1) / chunk);
+  double s[DIAG_NACC];
+#pragma unroll
+  for (int k = 0; k < DIAG_NACC; k++) s[k] = 0.0;
+  for (int b = b0 + (int)threadIdx.x; b <= b1; b += 32)
+#pragma unroll
+    for (int k = 0; k < DIAG_NACC; k++) s[k] += part[((long long)b + p) * DIAG_NACC + k];
+#pragma unroll
+  for (int k = 0; k < DIAG_NACC; k++) {
+    const double x = warp_sum(s[k]);
+    if (threadIdx.x == 0) acc[p].v[k] += x;
+  }
 }
 
 // mode 0 (stage 0, systems): entropy, KE and pressure-work KE dissipation of
@@ -134,7 +204,7 @@ __device__ inline void block_range_sums(const long long* start, int nprob, DiagA
 // problem): residual norms; scalar energy of U^(n+1).
 template <typename T>
 __global__ void __launch_bounds__(256) k_diag_cells(DiagArgs<T> A, int mode) {
-  block_range_sums(A.start, A.nprob, A.acc, [&](int p, long long g, double* t) {
+  block_range_sums(A.start, A.nprob, A.part, [&](int p, long long g, double* t) {
     const ProbDev& P = A.prob[p];
     if (!A.st[p].active) return;
     if (P.is_scalar) {
@@ -254,7 +324,7 @@ __device__ inline void node_state(const DiagArgs<T>& A, const ProbDev& P, int a,
 // (Nx+1)(Ny+1)(Nz+1) nodes of each problem, of U^n at stage 0
 template <typename T>
 __global__ void __launch_bounds__(256) k_diag_nodes(DiagArgs<T> A) {
-  block_range_sums(A.start, A.nprob, A.acc, [&](int p, long long g, double* t) {
+  block_range_sums(A.start, A.nprob, A.part, [&](int p, long long g, double* t) {
     const ProbDev& P = A.prob[p];
     if (!A.st[p].active || P.is_scalar) return;
     const long long l = g - A.start[p];

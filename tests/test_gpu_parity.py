@@ -396,7 +396,10 @@ def test_entropy_inequality_checked_every_step():
     s32.upload_prim(st)
     s32.step(20)
     got32, steps32 = s32.entropy_check()
-    assert steps32 == 20 and got32 < 1e-5, got32
+    # each cell's entropy in FP32 (relative rounding 6e-8), the sums in FP64:
+    # a rise beyond that rounding would be a real entropy production
+    print(f"FP32 DSP-WENO largest one-step relative entropy rise {got32:.3e}")
+    assert steps32 == 20 and got32 < 2e-7, got32
     # scalar entropy u^2/2 of an entropy-stable Burgers flux
     db = make_desc(model="burgers", flux="bur_tecno4", recon="sp_weno", nx=200, ny=1, nz=1, x=(-np.pi, np.pi))
     sb = Solver(db)
