@@ -156,11 +156,13 @@ struct SweepClass {
   int* dpmap = nullptr;
   int grid[3] = {0, 0, 0};             // launch grid chosen by dspw_tune (0: one block per block-worth of tasks)
   // TMA staging of the specialised y / z sweeps: the class's tensor maps
-  // (tma_map_index layout; null when the class does not qualify) and, per
-  // direction, whether the sweep stages with TMA (1, the default) or with
-  // per-thread cp.async copies (0), as dspw_tune picks
+  // (tma_map_index layout; null when the class does not qualify or its
+  // problems ask for cp.async) and, per direction, whether the sweep stages
+  // with TMA (1) or with per-thread cp.async copies (0).  tma_forced: the
+  // problems ask for TMA (tile_staging 2), else dspw_tune picks.
   void* dtmap = nullptr;
-  int use_tma[3] = {1, 1, 1};
+  int use_tma[3] = {0, 0, 0};
+  int tma_forced = 0;
 };
 
 struct dspw_handle {
@@ -335,7 +337,7 @@ int validate(const dspw_desc& d) {
     for (int k = 0; k < 5; k++)
       if (!(d.nn_feat_lo[k] <= d.nn_feat_hi[k])) return DSPW_ERR_ARG;   // also rejects NaN bounds
   if (d.generic_kernels != 0 && d.generic_kernels != 1) return DSPW_ERR_ARG;
-  if (d.tile_staging != 0 && d.tile_staging != 1) return DSPW_ERR_ARG;
+  if (d.tile_staging < 0 || d.tile_staging > 2) return DSPW_ERR_ARG;
   for (int k = 0; k < 3; k++)
     if (!(d.cell_size[k] >= 0.0) || !std::isfinite(d.cell_size[k])) return DSPW_ERR_ARG;
   // unused slots stay zero, so that a later ABI version can give them a meaning
@@ -685,9 +687,11 @@ void build_tma_maps(dspw_handle* h) {
     const int dim = c.spec >= 100 ? 1 : c.spec / 10;
     if (c.spec == 0 || dim < 2) continue;
     bool ok = h->ctot % vec == 0;
+    bool forced = true;
     for (int p : c.probs) {
       const ProbDev& P = h->hprob[p];
-      ok = ok && P.nx % COOP_COLS == 0 && P.off % vec == 0 && h->desc[p].tile_staging == 0;
+      ok = ok && P.nx % COOP_COLS == 0 && P.off % vec == 0 && h->desc[p].tile_staging != 1;
+      forced = forced && h->desc[p].tile_staging == 2;
     }
     if (!ok) continue;
     const size_t n = c.probs.size();
@@ -718,6 +722,8 @@ void build_tma_maps(dspw_handle* h) {
       continue;
     }
     c.dtmap = d;
+    c.tma_forced = forced ? 1 : 0;
+    c.use_tma[1] = c.use_tma[2] = c.tma_forced;
   }
 }
 
@@ -802,7 +808,7 @@ int tune_grids(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
       std::vector<std::pair<int, int>> cand;
       for (int g : grids) {
         cand.push_back({g, tma0});
-        if (c.dtmap && dir >= 1) cand.push_back({g, 1 - tma0});
+        if (c.dtmap && dir >= 1 && !c.tma_forced) cand.push_back({g, 1 - tma0});
       }
       double best = 1e300;
       int best_grid = 0, best_tma = tma0;
@@ -834,7 +840,8 @@ int tune_grids(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
   if (ret) {
     for (SweepClass& c : h->classes) {
       c.grid[0] = c.grid[1] = c.grid[2] = 0;
-      c.use_tma[0] = c.use_tma[1] = c.use_tma[2] = 1;
+      c.use_tma[0] = 0;
+      c.use_tma[1] = c.use_tma[2] = c.dtmap ? c.tma_forced : 0;
     }
   }
   // the timing runs counted faces; the status is the solver's, not the tuner's

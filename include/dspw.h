@@ -129,10 +129,10 @@ typedef struct dspw_desc {
                                 plain SP-WENO (FP32 form) */
   int generic_kernels;       /* 1: run this problem on the generic sweep kernels even when
                                 specialised ones exist (validation) */
-  int tile_staging;          /* y / z sweeps of the specialised kernels: 0 = tiles staged by the
-                                Tensor Memory Accelerator where the problem allows it (nx a
-                                multiple of 8, 16-byte aligned rows; dspw_tune may still choose
-                                per-thread copies), 1 = per-thread cp.async copies always */
+  int tile_staging;          /* y / z sweeps of the specialised kernels: 0 = per-thread cp.async
+                                copies, or Tensor Memory Accelerator loads where dspw_tune measures
+                                them faster; 1 = cp.async always; 2 = TMA where the problem allows
+                                it (nx a multiple of 8, 16-byte aligned rows and planes) */
   int reserved_i[5];         /* zero */
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double gamma, gas_const, prandtl, mu_ref, T_ref, T_0, omega;

@@ -51,7 +51,7 @@ CASES = {
         [_bump(32, 40), _bump(64, 33)]),
     "euler3d": lambda pr, rc: (
         [make_desc(model="euler", flux="kepes_tecno4_roe", recon=rc, nx=16, ny=24, nz=35, precision=pr,
-                   network=net(), bc=["periodic", "periodic", "neumann", "wall", "wall", "periodic"])],
+                   network=net(), bc=["periodic", "periodic", "neumann", "wall", "wall", "neumann"])],
         [_bump(16, 24, 35)]),
 }
 
@@ -62,8 +62,8 @@ CASES = {
 def test_tma_staging_equals_cp_async(case, precision, recon):
     d1, p1 = CASES[case](precision, recon)
     d2, p2 = CASES[case](precision, recon)
-    a, sa = _run(d1, p1, 6, 0)
-    b, sb = _run(d2, p2, 6, 1)
+    a, sa = _run(d1, p1, 6, 2)   # TMA
+    b, sb = _run(d2, p2, 6, 1)   # cp.async
     for x, y in zip(a, b):
         assert np.array_equal(x, y), float(np.max(np.abs(x - y)))
     assert sa.code == sb.code == 0
@@ -76,7 +76,7 @@ def test_tma_staging_on_slabs_with_halo_faces():
     interior, outside its tensor map.  Both staging paths give the same bits."""
     from dspw.slabs import LocalSlabs
     out = []
-    for staging in (0, 1):
+    for staging in (2, 1):
         dom = make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=32, ny=96)
         dom.tile_staging = staging
         sl = LocalSlabs(dom, 3)
@@ -87,6 +87,8 @@ def test_tma_staging_on_slabs_with_halo_faces():
 
 
 def test_tuner_keeps_results_with_either_staging():
+    """dspw_tune times both stagings (tile_staging 0) and keeps the faster;
+    the state it leaves steps to the same bits as cp.async staging."""
     (d,), (p,), _ = W.kh(128, "fp32_bf16", "sp_weno_dl", net())
     s = Solver(d)
     s.upload_prim(p)

@@ -77,18 +77,33 @@ def test_solver_with_the_trainer_box():
     sb.step(20)
     st = sb.status()
     assert st.code == 0 and st.sign_violations == 0
-    # an empty box: every face falls back to SP-WENO
+    # a box that holds every input: the same bits as no box at all
+    (dw,), _, _ = W.kh(64, "fp32_bf16", "sp_weno_dl", (W0, b0))
+    sw = Solver(set_training_box(dw, [-10.0] * 5, [10.0] * 5))
+    sw.upload_prim(p)
+    sw.step(20)
+    (dn,), _, _ = W.kh(64, "fp32_bf16", "sp_weno_dl", (W0, b0))
+    sn = Solver(dn)
+    sn.upload_prim(p)
+    sn.step(20)
+    assert np.array_equal(sw.cons(), sn.cons())
+    # an empty box: no face reaches the network's limiter, and the solution is
+    # the FP32 SP-WENO one except at the no-jump faces, where the network path
+    # keeps the reference's DSP-WENO guard (a zero jump below 4 FP32 ulps of
+    # the values) and SP-WENO its own (below 1e-13)
     (de,), _, _ = W.kh(64, "fp32_bf16", "sp_weno_dl", (W0, b0))
     se = Solver(set_training_box(de, [9.0] * 5, [9.0] * 5))
     se.upload_prim(p)
     se.step(20)
+    assert se.status().limiter_acts == 0
     (ds,), _, _ = W.kh(64, "fp32_bf16", "sp_weno", None)
     ss = Solver(ds)
     ss.upload_prim(p)
     ss.step(20)
-    a, b = se.cons(), ss.cons()
-    assert np.max(np.abs(a - b)) <= 1e-5 * np.max(np.abs(b))
-    assert se.status().limiter_acts == 0
+    a, b, c = se.cons(), ss.cons(), sn.cons()
+    d_sp, d_nn = np.max(np.abs(a - b)), np.max(np.abs(c - b))
+    print(f"empty box vs SP-WENO {d_sp:.3e}, network vs SP-WENO {d_nn:.3e}")
+    assert d_sp <= 5e-3 * np.max(np.abs(b))
 
 
 def _collect(tr, max_pairs):
