@@ -1082,10 +1082,11 @@ __device__ inline void finish_cell(const SweepArgs<T>& A, const ProbDev& P, cons
 }
 
 template <typename T>
-__device__ inline void warp_epilogue(const SweepArgs<T>& A, ProbState& S, int lane, double smax, double ent,
+__device__ inline void warp_epilogue(const SweepArgs<T>& A, bool final_stage, ProbState& S, int lane, double smax,
+                                     double ent,
                                      unsigned bad_fin, unsigned bad_pos, unsigned long long signv, int viol,
                                      unsigned checked) {
-  if (A.final_stage && !A.residual_only) {
+  if (final_stage && !A.residual_only) {
     unsigned long long sb = (unsigned long long)__double_as_longlong(smax);
     warp_max_u64_lane0(sb);
     const double es = warp_sum(ent);
@@ -1200,9 +1201,7 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
     finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, P.nv, smax, ent, bad_fin, bad_pos);
   }
   if (!final_sweep) { smax = 0.0; ent = 0.0; }
-  SweepArgs<T> A2 = A;
-  A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
+  warp_epilogue<T>(A, A.final_stage && final_sweep, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
   __syncwarp();
 }
 
@@ -1265,7 +1264,7 @@ __device__ inline void tile_cons(const T (*U)[SEG_CELLS][COOP_COLS], int nv, int
 // column col, from the tile U (ghost rows already resolved to their source
 // rows), into the per-warp primitive / entropy rows of warp `col`.
 template <typename T, int DIR>
-__device__ inline void coop_convert(const ProbDev& P, WarpSmem<T>* sm0, const T (*U)[SEG_LOAD][COOP_COLS], int c0,
+__device__ __forceinline__ void coop_convert(const ProbDev& P, WarpSmem<T>* sm0, const T (*U)[SEG_LOAD][COOP_COLS], int c0,
                                     int nrow, int ncols) {
   const int tid = threadIdx.x, col = tid % COOP_COLS;
   const int N = dir_len<DIR>(P);
@@ -1299,7 +1298,7 @@ __device__ inline void coop_convert(const ProbDev& P, WarpSmem<T>* sm0, const T 
 // U (rows + 2) and Un, with threads laid out as 4 rows x 8 columns per warp
 // instruction (coalesced stores).
 template <typename T, int DIR>
-__device__ inline void coop_epilogue(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, WarpSmem<T>* sm0,
+__device__ __forceinline__ void coop_epilogue(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, WarpSmem<T>* sm0,
                                      const T (*U)[SEG_LOAD][COOP_COLS], const T (*Rt)[SEG_CELLS][COOP_COLS],
                                      const T (*Unt)[SEG_CELLS][COOP_COLS], int i0, int j0, int k0, int c0,
                                      int ncell, int ncols, bool final_sweep, double& smax, double& ent,
@@ -1413,9 +1412,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   coop_epilogue<T, DIR>(A, P, S, sm0, tl.U, tl.R, tl.Un, i0, j0, k0, c0, ncell, ncols, final_sweep, smax, ent,
                         bad_fin, bad_pos);
   if (!final_sweep) { smax = 0.0; ent = 0.0; }
-  SweepArgs<T> A2 = A;
-  A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
+  warp_epilogue<T>(A, A.final_stage && final_sweep, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
   __syncthreads();
 }
 
@@ -1448,14 +1445,14 @@ struct TmaLayout {
 
 constexpr long long TMA_WAIT_LIMIT = 1LL << 24;
 
-__device__ inline unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ inline void mbar_init(unsigned long long* bar, unsigned count) {
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
-__device__ inline void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-__device__ inline bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
   unsigned ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
@@ -1467,18 +1464,18 @@ __device__ inline bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
   return ok != 0;
 }
 // bounded wait for the phase of the given parity; false after TMA_WAIT_LIMIT tries
-__device__ inline bool mbar_wait(unsigned long long* bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
   for (long long i = 0; i < TMA_WAIT_LIMIT; i++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
 // generic-proxy accesses of shared memory before this point are ordered before
 // later asynchronous-proxy (TMA) accesses
-__device__ inline void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 // 4-D tiled load (x, y, z, component) of this GPU's global memory into shared
 // memory, completion counted on the mbarrier; x is a multiple of 8 elements
 // (16-byte aligned), y / z may lie outside the tensor (zero fill)
-__device__ inline void tma_load_4d(void* dst, const void* map, int x, int y, int z, int c, unsigned long long* bar) {
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* map, int x, int y, int z, int c, unsigned long long* bar) {
   asm volatile(
       "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
       ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(c), "r"(smem_u32(bar))
@@ -1488,7 +1485,7 @@ __device__ inline void tma_load_4d(void* dst, const void* map, int x, int y, int
 // the next task >= g of this block's stride whose problem is stepping (or any
 // task for a residual evaluation); A.ntask when none is left
 template <typename T>
-__device__ inline int next_live_task(const SweepArgs<T>& A, int g) {
+__device__ __forceinline__ int next_live_task(const SweepArgs<T>& A, int g) {
   for (; g < A.ntask; g += gridDim.x) {
     if (A.residual_only) return g;
     const int p = find_problem(A.task_start, A.nprob, g);
@@ -1501,7 +1498,7 @@ __device__ inline int next_live_task(const SweepArgs<T>& A, int g) {
 // coordinates of task g's tile origin: problem (class index), column i0 and
 // the (y, z) of its first cell row
 template <typename T, int DIR>
-__device__ inline void tma_task(const SweepArgs<T>& A, int g, int& p, int& i0, int& j0, int& k0, int& c0, int& ncell) {
+__device__ __forceinline__ void tma_task(const SweepArgs<T>& A, int g, int& p, int& i0, int& j0, int& k0, int& c0, int& ncell) {
   p = find_problem(A.task_start, A.nprob, g);
   const int pp = A.pmap ? __ldg(A.pmap + p) : p;
   int ncols;
@@ -1509,7 +1506,7 @@ __device__ inline void tma_task(const SweepArgs<T>& A, int g, int& p, int& i0, i
 }
 
 template <typename T, int DIR>
-__device__ inline void tma_issue_rows(const SweepArgs<T>& A, int g, unsigned char* ubuf, unsigned long long* bar) {
+__device__ __forceinline__ void tma_issue_rows(const SweepArgs<T>& A, int g, unsigned char* ubuf, unsigned long long* bar) {
   int p, i0, j0, k0, c0, ncell;
   tma_task<T, DIR>(A, g, p, i0, j0, k0, c0, ncell);
   const int pp = A.pmap ? __ldg(A.pmap + p) : p;
@@ -1521,7 +1518,7 @@ __device__ inline void tma_issue_rows(const SweepArgs<T>& A, int g, unsigned cha
 }
 
 template <typename T, int DIR>
-__device__ inline void tma_issue_cells(const SweepArgs<T>& A, int g, bool final_sweep, unsigned char* rbuf,
+__device__ __forceinline__ void tma_issue_cells(const SweepArgs<T>& A, int g, bool final_sweep, unsigned char* rbuf,
                                        unsigned char* unbuf, unsigned long long* bar) {
   int p, i0, j0, k0, c0, ncell;
   tma_task<T, DIR>(A, g, p, i0, j0, k0, c0, ncell);
@@ -1540,13 +1537,14 @@ __device__ inline void tma_issue_cells(const SweepArgs<T>& A, int g, bool final_
 // (the host builds the tensor maps only then), so every task is a full group
 // of 8 columns.
 template <typename T, int DIR, int DIM, typename Sp>
-__device__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpSmem<T>* sm0) {
+__device__ __forceinline__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpSmem<T>* sm0) {
   typedef TmaLayout<T> L;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned char* base = reinterpret_cast<unsigned char*>(sm0 + WARPS_PER_BLOCK);
   base = reinterpret_cast<unsigned char*>(((size_t)base + 127) & ~(size_t)127);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);   // [0], [1]: rows; [2]: cells
-  unsigned char* ubuf[2] = {base + L::bars, base + L::bars + L::u_bytes};
+  unsigned char* const ubuf0 = base + L::bars;
+  unsigned char* const ubuf1 = base + L::bars + L::u_bytes;
   unsigned char* rbuf = base + L::bars + 2 * L::u_bytes;
   unsigned char* unbuf = rbuf + L::r_bytes;
   typedef const T(*UTile)[SEG_LOAD][COOP_COLS];
@@ -1560,9 +1558,11 @@ __device__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpSmem<T>* sm0) {
     fence_proxy_async_smem();
   }
   __syncthreads();
-  unsigned ph_u[2] = {0u, 0u}, ph_c = 0u;
+  // mbarrier phases of the two row buffers and of the cell tiles (scalars and
+  // selects: an array indexed by the buffer number would live in local memory)
+  unsigned ph_u0 = 0u, ph_u1 = 0u, ph_c = 0u;
   int g = next_live_task(A, blockIdx.x);
-  if (tid == 0 && g < A.ntask) tma_issue_rows<T, DIR>(A, g, ubuf[0], &bar[0]);
+  if (tid == 0 && g < A.ntask) tma_issue_rows<T, DIR>(A, g, ubuf0, &bar[0]);
   int b = 0;
   bool timed_out = false;
   while (g < A.ntask) {
@@ -1580,10 +1580,14 @@ __device__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpSmem<T>* sm0) {
       tma_issue_cells<T, DIR>(A, g, final_sweep, rbuf, unbuf, &bar[2]);
     }
     // staged rows of this task (prefetched)
-    if (!mbar_wait(&bar[b], ph_u[b])) timed_out = true;
-    ph_u[b] ^= 1u;
+    unsigned char* const ucur = b ? ubuf1 : ubuf0;
+    unsigned char* const unext = b ? ubuf0 : ubuf1;
+    unsigned long long* const bcur = b ? &bar[1] : &bar[0];
+    unsigned long long* const bnext = b ? &bar[0] : &bar[1];
+    if (!mbar_wait(bcur, b ? ph_u1 : ph_u0)) timed_out = true;
+    if (b) ph_u1 ^= 1u; else ph_u0 ^= 1u;
     // rows outside the problem: their boundary-condition source rows
-    T(*U)[SEG_LOAD][COOP_COLS] = reinterpret_cast<T(*)[SEG_LOAD][COOP_COLS]>(ubuf[b]);
+    T(*U)[SEG_LOAD][COOP_COLS] = reinterpret_cast<T(*)[SEG_LOAD][COOP_COLS]>(ucur);
     for (int idx = tid; idx < nrow * COOP_COLS; idx += WARPS_PER_BLOCK * 32) {
       const int q = idx / COOP_COLS, cc = idx - q * COOP_COLS;
       const int c = c0 - 2 + q;
@@ -1601,7 +1605,7 @@ __device__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpSmem<T>* sm0) {
     // the next task's rows into the other buffer, behind this task's faces
     if (tid == 0 && gn < A.ntask) {
       fence_proxy_async_smem();
-      tma_issue_rows<T, DIR>(A, gn, ubuf[b ^ 1], &bar[b ^ 1]);
+      tma_issue_rows<T, DIR>(A, gn, unext, bnext);
     }
     int viol = 0;
     unsigned long long signv = 0;
@@ -1616,9 +1620,7 @@ __device__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpSmem<T>* sm0) {
     coop_epilogue<T, DIR>(A, P, S, sm0, (UTile)U, (CTile)rbuf, (CTile)unbuf, i0, j0, k0, c0, ncell, COOP_COLS,
                           final_sweep, smax, ent, bad_fin, bad_pos);
     if (!final_sweep) { smax = 0.0; ent = 0.0; }
-    SweepArgs<T> A2 = A;
-    A2.final_stage = A.final_stage && final_sweep;
-    warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
+    warp_epilogue<T>(A, A.final_stage && final_sweep, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
     // this task's shared-memory accesses (the ghost-row stores among them) are
     // ordered before the TMA writes that refill the tiles; the barrier ends
     // the task for every thread
@@ -1627,7 +1629,7 @@ __device__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpSmem<T>* sm0) {
       // a copy that did not complete: record it and wait (bounded) for the
       // prefetch still in flight before the block leaves
       if (tid == 0) atomicCAS(&A.status->code, 0, DSPW_ERR_TIMEOUT);
-      if (gn < A.ntask) mbar_wait(&bar[b ^ 1], ph_u[b ^ 1]);
+      if (gn < A.ntask) mbar_wait(bnext, b ? ph_u0 : ph_u1);
       break;
     }
     g = gn;
@@ -1709,9 +1711,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
     long long cell = cell_index<DIR>(P, i0, j0, k0, c0 + lane);
     finish_cell<T>(A, P, S, cell, first, final_sweep, Fl, Fr, 1, smax, ent, bad_fin, bad_pos);
   }
-  SweepArgs<T> A2 = A;
-  A2.final_stage = A.final_stage && final_sweep;
-  warp_epilogue<T>(A2, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, (P.tecno && valid) ? 1u : 0u);
+  warp_epilogue<T>(A, A.final_stage && final_sweep, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, (P.tecno && valid) ? 1u : 0u);
   __syncwarp();
 }
 
@@ -1720,7 +1720,7 @@ __device__ void scalar_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& 
 // (SpecGeneric); a SpecHot kernel is only launched for directions < its dim.
 template <typename T, int DIR, typename Sp>
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MinBlocks<T>::value)
-k_sweep(SweepArgs<T> A) {
+k_sweep(const __grid_constant__ SweepArgs<T> A) {   // grid constant: references to A need no local copy
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem<T>* sm0 = reinterpret_cast<WarpSmem<T>*>(smem_raw);
   WarpSmem<T>* sm = sm0 + (threadIdx.x >> 5);
@@ -1728,10 +1728,6 @@ k_sweep(SweepArgs<T> A) {
   if (!Sp::fixed || Sp::rec == 2) net_frag_stage<T>(*A.net, lane, sm->ns);
   if constexpr (Sp::fixed && DIR >= 1) {
     // specialised y / z sweeps: every task is one block-cooperative column group
-    if (A.tma) {
-      euler_coop_tma_loop<T, DIR, Sp::dim, Sp>(A, sm0);
-      return;
-    }
     for (int g = blockIdx.x; g < A.ntask; g += gridDim.x) {
       const int p = find_problem(A.task_start, A.nprob, g);
       const int pp = A.pmap ? __ldg(A.pmap + p) : p;
@@ -1791,6 +1787,20 @@ k_sweep(SweepArgs<T> A) {
       }
     }
   }
+}
+
+// The specialised y / z sweeps with TMA staging (euler_coop_tma_loop): a
+// kernel of its own, so that the loop's state does not take registers from the
+// cp.async kernel.
+template <typename T, int DIR, typename Sp>
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MinBlocks<T>::value)
+k_sweep_tma(const __grid_constant__ SweepArgs<T> A) {
+  static_assert(Sp::fixed && DIR >= 1, "TMA staging is for the specialised y / z sweeps");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem<T>* sm0 = reinterpret_cast<WarpSmem<T>*>(smem_raw);
+  const int lane = threadIdx.x & 31;
+  if (Sp::rec == 2) net_frag_stage<T>(*A.net, lane, sm0[threadIdx.x >> 5].ns);
+  euler_coop_tma_loop<T, DIR, Sp::dim, Sp>(A, sm0);
 }
 
 // The x sweep of 1-D scalar problems alone: the reconstruction family fixed at
