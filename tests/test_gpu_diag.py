@@ -166,7 +166,8 @@ def test_diagnostics_and_globals_are_bitwise_reproducible():
         descs, prims = [dk], [pk]
         rng = np.random.default_rng(7)
         for nx in (100, 257, 3001, 5, 640):
-            descs.append(make_desc(model="burgers", flux="bur_tecno4", recon="sp_weno", nx=nx, x=(-np.pi, np.pi)))
+            descs.append(make_desc(model="burgers", flux="bur_tecno4", recon="sp_weno", nx=nx, x=(-np.pi, np.pi),
+                                   final_time=1e9))
             prims.append(W.burgers_fourier(nx, rng))
         s = Solver(descs)
         for k, p in enumerate(prims):
