@@ -272,49 +272,6 @@ DSPW_HD void nn_features(T u0, T u1, T u2, T u3, T feat[5], T vx[5], T vy[5]) {
   T x2 = T(1.0 / 8.0) * (T(1) + psi_p) - g2 * psi_p;
   T y2 = T(1.0 / 8.0) * (T(1) + psi_m) - g1 * psi_m;
   const T e = T(1.0 / 8.0), t = T(-3.0 / 8.0), o = T(-1.0 / 8.0);
-  if constexpr (sizeof(T) == 4) {
-    // FP32 form: the same vertex choice as the tree below, written as selects
-    // so that the lanes of a warp, which fall into different cases, run one
-    // path.  Cases, in the tree's order: A (tm, tp > 1), B (tm > 1 > tp) and
-    // C (tp > 1 > tm) with their sub-cases by psi_p < -1 and x1 / y2 < g2, D
-    // (tm = 1 < tp), E (tp = 1 < tm), F (the rest); "= 1" within thr.
-    const T dm = tm - T(1.0), dp = tp - T(1.0);
-    const bool cA = dm > thr && dp > thr;
-    const bool cB = !cA && dm > thr && dp < -thr;
-    const bool cC = !cA && !cB && dm < -thr && dp > thr;
-    const bool cD = !cA && !cB && !cC && m::abs(dm) < thr && dp > thr;
-    const bool cE = !cA && !cB && !cC && !cD && m::abs(dp) < thr && dm > thr;
-    const bool q = psi_p < T(-1.0);
-    const bool lx = x1 < g2, ly = y2 < g2;
-    // sub-cases of B and C
-    const bool n5 = (cB && q && lx) || (cC && !q && ly);          // (nx, ny) at every vertex
-    const bool bb = cB && q && !lx, ba = cB && !q && ly, bz = cB && !q && !ly;
-    const bool ca = cC && q && lx, cb = cC && q && !lx, cz = cC && !q && !ly;
-    const bool zero4 = ba || ca;                                      // (.., 0) fifth vertex
-    const T pm2 = psi_m * psi_m;
-    const T nx = (pm2 + psi_m) * m::div(T(1), T(8) * (pm2 + T(1)));
-    const T ny = T(1.0 / 8.0) * (T(1) + psi_m) - nx * psi_m;
-    const T third = T(1.0 / 3.0);
-    const T cxb = (T(2) * g2 + x1) * third, cyb = (T(2) * g1 + y2) * third;
-    const T cxc = (T(2) * g1 + x1) * third, cyc = (T(2) * g2 + y2) * third;
-    const bool cst = !(cB || cC);                                     // A, D, E, F
-    const bool ef = cst && !cA && !cD;                                // E, F
-    // vertex x
-    vx[0] = cst ? e : (n5 ? nx : ((cb || cz) ? g1 : g2));
-    vx[1] = cst ? e : (n5 ? nx : ((bb || cz) ? x1 : g1));
-    vx[2] = cst ? (ef ? t : e) : (n5 ? nx : (cz ? g1 : g2));
-    vx[3] = cst ? (ef ? t : e) : (n5 ? nx : (bb ? cxb : (cz ? cxc : (cb ? x1 : g1))));
-    vx[4] = cst ? (ef ? o : e) : (n5 ? nx : (bb ? cxb : (cz ? cxc : (zero4 ? T(0) : (bz ? x2 : g2)))));
-    // vertex y
-    const bool fF = ef && !cE;
-    vy[0] = cst ? (cD ? t : e) : (n5 ? ny : ((cb || cz) ? g2 : g1));
-    vy[1] = cst ? (fF ? t : e) : (n5 ? ny : (cz ? g2 : g1));
-    vy[2] = cst ? (fF ? t : e) : (n5 ? ny : ((bb || cz) ? y2 : g2));
-    vy[3] = cst ? (cD ? t : e) : (n5 ? ny : (bb ? cyb : (cz ? cyc : (bz ? y2 : (cb ? g1 : g2)))));
-    vy[4] = cst ? ((cD || fF) ? o : e) : (n5 ? ny : (bb ? cyb : (cz ? cyc : (zero4 ? T(0) : (cb ? y1 : g2)))));
-    (void)ca;
-    return;
-  }
 #define DSPW_SET5(a, v0, v1, v2, v3, v4) { a[0] = v0; a[1] = v1; a[2] = v2; a[3] = v3; a[4] = v4; }
   if ((tm - T(1.0)) > thr && (tp - T(1.0)) > thr) {
     DSPW_SET5(vx, e, e, e, e, e) DSPW_SET5(vy, e, e, e, e, e)
