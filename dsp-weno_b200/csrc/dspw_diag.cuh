@@ -176,26 +176,28 @@ __device__ inline void block_range_sums(const long long* start, int nprob, doubl
   if (pend >= 0) block_store(sum, part, pend);
 }
 
-// fold the partial rows of one launch into each problem's accumulator, in
-// block order: one warp per problem (T: the state type of the launch's unit)
+// fold the partial rows of one launch into each problem's accumulator in a
+// fixed order: one block of 256 threads per problem, thread t adds rows
+// b0 + t, b0 + t + 256, ..., then the block's fixed-order sum
 template <typename T>
-__global__ void k_diag_fold(const long long* start, int nprob, const double* part, int nblocks, DiagAcc* acc) {
+__global__ void __launch_bounds__(256) k_diag_fold(const long long* start, int nprob, const double* part, int nblocks,
+                                                   DiagAcc* acc) {
   const int p = blockIdx.x;
   if (p >= nprob) return;
   const long long total = start[nprob];
   const long long chunk = diag_chunk(total, nblocks);
-  if (start[p + 1] <= start[p]) return;
+  if (start[p + 1] <= start[p]) return;   // block-uniform
   const int b0 = (int)(start[p] / chunk), b1 = (int)((start[p + 1] - 1) / chunk);
   double s[DIAG_NACC];
 #pragma unroll
   for (int k = 0; k < DIAG_NACC; k++) s[k] = 0.0;
-  for (int b = b0 + (int)threadIdx.x; b <= b1; b += 32)
+  for (int b = b0 + (int)threadIdx.x; b <= b1; b += blockDim.x)
 #pragma unroll
     for (int k = 0; k < DIAG_NACC; k++) s[k] += part[((long long)b + p) * DIAG_NACC + k];
+  block_sum_fixed(s);
+  if (threadIdx.x == 0) {
 #pragma unroll
-  for (int k = 0; k < DIAG_NACC; k++) {
-    const double x = warp_sum(s[k]);
-    if (threadIdx.x == 0) acc[p].v[k] += x;
+    for (int k = 0; k < DIAG_NACC; k++) acc[p].v[k] += s[k];
   }
 }
 
