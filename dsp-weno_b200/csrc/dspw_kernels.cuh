@@ -730,8 +730,11 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>*
   // below which the scaled differences of the features are rounding noise.
   float mag = fmaxf(fabsf(u1), fabsf(u2));
   bool guard = fabsf(u2 - u1) < fmaxf(1e-15f, 4.0f * 1.1920929e-07f * mag);
-  float feat[5], vx[5], vy[5];
-  nn_features<float>(u0, u1, u2, u3, feat, vx, vy);
+  // the inputs before the network call, the vertices after it: the code in
+  // front of the warp-wide MMA is free of lane-dependent branches, and the ten
+  // vertices are not held across the call
+  float feat[5], tm, tp, md;
+  nn_inputs<float>(u0, u1, u2, u3, feat, tm, tp, md);
   bool inbox = true;
   if (NP.use_box) {
 #pragma unroll
@@ -746,6 +749,8 @@ __device__ inline int dsp_weno_warp<float>(const NetParams& NP, WarpSmem<float>*
   if (!valid) return 0;
   if (guard) { l = 0.f; r = 0.f; return 0; }
   if (inbox) {
+    float vx[5], vy[5];
+    nn_vertices<float>(tm, tp, md, vx, vy);
     nn_finish<float>(lg, vx, vy, u0, u1, u2, u3, l, r);
     // non-finite features or vertices (the only way to a non-finite
     // reconstruction of a finite stencil) fall back to SP-WENO below; so does

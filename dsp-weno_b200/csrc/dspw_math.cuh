@@ -229,10 +229,10 @@ struct NetParams {
   int use_box;
 };
 
-// features and vertices: scale (neural_network.cc:300-313), theta, deltas and
-// compute_vertices with vertex_mode 2 / permutation 2 (:135-260)
+// The network's inputs: scale (neural_network.cc:300-313), theta and deltas;
+// tm, tp and the largest delta md feed the vertices (nn_vertices)
 template <typename T>
-DSPW_HD void nn_features(T u0, T u1, T u2, T u3, T feat[5], T vx[5], T vy[5]) {
+DSPW_HD void nn_inputs(T u0, T u1, T u2, T u3, T feat[5], T& tm_out, T& tp_out, T& md_out) {
   typedef Mth<T> m;
   T mx = T(1.0);
   mx = m::max(mx, m::abs(u0)); mx = m::max(mx, m::abs(u1));
@@ -254,7 +254,16 @@ DSPW_HD void nn_features(T u0, T u1, T u2, T u3, T feat[5], T vx[5], T vy[5]) {
   T md = m::max(m::max(d1, d2), d3);
   feat[0] = m::tanh(tm); feat[1] = m::tanh(tp);
   feat[2] = d1; feat[3] = d2; feat[4] = d3;
+  tm_out = tm;
+  tp_out = tp;
+  md_out = md;
+}
 
+// The feasible-region vertices of compute_vertices with vertex_mode 2 /
+// permutation 2 (neural_network.cc:135-260) from tm, tp and md
+template <typename T>
+DSPW_HD void nn_vertices(T tm, T tp, T md, T vx[5], T vy[5]) {
+  typedef Mth<T> m;
   const T thr = T(1e-8);
   T psi_p, psi_m;
   if constexpr (sizeof(T) == 4) {
@@ -311,6 +320,15 @@ DSPW_HD void nn_features(T u0, T u1, T u2, T u3, T feat[5], T vx[5], T vy[5]) {
     DSPW_SET5(vx, e, e, t, t, o) DSPW_SET5(vy, e, t, t, e, o)
   }
 #undef DSPW_SET5
+}
+
+// inputs and vertices of one stencil (the reference's forward computes both
+// before the network)
+template <typename T>
+DSPW_HD void nn_features(T u0, T u1, T u2, T u3, T feat[5], T vx[5], T vy[5]) {
+  T tm, tp, md;
+  nn_inputs<T>(u0, u1, u2, u3, feat, tm, tp, md);
+  nn_vertices<T>(tm, tp, md, vx, vy);
 }
 
 // softmax (neural_network.cc:276-295) and the vertex combination / weights /
