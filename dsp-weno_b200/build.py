@@ -79,6 +79,21 @@ def build_cli(lib: Path) -> Path:
     return CLI
 
 
+NETBENCH = PKG / "libdspw_netbench.so"
+
+
+def build_netbench(verbose: bool) -> Path:
+    """The network measurement kernels (csrc/dspw_netbench.cu: the sweep
+    kernels' mma.sync form and a tcgen05 form), a library of their own."""
+    obj = compile_unit("dspw_netbench.cu", ["--fmad=true", "-ftz=true"], verbose)
+    if not NETBENCH.exists() or NETBENCH.stat().st_mtime < obj.stat().st_mtime:
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(NETBENCH), str(obj), "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stderr}")
+    return NETBENCH
+
+
 def build(verbose: bool = False) -> Path:
     BUILD.mkdir(parents=True, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
@@ -92,6 +107,7 @@ def build(verbose: bool = False) -> Path:
             raise RuntimeError(f"link failed:\n{r.stderr}")
     if LIB == PKG / "libdspw.so":
         build_cli(LIB)
+        build_netbench(verbose)
     return LIB
 
 
