@@ -163,6 +163,12 @@ struct SweepClass {
   void* dtmap = nullptr;
   int use_tma[3] = {0, 0, 0};
   int tma_forced = 0;
+  // narrow tiles of the specialised y / z sweeps (k_sweep_narrow: 4-column
+  // blocks, cp.async staging) per direction; the direction's task list then
+  // counts groups of 4 columns.  narrow_forced: the problems ask for them
+  // (tile_staging 3), else dspw_tune picks.
+  int narrow[3] = {0, 0, 0};
+  int narrow_forced = 0;
 };
 
 struct dspw_handle {
@@ -337,7 +343,7 @@ int validate(const dspw_desc& d) {
     for (int k = 0; k < 5; k++)
       if (!(d.nn_feat_lo[k] <= d.nn_feat_hi[k])) return DSPW_ERR_ARG;   // also rejects NaN bounds
   if (d.generic_kernels != 0 && d.generic_kernels != 1) return DSPW_ERR_ARG;
-  if (d.tile_staging < 0 || d.tile_staging > 2) return DSPW_ERR_ARG;
+  if (d.tile_staging < 0 || d.tile_staging > 3) return DSPW_ERR_ARG;
   for (int k = 0; k < 3; k++)
     if (!(d.cell_size[k] >= 0.0) || !std::isfinite(d.cell_size[k])) return DSPW_ERR_ARG;
   // unused slots stay zero, so that a later ABI version can give them a meaning
@@ -463,15 +469,32 @@ int spec_of(const ProbDev& P, const dspw_desc& d) {
 }
 
 // Tasks of one problem in direction dir: warp tasks (one line segment each),
-// or, for the y / z sweeps of a specialised batch, block tasks of 8 adjacent
-// columns (decode_group).
-long long tasks_for(const ProbDev& P, int dir, bool groups) {
+// or, for the y / z sweeps of a specialised batch, block tasks of `cols`
+// adjacent columns (decode_group: 8, or 4 for the narrow tiles).
+long long tasks_for(const ProbDev& P, int dir, bool groups, int cols = WARPS_PER_BLOCK) {
   if (dir >= P.dim) return 0;
   int N[3] = {P.nx, P.ny, P.nz};
   long long nseg = (N[dir] + SEG_CELLS - 1) / SEG_CELLS;
   long long other = (long long)P.nx * P.ny * P.nz / N[dir];
-  if (groups && dir >= 1) return nseg * (other / P.nx) * ((P.nx + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK);
+  if (groups && dir >= 1) return nseg * (other / P.nx) * ((P.nx + cols - 1) / cols);
   return nseg * other;
+}
+
+// The task list (prefix sums over the class's problems) of one direction, for
+// the class's current tile width; uploaded when the device copy exists.
+int class_tasks(SweepClass& c, const std::vector<ProbDev>& prob, int dir) {
+  const int cols = (c.spec != 0 && dir >= 1 && c.narrow[dir]) ? NARROW_COLS : WARPS_PER_BLOCK;
+  std::vector<int> ts(1, 0);
+  for (int p : c.probs) {
+    const long long nt = (long long)ts.back() + tasks_for(prob[p], dir, c.spec != 0, cols);
+    if (nt > (1LL << 30)) return DSPW_ERR_ARG;
+    ts.push_back((int)nt);
+  }
+  c.task_start[dir] = ts;
+  if (c.dtask[dir] &&
+      cudaMemcpy(c.dtask[dir], ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return DSPW_ERR_CUDA;
+  return DSPW_OK;
 }
 
 void* buf(dspw_handle* h, int which) {
@@ -646,7 +669,8 @@ cudaError_t launch_class_sweep(dspw_handle* h, SweepArgs<T> a, const SweepClass&
   a.nprob = (int)c.probs.size();
   a.ntask = c.task_start[dir].back();
   a.tmaps = c.dtmap;
-  a.tma = (c.dtmap && dir >= 1 && c.use_tma[dir]) ? 1 : 0;
+  a.narrow = (c.spec != 0 && dir >= 1 && c.narrow[dir]) ? 1 : 0;
+  a.tma = (!a.narrow && c.dtmap && dir >= 1 && c.use_tma[dir]) ? 1 : 0;
   int grid = c.grid[dir] ? c.grid[dir] : default_grid(c, dir);
   return Launch<T>::sweep(dir, a, grid, h->stream, c.spec);
 }
@@ -690,7 +714,8 @@ void build_tma_maps(dspw_handle* h) {
     bool forced = true;
     for (int p : c.probs) {
       const ProbDev& P = h->hprob[p];
-      ok = ok && P.nx % COOP_COLS == 0 && P.off % vec == 0 && h->desc[p].tile_staging != 1;
+      ok = ok && P.nx % COOP_COLS == 0 && P.off % vec == 0 && h->desc[p].tile_staging != 1 &&
+           h->desc[p].tile_staging != 3;
       forced = forced && h->desc[p].tile_staging == 2;
     }
     if (!ok) continue;
@@ -777,10 +802,12 @@ int enqueue_stage(dspw_handle* h, int rk, int residual_only) {
   return DSPW_OK;
 }
 
-// Launch-grid autotuner: for every kernel class and direction, time the sweep
+// Launch autotuner: for every kernel class and direction, time the sweep
 // (residual evaluation of the current state, which writes only the residual
 // buffer) with its default grid and with persistent grids of 1, 2 and 4 times
-// the resident blocks of the whole GPU, and keep the fastest.
+// the resident blocks of the whole GPU; the specialised y / z sweeps also with
+// both tile widths (8 columns, 4 columns) and, for 8 columns with tensor maps,
+// both stagings (cp.async, TMA).  The fastest candidate is kept.
 template <typename T>
 int tune_grids(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
   int dev = 0, nsm = 0;
@@ -797,43 +824,60 @@ int tune_grids(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
   for (SweepClass& c : h->classes) {
     for (int dir = 0; dir < h->maxdim; dir++) {
       if (c.task_start[dir].back() == 0) continue;
-      const int g0 = default_grid(c, dir);
-      const int bpsm = Launch<T>::sweep_blocks_per_sm(dir, c.spec);
-      std::vector<int> grids = {0};
-      for (int k : {1, 2, 4})
-        if (bpsm > 0 && (long long)nsm * bpsm * k < g0) grids.push_back(nsm * bpsm * k);
-      // candidates (grid, staging): the y / z sweeps of a class with tensor
-      // maps also try per-thread cp.async staging instead of TMA
-      const int tma0 = c.use_tma[dir];
-      std::vector<std::pair<int, int>> cand;
-      for (int g : grids) {
-        cand.push_back({g, tma0});
-        if (c.dtmap && dir >= 1 && !c.tma_forced) cand.push_back({g, 1 - tma0});
-      }
+      // tile widths: the specialised y / z sweeps of a 2-D / 3-D class also
+      // try the narrow tiles (4 columns, cp.async), unless the problems fix
+      // the staging
+      const int tma0 = c.use_tma[dir], nw0 = c.narrow[dir];
+      std::vector<int> widths = {nw0};
+      if (c.spec != 0 && c.spec < 100 && dir >= 1 && !c.tma_forced && !c.narrow_forced) widths.push_back(1 - nw0);
       double best = 1e300;
-      int best_grid = 0, best_tma = tma0;
-      for (auto [g, tm] : cand) {
-        c.grid[dir] = g;
-        c.use_tma[dir] = tm;
-        std::vector<float> t(reps);
-        for (int r = 0; r < reps && ret == DSPW_OK; r++) {
-          if (cudaEventRecord(e0, h->stream) != cudaSuccess ||
-              launch_class_sweep<T>(h, a, c, dir) != cudaSuccess ||
-              cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-              cudaEventElapsedTime(&t[r], e0, e1) != cudaSuccess)
-            ret = DSPW_ERR_CUDA;
+      int best_grid = 0, best_tma = tma0, best_nw = nw0;
+      for (int nw : widths) {
+        if (c.narrow[dir] != nw) {
+          c.narrow[dir] = nw;
+          if (class_tasks(c, h->hprob, dir) != DSPW_OK) { ret = DSPW_ERR_CUDA; break; }
+        }
+        const int g0 = default_grid(c, dir);
+        const int bpsm = Launch<T>::sweep_blocks_per_sm(dir, c.spec, nw);
+        std::vector<int> grids = {0};
+        for (int k : {1, 2, 4})
+          if (bpsm > 0 && (long long)nsm * bpsm * k < g0) grids.push_back(nsm * bpsm * k);
+        // candidates (grid, staging): the 8-column y / z sweeps of a class
+        // with tensor maps also try the other staging (TMA / cp.async)
+        std::vector<std::pair<int, int>> cand;
+        for (int g : grids) {
+          cand.push_back({g, nw ? 0 : tma0});
+          if (!nw && c.dtmap && dir >= 1 && !c.tma_forced) cand.push_back({g, 1 - tma0});
+        }
+        for (auto [g, tm] : cand) {
+          c.grid[dir] = g;
+          c.use_tma[dir] = tm;
+          std::vector<float> t(reps);
+          for (int r = 0; r < reps && ret == DSPW_OK; r++) {
+            if (cudaEventRecord(e0, h->stream) != cudaSuccess ||
+                launch_class_sweep<T>(h, a, c, dir) != cudaSuccess ||
+                cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&t[r], e0, e1) != cudaSuccess)
+              ret = DSPW_ERR_CUDA;
+          }
+          if (ret) break;
+          std::sort(t.begin(), t.end());
+          const double med = t[reps / 2];
+          if (g == 0 && tm == tma0 && nw == nw0) tot_before += med;
+          if (med < best) { best = med; best_grid = g; best_tma = tm; best_nw = nw; }
         }
         if (ret) break;
-        std::sort(t.begin(), t.end());
-        const double med = t[reps / 2];
-        if (g == 0 && tm == tma0) tot_before += med;
-        if (med < best) { best = med; best_grid = g; best_tma = tm; }
+      }
+      if (ret) break;
+      if (c.narrow[dir] != best_nw) {
+        c.narrow[dir] = best_nw;
+        if (class_tasks(c, h->hprob, dir) != DSPW_OK) { ret = DSPW_ERR_CUDA; break; }
       }
       c.grid[dir] = best_grid;
       c.use_tma[dir] = best_tma;
-      if (ret) break;
       tot_after += best;
     }
+    if (ret) break;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -842,6 +886,8 @@ int tune_grids(dspw_handle* h, int reps, double* before_ms, double* after_ms) {
       c.grid[0] = c.grid[1] = c.grid[2] = 0;
       c.use_tma[0] = 0;
       c.use_tma[1] = c.use_tma[2] = c.dtmap ? c.tma_forced : 0;
+      c.narrow[1] = c.narrow[2] = c.narrow_forced;
+      for (int dir = 1; dir < 3; dir++) class_tasks(c, h->hprob, dir);
     }
   }
   // the timing runs counted faces; the status is the solver's, not the tuner's
@@ -1115,14 +1161,13 @@ int dspw_create_batch(const dspw_desc* descs, int nprob, dspw_handle** out) {
     c->probs.push_back(p);
   }
   for (SweepClass& c : h->classes) {
-    for (int dir = 0; dir < 3; dir++) {
-      c.task_start[dir].push_back(0);
-      for (int p : c.probs) {
-        long long nt = (long long)c.task_start[dir].back() + tasks_for(h->hprob[p], dir, c.spec != 0);
-        if (nt > (1LL << 30)) { delete h; return DSPW_ERR_ARG; }
-        c.task_start[dir].push_back((int)nt);
-      }
-    }
+    // narrow tiles when every problem of a specialised 2-D / 3-D class asks for them
+    bool narrow = c.spec != 0 && c.spec < 100;
+    for (int p : c.probs) narrow = narrow && descs[p].tile_staging == 3 && h->hprob[p].dim >= 2;
+    c.narrow_forced = narrow ? 1 : 0;
+    c.narrow[1] = c.narrow[2] = c.narrow_forced;
+    for (int dir = 0; dir < 3; dir++)
+      if (class_tasks(c, h->hprob, dir) != DSPW_OK) { delete h; return DSPW_ERR_ARG; }
   }
   // network parameters (shared by the batch; taken from the first DL problem)
   const dspw_desc* dnet = &descs[0];

@@ -144,6 +144,7 @@ struct SweepArgs {
   const void* tmaps;
   int tma;
   int tma_in;              // 0: U^n, 1: Ua, 2: Ub
+  int narrow;              // 1: the specialised y / z sweep runs k_sweep_narrow (4-column tiles)
 };
 
 // Tensor maps of the TMA staging, per (class problem, direction 1 / 2):
@@ -324,18 +325,19 @@ DSPW_HD void decode_task(const ProbDev& P, int lt, int& i0, int& j0, int& k0, in
 }
 
 // (column group, segment) of a local group task of the specialised y / z
-// sweeps: groups of 8 adjacent x columns (the last of a row may be partial,
-// ncols < 8), then segments, then the remaining direction.
-template <int DIR>
+// sweeps: groups of COLS adjacent x columns (8, or 4 for the narrow tiles; the
+// last of a row may be partial, ncols < COLS), then segments, then the
+// remaining direction.
+template <int DIR, int COLS = WARPS_PER_BLOCK>
 DSPW_HD void decode_group(const ProbDev& P, int lg, int& i0, int& j0, int& k0, int& c0, int& ncell, int& ncols) {
   const int N = dir_len<DIR>(P);
   const int nseg = (N + SEG_CELLS - 1) / SEG_CELLS;
-  const int ngx = (P.nx + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+  const int ngx = (P.nx + COLS - 1) / COLS;
   const int ig = lg % ngx;
   lg /= ngx;
   const int seg = lg % nseg, o = lg / nseg;
-  i0 = ig * WARPS_PER_BLOCK;
-  ncols = min(WARPS_PER_BLOCK, P.nx - i0);
+  i0 = ig * COLS;
+  ncols = min(COLS, P.nx - i0);
   if (DIR == 1) { k0 = o; j0 = 0; } else { j0 = o; k0 = 0; }
   c0 = seg * SEG_CELLS;
   ncell = min(SEG_CELLS, N - c0);
@@ -1216,16 +1218,18 @@ __device__ void euler_task(const SweepArgs<T>& A, const ProbDev& P, ProbState& S
 // instruction (8 consecutive x per row), instead of one strided cell per lane;
 // the faces are evaluated per warp exactly as in euler_task.
 constexpr int COOP_COLS = WARPS_PER_BLOCK;
+// the narrow tiles of the y / z sweeps: 4 columns, one block of 4 warps
+constexpr int NARROW_COLS = 4;
 
 // Block-wide tiles of the cooperative sweep, behind the per-warp scratch in
 // dynamic shared memory: the staged conserved rows of the 8 columns (ghost rows
 // resolved), and the residual and U^n of the segment's cells for the epilogue.
 // Planes are the stored components 0 .. nv-1.
-template <typename T>
+template <typename T, int COLS = COOP_COLS>
 struct CoopTiles {
-  T U[5][SEG_LOAD][COOP_COLS];
-  T R[5][SEG_CELLS][COOP_COLS];
-  T Un[5][SEG_CELLS][COOP_COLS];
+  T U[5][SEG_LOAD][COLS];
+  T R[5][SEG_CELLS][COLS];
+  T Un[5][SEG_CELLS][COLS];
 };
 static_assert(sizeof(WarpSmem<double>) % 16 == 0, "WarpSmem<double> alignment");
 
@@ -1239,16 +1243,8 @@ template <int N>
 __device__ inline void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // u[5] of one tile entry (plane layout of load_cons)
-template <typename T>
-__device__ inline void tile_cons(const T (*U)[SEG_LOAD][COOP_COLS], int nv, int q, int col, T u[5]) {
-  u[0] = U[0][q][col];
-  u[1] = U[1][q][col];
-  if (nv == 5) { u[2] = U[2][q][col]; u[3] = U[3][q][col]; u[4] = U[4][q][col]; }
-  else if (nv == 4) { u[2] = U[2][q][col]; u[3] = T(0); u[4] = U[3][q][col]; }
-  else { u[2] = T(0); u[3] = T(0); u[4] = U[2][q][col]; }
-}
-template <typename T>
-__device__ inline void tile_cons(const T (*U)[SEG_CELLS][COOP_COLS], int nv, int q, int col, T u[5]) {
+template <typename T, int ROWS, int COLS>
+__device__ inline void tile_cons(const T (*U)[ROWS][COLS], int nv, int q, int col, T u[5]) {
   u[0] = U[0][q][col];
   u[1] = U[1][q][col];
   if (nv == 5) { u[2] = U[2][q][col]; u[3] = U[3][q][col]; u[4] = U[4][q][col]; }
@@ -1268,13 +1264,13 @@ __device__ inline void tile_cons(const T (*U)[SEG_CELLS][COOP_COLS], int nv, int
 // Conversion of the staged rows of a block task: row q = tid / 8 (+ 32) of
 // column col, from the tile U (ghost rows already resolved to their source
 // rows), into the per-warp primitive / entropy rows of warp `col`.
-template <typename T, int DIR>
-__device__ __forceinline__ void coop_convert(const ProbDev& P, WarpSmem<T>* sm0, const T (*U)[SEG_LOAD][COOP_COLS], int c0,
+template <typename T, int DIR, int COLS>
+__device__ __forceinline__ void coop_convert(const ProbDev& P, WarpSmem<T>* sm0, const T (*U)[SEG_LOAD][COLS], int c0,
                                     int nrow, int ncols) {
-  const int tid = threadIdx.x, col = tid % COOP_COLS;
+  const int tid = threadIdx.x, col = tid % COLS;
   const int N = dir_len<DIR>(P);
   const T G = T(P.gamma);
-  for (int q = tid / COOP_COLS; q < nrow && col < ncols; q += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
+  for (int q = tid / COLS; q < nrow && col < ncols; q += 32) {   // COLS warps: 32 rows per pass
     const int c = c0 - 2 + q;
     const int side = c < 0 ? 0 : 1;
     const int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + side];
@@ -1286,7 +1282,7 @@ __device__ __forceinline__ void coop_convert(const ProbDev& P, WarpSmem<T>* sm0,
       int flip;
       ghost_source(c, N, kind, flip);
       T u[5];
-      tile_cons<T>(U, P.nv, q, col, u);
+      tile_cons(U, P.nv, q, col, u);
       cons_to_prim<T>(u, G, p);
       if (flip) p[1 + DIR] = -p[1 + DIR];
     }
@@ -1302,18 +1298,18 @@ __device__ __forceinline__ void coop_convert(const ProbDev& P, WarpSmem<T>* sm0,
 // fluxes, then either the stored residual or the stage update from the tiles
 // U (rows + 2) and Un, with threads laid out as 4 rows x 8 columns per warp
 // instruction (coalesced stores).
-template <typename T, int DIR>
+template <typename T, int DIR, int COLS>
 __device__ __forceinline__ void coop_epilogue(const SweepArgs<T>& A, const ProbDev& P, const ProbState& S, WarpSmem<T>* sm0,
-                                     const T (*U)[SEG_LOAD][COOP_COLS], const T (*Rt)[SEG_CELLS][COOP_COLS],
-                                     const T (*Unt)[SEG_CELLS][COOP_COLS], int i0, int j0, int k0, int c0,
+                                     const T (*U)[SEG_LOAD][COLS], const T (*Rt)[SEG_CELLS][COLS],
+                                     const T (*Unt)[SEG_CELLS][COLS], int i0, int j0, int k0, int c0,
                                      int ncell, int ncols, bool final_sweep, double& smax, double& ent,
                                      unsigned& bad_fin, unsigned& bad_pos) {
-  const int tid = threadIdx.x, col = tid % COOP_COLS;
+  const int tid = threadIdx.x, col = tid % COLS;
   const int nv = P.nv;
-  for (int row = tid / COOP_COLS; row < ncell && col < ncols; row += (WARPS_PER_BLOCK * 32) / COOP_COLS) {
+  for (int row = tid / COLS; row < ncell && col < ncols; row += 32) {   // COLS warps: 32 rows per pass
     WarpSmem<T>* sc = sm0 + col;
     T R[5], r0[5];
-    tile_cons<T>(Rt, nv, row, col, r0);
+    tile_cons(Rt, nv, row, col, r0);
 #pragma unroll
     for (int v = 0; v < 5; v++) R[v] = (r0[v] - sc->F[v][row]) + sc->F[v][row + 1];
     const long long cell = cell_index<DIR>(P, i0 + col, j0, k0, c0 + row);
@@ -1321,8 +1317,8 @@ __device__ __forceinline__ void coop_epilogue(const SweepArgs<T>& A, const ProbD
       store_cons<T>(A.R, A.ctot, cell, nv, R);
     } else {
       T u[5], un[5];
-      tile_cons<T>(U, nv, row + 2, col, u);
-      tile_cons<T>(Unt, nv, row, col, un);
+      tile_cons(U, nv, row + 2, col, u);
+      tile_cons(Unt, nv, row, col, un);
       update_euler_cell<T>(A, P, S, cell, R, u, un, smax, ent, bad_fin, bad_pos);
     }
   }
@@ -1337,27 +1333,32 @@ __device__ __forceinline__ void coop_epilogue(const SweepArgs<T>& A, const ProbD
 // epilogue from shared memory.  When the rows are not 16-byte aligned in
 // global memory (nx, the problem offset or the plane stride not a multiple of
 // 16 bytes) the same tiles are filled by plain loads.
-template <typename T, int DIR, int DIM, typename Sp>
+// COLS: columns of the block, one warp each (8, or 4 for the narrow tiles of
+// k_sweep_narrow); the block has COLS warps.
+template <typename T, int DIR, int DIM, typename Sp, int COLS = COOP_COLS>
 __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbState& S,
                                  WarpSmem<T>* sm0, int lt0, bool group) {
+  static_assert(COLS == COOP_COLS || COLS == NARROW_COLS, "column count of a block");
+  constexpr int NT = COLS * 32;                       // threads of the block
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int i0, j0, k0, c0, ncell, ncols = COOP_COLS;
-  // i0 of column 0 (a multiple of 8); group tasks may end in a partial group
-  if (group) decode_group<DIR>(P, lt0, i0, j0, k0, c0, ncell, ncols);
+  int i0, j0, k0, c0, ncell, ncols = COLS;
+  // i0 of column 0 (a multiple of COLS); group tasks may end in a partial group
+  if (group) decode_group<DIR, COLS>(P, lt0, i0, j0, k0, c0, ncell, ncols);
   else decode_task<DIR>(P, lt0, i0, j0, k0, c0, ncell);
   const int N = dir_len<DIR>(P);
   const int nv = P.nv;
-  CoopTiles<T>& tl = *reinterpret_cast<CoopTiles<T>*>(sm0 + WARPS_PER_BLOCK);
+  CoopTiles<T, COLS>& tl = *reinterpret_cast<CoopTiles<T, COLS>*>(sm0 + COLS);
   const bool final_sweep = !A.residual_only && !A.viscous && (DIR == DIM - 1);
   constexpr int VEC = 16 / (int)sizeof(T);           // elements per 16-byte copy
-  constexpr int CH = COOP_COLS / VEC;                 // copies per row and plane
-  const bool aligned = ncols == COOP_COLS && (A.ctot % VEC) == 0 && (P.off % VEC) == 0 && (P.nx % VEC) == 0;
+  constexpr int CH = COLS / VEC;                      // copies per row and plane
+  static_assert(CH >= 1, "a row of the tile is at least one 16-byte copy");
+  const bool aligned = ncols == COLS && (A.ctot % VEC) == 0 && (P.off % VEC) == 0 && (P.nx % VEC) == 0;
   // group 1: staged rows q = 0 .. ncell+3 (cells c0-2 .. c0+ncell+1)
   const int nrow = ncell + 4;
   if (aligned) {
     // one thread per (row, 16-byte chunk): its ghost source is found once and
     // it issues the copies of every component (no division by the row count)
-    static_assert((SEG_CELLS + 4) * CH <= WARPS_PER_BLOCK * 32, "one pass of the block covers the staged rows");
+    static_assert((SEG_CELLS + 4) * CH <= NT, "one pass of the block covers the staged rows");
     if (tid < nrow * CH) {
       const int q = tid / CH, ch = tid - q * CH;
       const int c = c0 - 2 + q;
@@ -1382,9 +1383,8 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
     cp_async_commit();
     cp_async_wait<1>();
   } else {
-    for (int idx = tid; idx < nv * nrow * COOP_COLS; idx += WARPS_PER_BLOCK * 32) {
-      const int comp = idx / (nrow * COOP_COLS), rem = idx - comp * nrow * COOP_COLS, q = rem / COOP_COLS,
-                cc = rem - q * COOP_COLS;
+    for (int idx = tid; idx < nv * nrow * COLS; idx += NT) {
+      const int comp = idx / (nrow * COLS), rem = idx - comp * nrow * COLS, q = rem / COLS, cc = rem - q * COLS;
       const int c = c0 - 2 + q;
       const int kind = (c >= 0 && c < N) ? DSPW_BC_PERIODIC : P.bc[2 * DIR + (c < 0 ? 0 : 1)];
       if (kind == DSPW_BC_DIRICHLET || cc >= ncols) continue;
@@ -1392,9 +1392,8 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
       const int src = ghost_source(c, N, kind, flip);
       tl.U[comp][q][cc] = A.Uin[comp * A.ctot + cell_index<DIR>(P, i0 + cc, j0, k0, src)];
     }
-    for (int idx = tid; idx < nv * ncell * COOP_COLS; idx += WARPS_PER_BLOCK * 32) {
-      const int comp = idx / (ncell * COOP_COLS), rem = idx - comp * ncell * COOP_COLS, q = rem / COOP_COLS,
-                cc = rem - q * COOP_COLS;
+    for (int idx = tid; idx < nv * ncell * COLS; idx += NT) {
+      const int comp = idx / (ncell * COLS), rem = idx - comp * ncell * COLS, q = rem / COLS, cc = rem - q * COLS;
       if (cc >= ncols) continue;
       const long long off = comp * A.ctot + cell_index<DIR>(P, i0 + cc, j0, k0, c0 + q);
       tl.R[comp][q][cc] = A.R[off];
@@ -1402,7 +1401,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
     }
   }
   __syncthreads();
-  coop_convert<T, DIR>(P, sm0, tl.U, c0, nrow, ncols);
+  coop_convert<T, DIR, COLS>(P, sm0, tl.U, c0, nrow, ncols);
   __syncthreads();
   int viol = 0;
   unsigned long long signv = 0;
@@ -1414,8 +1413,8 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
   double smax = 0.0;
   double ent = 0.0;
   unsigned bad_fin = 0, bad_pos = 0;
-  coop_epilogue<T, DIR>(A, P, S, sm0, tl.U, tl.R, tl.Un, i0, j0, k0, c0, ncell, ncols, final_sweep, smax, ent,
-                        bad_fin, bad_pos);
+  coop_epilogue<T, DIR, COLS>(A, P, S, sm0, tl.U, tl.R, tl.Un, i0, j0, k0, c0, ncell, ncols, final_sweep, smax,
+                              ent, bad_fin, bad_pos);
   if (!final_sweep) { smax = 0.0; ent = 0.0; }
   warp_epilogue<T>(A, A.final_stage && final_sweep, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
   __syncthreads();
@@ -1605,7 +1604,7 @@ __device__ __forceinline__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpS
       for (int comp = 0; comp < P.nv; comp++) U[comp][q][cc] = A.Uin[comp * A.ctot + cell];
     }
     __syncthreads();
-    coop_convert<T, DIR>(P, sm0, (UTile)U, c0, nrow, COOP_COLS);
+    coop_convert<T, DIR, COOP_COLS>(P, sm0, (UTile)U, c0, nrow, COOP_COLS);
     __syncthreads();
     // the next task's rows into the other buffer, behind this task's faces
     if (tid == 0 && gn < A.ntask) {
@@ -1622,7 +1621,7 @@ __device__ __forceinline__ void euler_coop_tma_loop(const SweepArgs<T>& A, WarpS
     __syncthreads();
     double smax = 0.0, ent = 0.0;
     unsigned bad_fin = 0, bad_pos = 0;
-    coop_epilogue<T, DIR>(A, P, S, sm0, (UTile)U, (CTile)rbuf, (CTile)unbuf, i0, j0, k0, c0, ncell, COOP_COLS,
+    coop_epilogue<T, DIR, COOP_COLS>(A, P, S, sm0, (UTile)U, (CTile)rbuf, (CTile)unbuf, i0, j0, k0, c0, ncell, COOP_COLS,
                           final_sweep, smax, ent, bad_fin, bad_pos);
     if (!final_sweep) { smax = 0.0; ent = 0.0; }
     warp_epilogue<T>(A, A.final_stage && final_sweep, S, lane, smax, ent, bad_fin, bad_pos, signv, viol, checked);
@@ -1806,6 +1805,29 @@ k_sweep_tma(const __grid_constant__ SweepArgs<T> A) {
   const int lane = threadIdx.x & 31;
   if (Sp::rec == 2) net_frag_stage<T>(*A.net, lane, sm0[threadIdx.x >> 5].ns);
   euler_coop_tma_loop<T, DIR, Sp::dim, Sp>(A, sm0);
+}
+
+// The specialised y / z sweeps with narrow tiles: blocks of 4 warps on 4
+// adjacent columns (16-byte FP32 rows, per-thread cp.async staging), twice the
+// resident blocks per SM of k_sweep at the same registers per thread.  Each
+// block barrier then waits for 4 warps instead of 8.  The task list of a
+// direction that runs it counts groups of 4 columns (decode_group).
+template <typename T, int DIR, typename Sp>
+__global__ void __launch_bounds__(NARROW_COLS * 32, 2 * MinBlocks<T>::value)
+k_sweep_narrow(const __grid_constant__ SweepArgs<T> A) {
+  static_assert(Sp::fixed && DIR >= 1, "narrow tiles are for the specialised y / z sweeps");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem<T>* sm0 = reinterpret_cast<WarpSmem<T>*>(smem_raw);
+  const int lane = threadIdx.x & 31;
+  if (Sp::rec == 2) net_frag_stage<T>(*A.net, lane, sm0[threadIdx.x >> 5].ns);
+  for (int g = blockIdx.x; g < A.ntask; g += gridDim.x) {
+    const int p = find_problem(A.task_start, A.nprob, g);
+    const int pp = A.pmap ? __ldg(A.pmap + p) : p;
+    const ProbDev& P = A.prob[pp];
+    ProbState& S = A.st[pp];
+    if (!A.residual_only && !*((volatile int*)&S.active)) continue;
+    euler_coop_block<T, DIR, Sp::dim, Sp, NARROW_COLS>(A, P, S, sm0, g - __ldg(A.task_start + p), true);
+  }
 }
 
 // The x sweep of 1-D scalar problems alone: the reconstruction family fixed at

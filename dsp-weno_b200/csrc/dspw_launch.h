@@ -15,7 +15,8 @@ struct Launch {
   // spec: 0 for the generic kernel, spec_code(dim, rec) for a SpecHot kernel
   static cudaError_t sweep(int dir, const SweepArgs<T>& a, int grid, cudaStream_t s, int spec);
   // resident blocks per SM of that sweep kernel (occupancy calculator)
-  static int sweep_blocks_per_sm(int dir, int spec);
+  // narrow: the 4-column tiles of k_sweep_narrow (specialised y / z sweeps)
+  static int sweep_blocks_per_sm(int dir, int spec, int narrow = 0);
   static cudaError_t upload(const ProbDev* prob, ProbState* st, int p, const double* prim, T* U, long long ctot,
                             long long ncell, cudaStream_t s);
   static cudaError_t speed(const ProbDev* prob, ProbState* st, int p, const T* U, long long ctot, long long ncell,

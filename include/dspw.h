@@ -129,10 +129,12 @@ typedef struct dspw_desc {
                                 plain SP-WENO (FP32 form) */
   int generic_kernels;       /* 1: run this problem on the generic sweep kernels even when
                                 specialised ones exist (validation) */
-  int tile_staging;          /* y / z sweeps of the specialised kernels: 0 = per-thread cp.async
-                                copies, or Tensor Memory Accelerator loads where dspw_tune measures
-                                them faster; 1 = cp.async always; 2 = TMA where the problem allows
-                                it (nx a multiple of 8, 16-byte aligned rows and planes) */
+  int tile_staging;          /* y / z sweeps of the specialised kernels: 0 = tiles of 8 columns
+                                staged by per-thread cp.async copies, or the variant dspw_tune
+                                measures faster (Tensor Memory Accelerator loads, or tiles of 4
+                                columns); 1 = 8 columns, cp.async always; 2 = 8 columns, TMA where
+                                the problem allows it (nx a multiple of 8, 16-byte aligned rows and
+                                planes); 3 = 4 columns (blocks of 4 warps), cp.async */
   int reserved_i[5];         /* zero */
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double gamma, gas_const, prandtl, mu_ref, T_ref, T_0, omega;
@@ -234,16 +236,19 @@ DSPW_API int dspw_errors(dspw_handle* h, int p, int comp, const double* exact, d
  * milliseconds (kernel_ms, up to max_k entries, launch order: begin-step,
  * per stage the sweeps x/y/z [and the viscous kernels], end-step) and a short
  * name per launch (names: max_k rows of 16 chars).  For measurement only. */
-/* Launch-grid autotuner (no counterpart in the reference, whose loops are
+/* Launch autotuner (no counterpart in the reference, whose loops are
    serial): for every kernel class and sweep direction of the handle, times the
    sweep on the current state (a residual evaluation, which writes only the
    residual buffer) with its default grid and with persistent grids of 1, 2 and
-   4 times the resident blocks of the GPU, keeps the fastest, and drops the
-   step graph so that the next step is captured with the chosen grids.  The
-   state, the problems' clocks and the status counters are unchanged.  reps:
-   timed launches per candidate (their median is compared, 1..1000).
+   4 times the resident blocks of the GPU, for the specialised y / z sweeps
+   also with tiles of 8 and of 4 columns and, where tensor maps exist, with
+   cp.async and TMA staging (within what tile_staging allows); keeps the
+   fastest, and drops the step graph so that the next step is captured with
+   the choice.  Every candidate computes the same bits.  The state, the
+   problems' clocks and the status counters are unchanged.  reps: timed
+   launches per candidate (their median is compared, 1..1000).
    before_ms / after_ms (nullable): summed sweep times with the default and the
-   chosen grids. */
+   chosen launches. */
 DSPW_API int dspw_tune(dspw_handle* h, int reps, double* before_ms, double* after_ms);
 
 DSPW_API int dspw_profile_step(dspw_handle* h, double* kernel_ms, char* names, int max_k, int* nk);

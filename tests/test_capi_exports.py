@@ -96,7 +96,7 @@ def test_bad_descriptor_rejected_without_gpu():
     d.generic_kernels = 2
     assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
     d = capi.make_desc()
-    d.tile_staging = 3   # 0 automatic, 1 cp.async, 2 TMA
+    d.tile_staging = 4   # 0 automatic, 1 cp.async, 2 TMA, 3 narrow tiles
     assert lib.dspw_create(ctypes.byref(d), ctypes.byref(h)) == 1
     d = capi.set_training_box(capi.make_desc(), [0, 0, 0, 0, 0], [1, 1, 1, 1, 1])
     d.nn_feat_lo[3] = 2.0   # lo above hi

@@ -1,10 +1,13 @@
-"""TMA staging of the specialised y / z sweeps against per-thread cp.async
-staging.  The two paths stage the same tiles and run the same arithmetic, so
-the FP64 cases agree bit for bit and the FP32 ones to rounding: periodic wrap, walls and neumann faces
-(whose ghost rows lie outside the tensor map and are patched after the box
-load), partial last segments, several problems per kernel class (tensor maps
-per problem), 3-D (the z sweep), FP64 and FP32 + BF16 DSP-WENO, a slab with
-halo faces, and the residual evaluation of the grid tuner."""
+"""The tile variants of the specialised y / z sweeps against 8-column tiles
+staged by per-thread cp.async copies: TMA staging (tile_staging 2) and narrow
+tiles of 4 columns (tile_staging 3, k_sweep_narrow).  Every variant stages the
+same rows and runs the same arithmetic per face and cell, so the FP64 cases
+agree bit for bit and the FP32 ones to rounding: periodic wrap, walls and
+neumann faces (whose ghost rows lie outside the tensor map and are patched
+after the box load), partial last segments and partial column groups, several
+problems per kernel class (tensor maps per problem), 3-D (the z sweep), FP64
+and FP32 + BF16 DSP-WENO, a slab with halo faces, and the residual evaluation
+of the tuner."""
 import numpy as np
 import pytest
 
@@ -53,17 +56,23 @@ CASES = {
         [make_desc(model="euler", flux="kepes_tecno4_roe", recon=rc, nx=16, ny=24, nz=35, precision=pr,
                    network=net(), bc=["periodic", "periodic", "neumann", "wall", "wall", "neumann"])],
         [_bump(16, 24, 35)]),
+    # nx = 30: the last column group of a row is partial for both widths
+    # (TMA does not qualify; the narrow and wide tiles run plain loads there)
+    "partial_groups": lambda pr, rc: (
+        [make_desc(model="euler", flux="kepes_tecno4_roe", recon=rc, nx=30, ny=50, precision=pr, network=net(),
+                   bc=["periodic", "periodic", "wall", "neumann", "periodic", "periodic"])], [_bump(30, 50)]),
 }
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
 @pytest.mark.parametrize("precision,recon", [("fp64", "sp_weno"), ("fp64", "sp_weno_dl"),
                                              ("fp32_bf16", "sp_weno_dl"), ("fp32_bf16", "sp_weno")])
-def test_tma_staging_equals_cp_async(case, precision, recon):
+@pytest.mark.parametrize("variant", [2, 3], ids=["tma", "narrow"])
+def test_tile_variant_equals_cp_async(case, precision, recon, variant):
     d1, p1 = CASES[case](precision, recon)
     d2, p2 = CASES[case](precision, recon)
-    a, sa = _run(d1, p1, 6, 2)   # TMA
-    b, sb = _run(d2, p2, 6, 1)   # cp.async
+    a, sa = _run(d1, p1, 6, variant)   # TMA / narrow tiles
+    b, sb = _run(d2, p2, 6, 1)         # 8-column tiles, cp.async
     for x, y in zip(a, b):
         if precision == "fp64":
             # IEEE arithmetic without contraction: the two kernels give the same bits
@@ -79,25 +88,25 @@ def test_tma_staging_equals_cp_async(case, precision, recon):
     assert sa.faces_checked == sb.faces_checked and sa.sign_violations == sb.sign_violations
 
 
-def test_tma_staging_on_slabs_with_halo_faces():
+def test_tile_variants_on_slabs_with_halo_faces():
     """Three slabs of a periodic 2-D domain stepped with their halo layers
     exchanged: the ghost rows are the stored halo layers beside each slab's
-    interior, outside its tensor map.  Both staging paths give the same bits."""
+    interior, outside its tensor map.  Every variant gives the same bits."""
     from dspw.slabs import LocalSlabs
     out = []
-    for staging in (2, 1):
+    for staging in (2, 1, 3):
         dom = make_desc(model="euler", flux="kepes_tecno4_roe", recon="sp_weno", nx=32, ny=96)
         dom.tile_staging = staging
         sl = LocalSlabs(dom, 3)
         sl.upload_prim(_bump(32, 96))
         sl.step(3)
         out.append(sl.cons())
-    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[2], out[1])
 
 
 def test_tuner_keeps_results_with_either_staging():
-    """dspw_tune times both stagings (tile_staging 0) and keeps the faster;
-    the state it leaves steps to the same bits as cp.async staging."""
+    """dspw_tune times the tile variants (tile_staging 0) and keeps the
+    fastest; the state it leaves steps to the cp.async results."""
     (d,), (p,), _ = W.kh(128, "fp32_bf16", "sp_weno_dl", net())
     s = Solver(d)
     s.upload_prim(p)
@@ -110,5 +119,5 @@ def test_tuner_keeps_results_with_either_staging():
     s2.upload_prim(p)
     s2.step(3)
     a, b = s.cons(), s2.cons()
-    # the same bits when the tuner kept cp.async; FP32 rounding when it took TMA
+    # the same bits when the tuner kept cp.async; FP32 rounding for another variant
     assert np.max(np.abs(a - b)) <= 1e-3 * np.max(np.abs(b))
