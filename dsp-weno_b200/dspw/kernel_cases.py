@@ -2,6 +2,10 @@
 captures of single kernels (no timing, no output beyond "ok"):
 
     python -m dspw.kernel_cases kh N PRECISION RECON STEPS   (run from dsp-weno_b200/)
+    python -m dspw.kernel_cases kh_tuned N PRECISION RECON STEPS
+                                               the same after dspw_tune (as the benchmark
+                                               runs it); the profiler is started after the
+                                               tuning (ncu --profile-from-start off)
     python -m dspw.kernel_cases burgers        4096 Burgers problems, k_sweep_scalar
     python -m dspw.kernel_cases tgv N PRECISION RECON STEPS  Navier-Stokes: k_entvars,
                                                k_visc_nodes, k_visc_update, the z sweep
@@ -22,11 +26,17 @@ NET_FILE = Path(__file__).resolve().parents[2] / "tests" / "golden" / "dsp_weno.
 def main(argv):
     net = load_network_file(NET_FILE)
     mode = argv[0]
-    if mode in ("kh", "tgv"):
+    if mode in ("kh", "tgv", "kh_tuned"):
         n, prec, rec, steps = int(argv[1]), argv[2], argv[3], int(argv[4])
-        d, p, _ = (W.kh if mode == "kh" else W.tgv)(n, prec, rec, net)
+        d, p, _ = (W.tgv if mode == "tgv" else W.kh)(n, prec, rec, net)
         s = Solver(d)
         s.upload_prim(p[0])
+        if mode == "kh_tuned":
+            import torch
+
+            s.tune(reps=3)
+            s.sync()
+            torch.cuda.profiler.start()
         s.step(steps)
         s.sync()
     elif mode == "burgers":
