@@ -367,6 +367,8 @@ def measure_gpu(args, torch, dist, rank, world):
 
     s = solver(descs, prims)
     if args.profile_only:
+        # the profiler starts after upload and tuning (ncu --profile-from-start off)
+        torch.cuda.profiler.start()
         s.step(args.warmup)
         s.step(args.steps)
         s.sync()
@@ -617,7 +619,8 @@ def main():
     ap.add_argument("--no-matched-error", action="store_true",
                     help="leave the matched-error summary out of the KH line")
     ap.add_argument("--profile-only", action="store_true",
-                    help="warm-up and timed steps only (no e2e, CPU or FP64 legs); for ncu captures")
+                    help="warm-up and timed steps only (no e2e, CPU or FP64 legs), the profiler started "
+                         "after upload and tuning; for ncu captures with --profile-from-start off")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
