@@ -56,13 +56,37 @@ SOURCES = sorted(f for f in (REPO / "dsp-weno_b200" / "csrc").glob("*") if f.nam
     [REPO / "include" / "dspw.h"]
 
 
+def strip_comments(src: str) -> str:
+    """C / C++ source without its // and /* */ comments (string and character
+    literals kept as they are), so that a comment edit keeps the build's hash."""
+    out, i, n = [], 0, len(src)
+    while i < n:
+        c = src[i]
+        if c in "\"'":
+            j = i + 1
+            while j < n and src[j] != c:
+                j += 2 if src[j] == "\\" else 1
+            out.append(src[i:j + 1])
+            i = j + 1
+        elif src.startswith("//", i):
+            j = src.find("\n", i)
+            i = n if j < 0 else j
+        elif src.startswith("/*", i):
+            j = src.find("*/", i + 2)
+            i = n if j < 0 else j + 2
+        else:
+            out.append(c)
+            i += 1
+    return "".join(out)
+
+
 def source_hash() -> str:
-    """sha256 (16 hex digits) of the device sources and the C ABI header."""
+    """sha256 (16 hex digits) of the device sources and the C ABI header, comments removed."""
     import hashlib
     h = hashlib.sha256()
     for f in SOURCES:
         h.update(f.name.encode())
-        h.update(f.read_bytes())
+        h.update(strip_comments(f.read_text()).encode())
     return h.hexdigest()[:16]
 
 

@@ -1425,7 +1425,7 @@ __device__ void euler_coop_block(const SweepArgs<T>& A, const ProbDev& P, ProbSt
 // The specialised y and z sweeps can stage their tiles with the Tensor Memory
 // Accelerator instead of per-thread cp.async copies: one thread issues one
 // cp.async.bulk.tensor per tile (box of 8 columns x rows x nv planes of this
-// GPU's own state, no multicast) that signals an mbarrier when its bytes have
+// GPU's own state, loaded into this block alone) that signals an mbarrier when its bytes have
 // landed.  Each block runs its tasks in a loop that prefetches the next task's
 // staged rows into a second buffer while the current task's faces are
 // evaluated, and loads the residual and U^n of a task at the task's start (they
