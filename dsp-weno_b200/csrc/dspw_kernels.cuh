@@ -396,6 +396,10 @@ struct WarpSmem {
   T W[5][32];      // wide two-point fluxes, centre g = c0 - 1 + idx
   T F[5][32];      // face fluxes, face f = c0 + idx
   NetScratch<T> ns;
+  // padding to a length of 12 words mod 32 (FP32: 1580 words, FP64: 1420):
+  // the cooperative block's accesses to 8 warps' scratch at one index (4 rows
+  // x 8 columns per warp instruction) then hit 32 different banks
+  T pad[sizeof(T) == 4 ? 4 : 16];
 };
 // mlp_warp_tiles addresses the scratch by these byte offsets, with 16-byte
 // vector accesses to the rows of every warp's scratch
@@ -403,6 +407,7 @@ static_assert(offsetof(NetScratch<float>, logit) == 1024 && offsetof(NetScratch<
               "NetScratch<float> layout");
 static_assert(offsetof(WarpSmem<float>, ns) % 16 == 0 && sizeof(WarpSmem<float>) % 16 == 0,
               "WarpSmem<float> alignment");
+static_assert((sizeof(WarpSmem<float>) / 4) % 32 == 12, "WarpSmem<float> bank spread");
 
 // ---------------------------------------------------- two-point fluxes ------
 
@@ -686,7 +691,9 @@ static __device__ __noinline__ void mlp_warp_tiles(unsigned ns_addr) {
                : "=f"(nf.bias0[0]), "=f"(nf.bias0[1]), "=f"(nf.bias0[2]), "=f"(nf.bias0[3]) : "r"(fa + 16u));
   asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
                : "=f"(nf.bias1[0]), "=f"(nf.bias1[1]), "=f"(nf.bias1[2]), "=f"(nf.bias1[3]) : "r"(fa + 32u));
-  const unsigned r = lane >> 2, kq = (lane & 3) * 2;
+  // rows 16 t + r and 16 t + r + 8 share the half swap of rows with bit 2 set
+  // (warp_mlp_bf16): (16 t + r) >> 2 & 1 = r >> 2 & 1 = lane >> 4 & 1
+  const unsigned r = lane >> 2, kq = ((lane & 3) * 2) ^ (((lane >> 4) & 1u) << 2);
 #pragma unroll
   for (unsigned t = 0; t < 2; t++) {
     const unsigned lo = ((16 * t + r) * 8 + kq) * 4, hi = ((16 * t + r + 8) * 8 + kq) * 4;
@@ -696,15 +703,19 @@ static __device__ __noinline__ void mlp_warp_tiles(unsigned ns_addr) {
 }
 
 // in: this lane's 5 inputs; out: this lane's 5 logits.  Every lane of the
-// warp must call it.
+// warp must call it.  A row of 8 floats holds columns 0-3 and 4-7 in its two
+// 16-byte halves, swapped in rows with bit 2 set: the 16-byte accesses of 8
+// consecutive lanes (rows 32 bytes apart) then fall into 32 different banks.
 __device__ inline void warp_mlp_bf16(NetScratch<float>& ns, const float in[5], float out[5], int lane) {
+  const int h = (lane >> 2) & 1;
   float4* f = reinterpret_cast<float4*>(&ns.feat[lane][0]);
-  f[0] = make_float4(in[0], in[1], in[2], in[3]);
-  f[1] = make_float4(in[4], 0.f, 0.f, 0.f);
+  f[h] = make_float4(in[0], in[1], in[2], in[3]);
+  f[h ^ 1] = make_float4(in[4], 0.f, 0.f, 0.f);
   mlp_warp_tiles((unsigned)__cvta_generic_to_shared(&ns));
-  const float4 o = *reinterpret_cast<const float4*>(&ns.logit[lane][0]);
-  out[0] = o.x; out[1] = o.y; out[2] = o.z; out[3] = o.w;
-  out[4] = ns.logit[lane][4];
+  const float4* o = reinterpret_cast<const float4*>(&ns.logit[lane][0]);
+  const float4 lo = o[h], hi = o[h ^ 1];
+  out[0] = lo.x; out[1] = lo.y; out[2] = lo.z; out[3] = lo.w;
+  out[4] = hi.x;
 }
 
 // DSP-WENO reconstruction of one stencil per lane, warp-cooperative network.
@@ -1232,6 +1243,7 @@ struct CoopTiles {
   T Un[5][SEG_CELLS][COLS];
 };
 static_assert(sizeof(WarpSmem<double>) % 16 == 0, "WarpSmem<double> alignment");
+static_assert((sizeof(WarpSmem<double>) / 4) % 32 == 12, "WarpSmem<double> bank spread");
 
 // 16-byte global -> shared copy that completes asynchronously (L2 only)
 __device__ inline void cp_async16(void* smem, const void* gmem) {
