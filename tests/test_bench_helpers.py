@@ -38,3 +38,14 @@ def test_records_parse(tmp_path, monkeypatch):
     a = bench.read_records("accuracy")
     assert a[0]["n"] == 2048 and a[0]["l1_ratio"] == 1.1
     assert len(bench.source_hash()) == 16
+
+
+def test_source_hash_ignores_comments_only():
+    """The build hash drops // and /* */ comments but keeps string and
+    character literals (a "//" inside a PTX string is code)."""
+    src = 'asm("mov.u32 %0, 1; // not a comment");\n/* block\ncomment */ int a = \'/\'; // tail\nint b;\n'
+    out = bench.strip_comments(src)
+    assert '"mov.u32 %0, 1; // not a comment"' in out and "'/'" in out
+    assert "block" not in out and "tail" not in out and "int b;" in out
+    assert bench.strip_comments("int x = 1; // one") == bench.strip_comments("int x = 1; // two")
+    assert bench.strip_comments("int x = 1;") != bench.strip_comments("int x = 2;")
